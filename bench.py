@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark: CP-ALS sweeps and MTTKRP bandwidth on the 512 x 512 x 512,
+rank-64 FP32 workload (synthetic: sum of 64 rank-1 terms with uniform [0,1)
+factors plus 1e-3 relative Gaussian noise), one process per GPU.
+
+A step is one CP-ALS sweep (three MTTKRPs, the FP64 normal-equation solves,
+Gram updates and the fit) on device-resident data, replayed from the sweep's
+CUDA graph.  `value` is the MTTKRP traffic the sweep implies (3 x algorithmic
+bytes per MTTKRP) divided by the sweep time, in GB/s, summed over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's CPU path (the ALS of
+decomposition/CPU/python/mycp.py, restated on NumPy/OpenBLAS because
+TensorLy is not installed) on a bounded slab of the same workload, on this
+host's cores, and reports the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "first-project_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "CP-ALS time-to-fit & MTTKRP GB/s (% HBM peak), mixed/learned vs plain FP32"
+
+
+def mttkrp_bytes(dims, R, mode):
+    """Algorithmic bytes of one MTTKRP: the FP32 tensor once, the input
+    factors and the output factor (4 B each)."""
+    n = 1
+    for d in dims:
+        n *= d
+    fac = sum(d for i, d in enumerate(dims) if i != mode) + dims[mode]
+    return 4 * n + 4 * R * fac
+
+
+def sweep_bytes(dims, R):
+    return sum(mttkrp_bytes(dims, R, m) for m in range(len(dims)))
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        if not getattr(self, "lines", None):
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sweep_gbs(X3, factors, sweeps=1):
+    """Times NumPy ALS sweeps (oracle port of mycp.py) -> (GB/s, seconds)."""
+    import numpy as np
+    import oracle
+    dims = X3.shape
+    R = factors[0].shape[1]
+    oracle.numpy_cp_als_sweep(X3, [f.copy() for f in factors])  # warm the BLAS threads
+    t0 = time.perf_counter()
+    for _ in range(sweeps):
+        oracle.numpy_cp_als_sweep(X3, factors)
+    dt = time.perf_counter() - t0
+    return sweep_bytes(dims, R) * sweeps / dt / 1e9, dt
+
+
+def cpu_sample(dims, R, seed=0, slab=64):
+    """A bounded slab (first `slab` indices of the last mode) of the same
+    synthetic workload, generated on the host."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    d = list(dims)
+    d[-1] = min(slab, d[-1])
+    facs = [rng.random((n, R)) for n in d]
+    K = facs[1]
+    for m in range(2, len(d)):
+        K = (facs[m][:, None, :] * K[None, :, :]).reshape(-1, R)
+    X = (facs[0] @ K.T).reshape(d, order="F")
+    X += 1e-3 * np.linalg.norm(X) / np.sqrt(X.size) * rng.standard_normal(X.shape)
+    X = np.asfortranarray(X.astype(np.float32).astype(np.float64))
+    init = [rng.random((n, R)) for n in d]
+    return X, init, d
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU ALS on the host cores."""
+    import numpy as np
+    dims = [int(x) for x in args.dims.split(",")]
+    R = args.rank
+    X3, init, sd = cpu_sample(dims, R, slab=args.cpu_slab)
+    cores = os.cpu_count()
+    for _ in range(max(0, args.warmup)):
+        cpu_sweep_gbs(X3, [f.copy() for f in init], 1)
+    times = []
+    facs = [f.copy() for f in init]
+    for _ in range(args.steps):
+        _, dt = cpu_sweep_gbs(X3, facs, 1)
+        times.append(dt)
+    tot = sum(times)
+    value = sweep_bytes(sd, R) * args.steps / tot / 1e9
+    line = {
+        "metric": METRIC, "impl": "reference", "value": round(value, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * tot / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+        "config": config_dict(dims, R, "fp64-numpy"),
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+                         "sample": f"one ALS sweep per step on a {sd[0]}x{sd[1]}x{sd[2]} slab "
+                                   f"(rank {R}) of the workload; NumPy/OpenBLAS restatement of "
+                                   f"decomposition/CPU/python/mycp.py"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(dims, R, precision, world=1):
+    return {"workload": f"cp_als_sweep_{'x'.join(map(str, dims))}_r{R}", "dims": dims, "rank": R,
+            "precision": precision, "global_batch": world, "seq_len": None,
+            "parallelism": f"dp{world}" if world > 1 else "single",
+            "l2": "inputs (512 MiB per tensor) exceed the 126 MB L2; no flush between steps"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--dims", default="512,512,512")
+    ap.add_argument("--rank", type=int, default=64)
+    ap.add_argument("--precision", default="default")
+    ap.add_argument("--e2e-sweeps", type=int, default=10)
+    ap.add_argument("--cpu-slab", type=int, default=64)
+    ap.add_argument("--no-ttf", action="store_true", help="skip the time-to-fit runs")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+    import cudecompose as cd
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = dist_mod
+
+    dims = [int(x) for x in args.dims.split(",")]
+    R = args.rank
+    prec = cd.PRECISIONS[args.precision]
+    prec_name = "bf16x3" if prec in (cd.PREC_DEFAULT, cd.PREC_BF16X3) else args.precision
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        X, _ = cd.make_cp_tensor(dims, R, seed=1000 + rank)
+        init = cd.make_init(dims, R, seed=2000 + rank)
+    stream.synchronize()
+
+    # ---- kernel level: MTTKRP per mode, CUDA events on the launching stream
+    kern = {}
+    U = [u.clone() for u in init]
+    outs = [torch.empty(d * R, device="cuda") for d in dims]
+    reps = 10
+    for mode in range(len(dims)):
+        for _ in range(3):
+            cd.mttkrp(X, dims, U, mode, R, outs[mode], prec, stream=sptr)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            cd.mttkrp(X, dims, U, mode, R, outs[mode], prec, stream=sptr)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        kern[mode] = {"ms": round(ms, 5), "gbs": round(mttkrp_bytes(dims, R, mode) / ms / 1e6, 1)}
+
+    # ---- timed sweeps through the plan (graph replay)
+    plan = cd.CpPlan(X, dims, R, U, precision=prec, stream=sptr)
+    plan.run(args.warmup, stream=sptr)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.run(args.steps, stream=sptr)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    kps, fallbacks = plan.info()
+    fit_now, _ = plan.fit(stream=sptr)
+    plan.close()
+    per_rank_bytes = sweep_bytes(dims, R) * args.steps
+    value = world * per_rank_bytes / (ms_total * 1e-3) / 1e9
+
+    peak, peak_kind = load_peaks()
+    dom_mode = max(kern, key=lambda m: kern[m]["ms"])
+    avg_ms = sum(k["ms"] for k in kern.values()) / len(kern)
+    avg_bytes = sum(mttkrp_bytes(dims, R, m) for m in kern) / len(kern)
+    achieved = avg_bytes / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "mttkrp_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        key = f"{'x'.join(map(str, dims))}_r{R}_{prec_name}"
+        traffic = tj.get(key)
+
+    result = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_total / args.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic", "config": config_dict(dims, R, prec_name, world),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "kernel": "MTTKRP (mean over the 3 modes)", "per_mode": kern},
+        "gpu_launches": kps * args.steps if kps and kps > 0 else None,
+        "kernels_per_sweep": kps, "fit_after_timed_sweeps": round(fit_now, 8),
+        "clocks": clk.summary(),
+    }
+
+    # ---- time to fit (<= 50 sweeps or delta fit < 1e-6), per precision
+    if not args.no_ttf:
+        ttf = {}
+        for name in ("fp32", "bf16x3", "bf16"):
+            Ut = [u.clone() for u in init]
+            torch.cuda.synchronize()
+            res = cd.cp_als(X, dims, R, Ut, max_sweeps=50, tol=1e-6,
+                            precision=cd.PRECISIONS[name], stream=sptr)
+            ttf[name] = {"seconds": round(res.seconds, 5), "sweeps": res.sweeps,
+                         "fit": round(res.fit, 8)}
+        base = ttf["fp32"]["seconds"]
+        for name in ttf:
+            ttf[name]["speedup_vs_fp32"] = round(base / ttf[name]["seconds"], 3) if ttf[name]["seconds"] else None
+            ttf[name]["fit_delta_vs_fp32"] = round(abs(ttf[name]["fit"] - ttf["fp32"]["fit"]), 8)
+        result["time_to_fit"] = ttf
+
+    # ---- end to end through the C ABI with host buffers: H2D of X and the
+    # initial factors, cud_cp_als (plan + e2e_sweeps sweeps), D2H of factors
+    n = X.numel()
+    hX = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    hX.copy_(X)
+    hU = [u.cpu().pin_memory() for u in init]
+    dX = torch.empty_like(X)
+    dU = [torch.empty_like(u) for u in init]
+    oU = [torch.empty(u.numel(), dtype=torch.float32, pin_memory=True) for u in init]
+    e2e_steps = max(2, min(args.steps, 5))
+    times = []
+    for it in range(e2e_steps + 1):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            dX.copy_(hX, non_blocking=True)
+            for a, b in zip(dU, hU):
+                a.copy_(b, non_blocking=True)
+        cd.cp_als(dX, dims, R, dU, max_sweeps=args.e2e_sweeps, tol=0.0, precision=prec, stream=sptr)
+        with torch.cuda.stream(stream):
+            for a, b in zip(oU, dU):
+                a.copy_(b, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if it > 0:
+            times.append(max(e0.elapsed_time(e1) * 1e-3, time.perf_counter() - t0))
+    e2e_s = sum(times) / len(times)
+    h2d = 4 * n + sum(4 * u.numel() for u in init)
+    d2h = sum(4 * u.numel() for u in init)
+    result["e2e"] = {"value": round(world * sweep_bytes(dims, R) * args.e2e_sweeps / e2e_s / 1e9, 3),
+                     "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                     "step": f"cud_cp_als, {args.e2e_sweeps} sweeps, from pinned host buffers",
+                     "seconds_per_step": round(e2e_s, 5)}
+
+    # ---- CPU baseline (rank 0, bounded sample)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        X3, cinit, sd = cpu_sample(dims, R, slab=args.cpu_slab)
+        gbs, dt = cpu_sweep_gbs(X3, cinit, 1)
+        result["cpu_baseline"] = {
+            "value": round(gbs, 3), "unit": "GB/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"one ALS sweep on a {sd[0]}x{sd[1]}x{sd[2]} slab (rank {R}), "
+                      f"{dt:.2f} s; NumPy/OpenBLAS restatement of decomposition/CPU/python/mycp.py"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

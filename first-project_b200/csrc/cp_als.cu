@@ -1,0 +1,353 @@
+// CP-ALS driver: a reusable plan (workspace + captured per-sweep CUDA graph)
+// and the one-shot cud_cp_als built on it.
+//
+// One sweep = for each mode n: MTTKRP_n (native layout) -> V^-1 from the
+// Hadamard product of the other factors' FP64 Grams (Cholesky, pinv
+// fallback) -> U_n = M V^-1 -> Gram of U_n; then the fit from the identity
+// ||X - Xhat||^2 = ||X||^2 - 2 <M_N, U_N> + sum prod_m G_m.  The sweep is
+// captured once into a CUDA graph and replayed; the plan owns every buffer
+// the graph touches.  Mirrors the update order and equations of
+// src/cp_als.cu:44-119 and src/cp4_als.cu:198-307, without their per-sweep
+// allocations and device synchronisations.
+#include <vector>
+#include <curand.h>
+
+#include "kernels.cuh"
+#include "solve.cuh"
+
+using namespace cud;
+
+struct cud_cp_plan_s {
+    int order = 0;
+    long dims[kMaxOrder] = {0};
+    long R = 0;
+    const float *X = nullptr;
+    float *U[kMaxOrder] = {nullptr};
+    cud_cp_options opt;
+    int device = 0;
+    double normx2 = 0.0;
+    // device memory owned by the plan
+    char *mem = nullptr;
+    float *M = nullptr;
+    double *G = nullptr, *Vinv = nullptr, *work = nullptr, *fit = nullptr;
+    int *fallbacks = nullptr;
+    void *ws = nullptr;
+    double *hbuf = nullptr;  // pinned
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels_per_sweep = -1;
+};
+
+namespace {
+
+bool valid_dims(int order, const long *dims) {
+    if (order < 1 || order > kMaxOrder || !dims) return false;
+    for (int m = 0; m < order; m++)
+        if (dims[m] <= 0) return false;
+    return true;
+}
+
+int count_kernel_nodes(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return -1;
+    int k = 0;
+    for (size_t i = 0; i < n; i++) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
+
+int enqueue_sweep(cud_cp_plan_s *p, cudaStream_t s) {
+    int st;
+    const long R = p->R;
+    for (int n = 0; n < p->order; n++) {
+        st = mttkrp_run(p->X, p->order, p->dims, (const float *const *)p->U, n, R, p->M,
+                        p->opt.precision, p->ws, s);
+        if (st) return st;
+        NormalArgs na;
+        for (int m = 0; m < p->order; m++) na.G[m] = p->G + (size_t)m * R * R;
+        na.nG = p->order;
+        na.mode = n;
+        na.R = (int)R;
+        na.Vinv = p->Vinv;
+        na.work = p->work;
+        na.fallbacks = p->fallbacks;
+        if ((st = normal_inverse(na, s))) return st;
+        if ((st = apply_inverse(p->M, p->Vinv, p->dims[n], R, p->U[n], s))) return st;
+        if ((st = factor_gram(p->U[n], p->dims[n], R, p->G + (size_t)n * R * R, s))) return st;
+    }
+    FitArgs fa;
+    fa.M = p->M;
+    fa.U = p->U[p->order - 1];
+    fa.IR = p->dims[p->order - 1] * R;
+    for (int m = 0; m < p->order; m++) fa.G[m] = p->G + (size_t)m * R * R;
+    fa.nG = p->order;
+    fa.R = (int)R;
+    fa.normx2 = p->normx2;
+    fa.out = p->fit;
+    return fit_eval(fa, s);
+}
+
+// Capture needs a stream other than the legacy default one.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaStream_t user = nullptr;
+    bool own = false;
+    int open(cudaStream_t u) {
+        user = u;
+        if (u != nullptr && u != cudaStreamLegacy && u != cudaStreamPerThread) {
+            s = u;
+            return CUD_OK;
+        }
+        CUD_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        own = true;
+        cudaEvent_t ev;
+        CUD_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CUD_CHECK(cudaEventRecord(ev, u));
+        CUD_CHECK(cudaStreamWaitEvent(s, ev, 0));
+        cudaEventDestroy(ev);
+        return CUD_OK;
+    }
+    int close() {
+        if (!own || !s) return CUD_OK;
+        // later work on the caller's stream orders after ours
+        cudaEvent_t ev;
+        CUD_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CUD_CHECK(cudaEventRecord(ev, s));
+        CUD_CHECK(cudaStreamWaitEvent(user, ev, 0));
+        cudaEventDestroy(ev);
+        cudaStreamDestroy(s);
+        s = nullptr;
+        return CUD_OK;
+    }
+};
+
+}  // namespace
+
+extern "C" void cud_cp_default_options(cud_cp_options *opt) {
+    if (!opt) return;
+    opt->max_sweeps = 500;
+    opt->tol = 0.0;
+    opt->precision = CUD_PREC_DEFAULT;
+    opt->use_graph = 1;
+    opt->check_every = 1;
+}
+
+extern "C" int cud_cp_init_curand(int order, const long *dims, long R, float *const *U,
+                                  unsigned long long seed, void *stream) {
+    if (!valid_dims(order, dims) || R <= 0 || !U) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    curandGenerator_t gen;
+    if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS)
+        return set_status(CUD_ERR_CUDA);
+    int st = CUD_OK;
+    if (curandSetStream(gen, as_stream(stream)) != CURAND_STATUS_SUCCESS ||
+        curandSetPseudoRandomGeneratorSeed(gen, seed) != CURAND_STATUS_SUCCESS)
+        st = CUD_ERR_CUDA;
+    for (int m = 1; m < order && st == CUD_OK; m++) {
+        if (!U[m]) { st = CUD_ERR_INVALID_ARGUMENT; break; }
+        if (curandGenerateUniform(gen, U[m], (size_t)(dims[m] * R)) != CURAND_STATUS_SUCCESS)
+            st = CUD_ERR_CUDA;
+    }
+    curandDestroyGenerator(gen);
+    return set_status(st);
+}
+
+extern "C" int cud_cp_plan_destroy(cud_cp_plan p) {
+    if (!p) return set_status(CUD_OK);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->mem) cudaFree(p->mem);
+    if (p->hbuf) cudaFreeHost(p->hbuf);
+    if (prev >= 0) cudaSetDevice(prev);
+    delete p;
+    return set_status(CUD_OK);
+}
+
+extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, long R,
+                                  float *const *U, const cud_cp_options *opt_in, void *stream,
+                                  cud_cp_plan *out) {
+    if (!out) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    *out = nullptr;
+    if (!valid_dims(order, dims) || order < 2 || R <= 0 || !X || !U) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    for (int m = 0; m < order; m++)
+        if (!U[m]) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    if (R > 160) return set_status(CUD_ERR_UNSUPPORTED);
+    cud_cp_options opt;
+    cud_cp_default_options(&opt);
+    if (opt_in) opt = *opt_in;
+    if (opt.max_sweeps < 0 || opt.check_every < 0 || opt.precision < 0 || opt.precision > CUD_PREC_DEFAULT)
+        return set_status(CUD_ERR_INVALID_ARGUMENT);
+    if (opt.check_every == 0) opt.check_every = 1;
+
+    cud_cp_plan_s *p = new cud_cp_plan_s();
+    p->order = order;
+    p->R = R;
+    p->X = X;
+    p->opt = opt;
+    cudaGetDevice(&p->device);
+    long maxd = 0, total = 1;
+    size_t wsb = 0;
+    for (int m = 0; m < order; m++) {
+        p->dims[m] = dims[m];
+        p->U[m] = U[m];
+        maxd = std::max(maxd, dims[m]);
+        total *= dims[m];
+    }
+    for (int m = 0; m < order; m++) wsb = std::max(wsb, mttkrp_ws_bytes(order, dims, m, R, opt.precision));
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t off_M = 0;
+    size_t off_G = off_M + up(sizeof(float) * maxd * R);
+    size_t off_V = off_G + up(sizeof(double) * order * R * R);
+    size_t off_W = off_V + up(sizeof(double) * R * R);
+    size_t off_F = off_W + up(sizeof(double) * 2 * R * R);
+    size_t off_C = off_F + up(sizeof(double) * 4);
+    size_t off_S = off_C + 256;
+    size_t bytes = off_S + up(wsb);
+    cudaError_t e = cudaMalloc((void **)&p->mem, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cud_cp_plan_destroy(p);
+        return set_status(cuda_status(e, "cud_cp_plan_create cudaMalloc"));
+    }
+    if (cudaMallocHost((void **)&p->hbuf, 8 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        cud_cp_plan_destroy(p);
+        return set_status(CUD_ERR_NO_MEMORY);
+    }
+    p->M = (float *)(p->mem + off_M);
+    p->G = (double *)(p->mem + off_G);
+    p->Vinv = (double *)(p->mem + off_V);
+    p->work = (double *)(p->mem + off_W);
+    p->fit = (double *)(p->mem + off_F);
+    p->fallbacks = (int *)(p->mem + off_C);
+    p->ws = p->mem + off_S;
+
+    SideStream ss;
+    int st = ss.open(as_stream(stream));
+    if (st == CUD_OK) {
+        double o[2];
+        st = residual_norms(X, nullptr, total, 0, o, ss.s);
+        p->normx2 = o[1];
+    }
+    if (st == CUD_OK && cudaMemsetAsync(p->fit, 0, sizeof(double) * 4 + 256, ss.s) != cudaSuccess)
+        st = CUD_ERR_CUDA;
+    for (int m = 0; m < order && st == CUD_OK; m++)
+        st = factor_gram(U[m], dims[m], R, p->G + (size_t)m * R * R, ss.s);
+    if (st == CUD_OK) st = normal_inverse_prepare();
+    if (st == CUD_OK && opt.use_graph) {
+        if (cudaStreamBeginCapture(ss.s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            st = CUD_ERR_CUDA;
+        } else {
+            int cst = enqueue_sweep(p, ss.s);
+            e = cudaStreamEndCapture(ss.s, &p->graph);
+            if (cst) st = cst;
+            else if (e != cudaSuccess) st = cuda_status(e, "cp plan capture");
+            else {
+                e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+                if (e != cudaSuccess) st = cuda_status(e, "cp plan instantiate");
+                else p->kernels_per_sweep = count_kernel_nodes(p->graph);
+            }
+        }
+    }
+    if (st == CUD_OK && cudaStreamSynchronize(ss.s) != cudaSuccess) st = CUD_ERR_CUDA;
+    ss.close();
+    if (st != CUD_OK) {
+        cud_cp_plan_destroy(p);
+        return set_status(st);
+    }
+    *out = p;
+    return set_status(CUD_OK);
+}
+
+extern "C" int cud_cp_plan_run(cud_cp_plan p, int sweeps, void *stream) {
+    if (!p || sweeps < 0) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cudaStream_t s = as_stream(stream);
+    for (int i = 0; i < sweeps; i++) {
+        if (p->exec) {
+            CUD_CHECK(cudaGraphLaunch(p->exec, s));
+        } else {
+            int st = enqueue_sweep(p, s);
+            if (st) return set_status(st);
+        }
+    }
+    return set_status(CUD_OK);
+}
+
+extern "C" int cud_cp_plan_fit(cud_cp_plan p, double *fit, double *fit_prev, void *stream) {
+    if (!p) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cudaStream_t s = as_stream(stream);
+    CUD_CHECK(cudaMemcpyAsync(p->hbuf, p->fit, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUD_CHECK(cudaMemcpyAsync(p->hbuf + 2, p->fallbacks, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUD_CHECK(cudaStreamSynchronize(s));
+    if (fit) *fit = p->hbuf[0];
+    if (fit_prev) *fit_prev = p->hbuf[1];
+    return set_status(CUD_OK);
+}
+
+extern "C" int cud_cp_plan_info(cud_cp_plan p, int *kernels_per_sweep, int *fallbacks) {
+    if (!p) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    if (kernels_per_sweep) *kernels_per_sweep = p->kernels_per_sweep;
+    if (fallbacks) {
+        int v = 0;
+        CUD_CHECK(cudaMemcpy(&v, p->fallbacks, sizeof(int), cudaMemcpyDeviceToHost));
+        *fallbacks = v;
+    }
+    return set_status(CUD_OK);
+}
+
+extern "C" int cud_cp_als(const float *X, int order, const long *dims, long R, float *const *U,
+                          const cud_cp_options *opt_in, cud_cp_result *res, void *stream) {
+    cud_cp_options opt;
+    cud_cp_default_options(&opt);
+    if (opt_in) opt = *opt_in;
+    cud_cp_plan p = nullptr;
+    int st = cud_cp_plan_create(X, order, dims, R, U, &opt, stream, &p);
+    if (st) return set_status(st);
+    SideStream ss;
+    st = ss.open(as_stream(stream));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    int sweeps = 0;
+    double fit = 0.0, fit_prev = 0.0;
+    if (st == CUD_OK) {
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, ss.s);
+        int chunk = (opt.tol > 0) ? opt.check_every : opt.max_sweeps;
+        if (chunk <= 0) chunk = 1;
+        while (sweeps < opt.max_sweeps && st == CUD_OK) {
+            int n = std::min(chunk, opt.max_sweeps - sweeps);
+            st = cud_cp_plan_run(p, n, ss.s);
+            sweeps += n;
+            if (st == CUD_OK && opt.tol > 0) {
+                st = cud_cp_plan_fit(p, &fit, &fit_prev, ss.s);
+                if (st == CUD_OK && sweeps >= 2 && fabs(fit - fit_prev) < opt.tol) break;
+            }
+        }
+        cudaEventRecord(t1, ss.s);
+        if (st == CUD_OK) st = cud_cp_plan_fit(p, &fit, &fit_prev, ss.s);
+    }
+    if (st == CUD_OK && res) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        res->sweeps = sweeps;
+        res->fit = fit;
+        res->fit_prev = fit_prev;
+        res->seconds = ms * 1e-3;
+        cud_cp_plan_info(p, &res->kernels_per_sweep, &res->fallbacks);
+    }
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    ss.close();
+    cud_cp_plan_destroy(p);
+    if (st == CUD_OK) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_status(e, "cud_cp_als");
+    }
+    return set_status(st);
+}

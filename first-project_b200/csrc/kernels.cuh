@@ -1,0 +1,84 @@
+// Internal interfaces shared between the library's translation units.
+#pragma once
+
+#include "common.cuh"
+
+namespace cud {
+
+// General strided GEMM on CUDA cores (FP32 FMA):
+//   C[b](m, n) = alpha * sum_{kin, kout} A(m, kin, kout) * B(kin, kout, n) + beta * C
+// with element strides for every index, so unfoldings, mode products and
+// unfolding Grams of column-major tensors are expressed without copies.
+// `kout` is a second contraction index (it lets a contraction run over two
+// non-adjacent tensor modes).  With out_f64 set, C is double and the partial
+// sums over `splits` chunks of the contraction are reduced in FP64.
+struct GemmDesc {
+    long M = 0, N = 0, Kin = 1, Kout = 1, batch = 1;
+    const float *A = nullptr;
+    long a_m = 0, a_kin = 0, a_kout = 0, a_b = 0;
+    const float *B = nullptr;
+    long b_kin = 0, b_kout = 0, b_n = 0, b_b = 0;
+    void *C = nullptr;
+    long c_m = 0, c_n = 0, c_b = 0;
+    float alpha = 1.0f, beta = 0.0f;
+    bool out_f64 = false;
+    int splits = 0;  // 0 = choose
+};
+int gemm_simt(const GemmDesc &d, cudaStream_t s);
+
+// Residual/norm helper (elementwise.cu).  Synchronises the stream.
+int residual_norms(const float *X, float *X1, long n, int subtract, double *out, cudaStream_t s);
+
+// Tensor views used by the contraction kernels: a column-major tensor seen as
+// (P, Q, S) around mode n -- P = prod of the dims before n, Q = dims[n],
+// S = prod of the dims after n.
+struct ModeView {
+    long P = 1, Q = 1, S = 1;
+};
+inline ModeView mode_view(int order, const long *dims, int mode) {
+    ModeView v;
+    for (int m = 0; m < mode; m++) v.P *= dims[m];
+    v.Q = dims[mode];
+    for (int m = mode + 1; m < order; m++) v.S *= dims[m];
+    return v;
+}
+
+constexpr int kMaxOrder = 8;
+
+// Factor set for on-the-fly Khatri-Rao rows: up to kMaxOrder-1 factor
+// matrices (column-major rows x R) listed fastest-first.
+struct KrFactors {
+    int n = 0;
+    const float *U[kMaxOrder];
+    long rows[kMaxOrder];
+};
+
+// MTTKRP kernels take an explicit device workspace (split-contraction
+// partials), so a captured CUDA graph can own its memory.
+//
+// CUDA-core path (mttkrp_simt.cu): FP32 FMA; with round = 1 (FP16) or 2
+// (BF16) the operands -- X and each formed KR row -- are rounded first.
+size_t mttkrp_simt_ws_bytes(int order, const long *dims, int mode, long R, int round);
+int mttkrp_simt_rounded(const float *X, int order, const long *dims, const float *const *U,
+                        int mode, long R, float *out, int round, void *ws, cudaStream_t s);
+// Tensor-core path (mttkrp_tc.cu): CUD_OK and the workspace size when it
+// applies to this shape/precision, CUD_ERR_UNSUPPORTED otherwise.
+int mttkrp_tc_query(int order, const long *dims, int mode, long R, int precision, size_t *ws_bytes);
+int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U, int mode,
+              long R, float *out, int precision, void *ws, cudaStream_t s);
+// Dispatcher (mttkrp.cu): tensor cores when they apply, else CUDA cores.
+size_t mttkrp_ws_bytes(int order, const long *dims, int mode, long R, int precision);
+int mttkrp_run(const float *X, int order, const long *dims, const float *const *U, int mode,
+               long R, float *out, int precision, void *ws, cudaStream_t s);
+
+// Mode product Y = X x_mode W (contract.cu); W is J x dims[mode], or its
+// transpose when w_trans is set.
+int mode_product(const float *X, int order, const long *dims, int mode, const float *W, long J,
+                 float *Y, cudaStream_t s, bool w_trans = false);
+// G (dims[mode]^2, FP64) = X_(mode) X_(mode)^T
+int unfold_gram(const float *X, int order, const long *dims, int mode, double *G, cudaStream_t s);
+
+// Symmetric eigensolver (eig.cu): A (n x n, FP64, destroyed) -> ascending W, V.
+int syev_jacobi(double *A, long n, double *W, double *V, int max_sweeps, cudaStream_t s);
+
+}  // namespace cud

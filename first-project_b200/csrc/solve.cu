@@ -1,0 +1,293 @@
+// The R x R side of CP-ALS, all in FP64 on the device: factor Grams, the
+// Hadamard product of Grams, Cholesky factorisation and inverse with a
+// pseudo-inverse (Jacobi eigen) fallback, the factor update U_n = M V^-1, and
+// the fit from the Gram/MTTKRP identity.  Replaces the FP32 getrf/getrs +
+// geam sequence of src/cp_als.cu:53-63 (and :73-82, :92-101).
+#include "kernels.cuh"
+#include "solve.cuh"
+
+namespace cud {
+
+namespace {
+
+// G = U^T U (R x R, FP64) for U (I x R, FP32).  16x16 output tile per CTA,
+// rows staged through shared memory in chunks of 64.
+__global__ void __launch_bounds__(256) k_factor_gram(const float *__restrict__ U, long I, long R,
+                                                     double *__restrict__ G) {
+    __shared__ double sa[64][17];
+    __shared__ double sb[64][17];
+    long a0 = blockIdx.x * 16L, b0 = blockIdx.y * 16L;
+    int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc = 0.0;
+    for (long i0 = 0; i0 < I; i0 += 64) {
+        for (int e = threadIdx.x; e < 64 * 16; e += 256) {
+            int ii = e & 63, cc = e >> 6;
+            long i = i0 + ii;
+            sa[ii][cc] = (i < I && a0 + cc < R) ? (double)U[i + I * (a0 + cc)] : 0.0;
+            sb[ii][cc] = (i < I && b0 + cc < R) ? (double)U[i + I * (b0 + cc)] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int ii = 0; ii < 64; ii++) acc = fma(sa[ii][tx], sb[ii][ty], acc);
+        __syncthreads();
+    }
+    long a = a0 + tx, b = b0 + ty;
+    if (a < R && b < R) G[a + R * b] = acc;
+}
+
+// Cyclic Jacobi on the symmetric n x n matrix held in shared memory (A), with
+// eigenvectors accumulated in Q (global).  One CTA; rotations of disjoint
+// (p, q) pairs run in parallel in round-robin order.  Returns sweeps used.
+__device__ int block_jacobi_smem(double *A, double *Q, int n, int max_sweeps, double tol) {
+    __shared__ double s_cos[128], s_sin[128];
+    __shared__ int s_p[128], s_q[128];
+    __shared__ double s_off;
+    int m = (n + 1) & ~1;  // even number of players (a dummy when n is odd)
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) Q[e] = (e % n == e / n) ? 1.0 : 0.0;
+    __syncthreads();
+    int sweep;
+    for (sweep = 0; sweep < max_sweeps; sweep++) {
+        if (threadIdx.x == 0) {
+            double off = 0.0, dia = 0.0;
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    double v = A[i + n * j] * A[i + n * j];
+                    if (i == j) dia += v; else off += v;
+                }
+            s_off = (off <= tol * tol * (dia + off)) ? -1.0 : off;
+        }
+        __syncthreads();
+        if (s_off < 0) break;
+        for (int round = 0; round < m - 1; round++) {
+            // round-robin pairing: player 0 fixed, others rotate
+            for (int k = threadIdx.x; k < m / 2; k += blockDim.x) {
+                int a = (k == 0) ? 0 : 1 + (k - 1 + round) % (m - 1);
+                int b = 1 + (m - 2 - k + round) % (m - 1);
+                int p = min(a, b), q = max(a, b);
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    double apq = A[p + n * q];
+                    if (apq != 0.0) {
+                        double app = A[p + n * p], aqq = A[q + n * q];
+                        double theta = (aqq - app) / (2.0 * apq);
+                        double tt = (theta >= 0 ? 1.0 : -1.0) /
+                                    (fabs(theta) + sqrt(theta * theta + 1.0));
+                        c = 1.0 / sqrt(tt * tt + 1.0);
+                        s = tt * c;
+                    }
+                }
+                s_p[k] = p; s_q[k] = q; s_cos[k] = c; s_sin[k] = s;
+            }
+            __syncthreads();
+            // rows: A <- J^T A
+            for (int e = threadIdx.x; e < (m / 2) * n; e += blockDim.x) {
+                int k = e / n, col = e % n;
+                int p = s_p[k], q = s_q[k];
+                if (q >= n) continue;
+                double c = s_cos[k], s = s_sin[k];
+                double ap = A[p + n * col], aq = A[q + n * col];
+                A[p + n * col] = c * ap - s * aq;
+                A[q + n * col] = s * ap + c * aq;
+            }
+            __syncthreads();
+            // columns: A <- A J, Q <- Q J
+            for (int e = threadIdx.x; e < (m / 2) * n; e += blockDim.x) {
+                int k = e / n, row = e % n;
+                int p = s_p[k], q = s_q[k];
+                if (q >= n) continue;
+                double c = s_cos[k], s = s_sin[k];
+                double ap = A[row + n * p], aq = A[row + n * q];
+                A[row + n * p] = c * ap - s * aq;
+                A[row + n * q] = s * ap + c * aq;
+                double vp = Q[row + n * p], vq = Q[row + n * q];
+                Q[row + n * p] = c * vp - s * vq;
+                Q[row + n * q] = s * vp + c * vq;
+            }
+            __syncthreads();
+        }
+    }
+    return sweep;
+}
+
+// V = Hadamard of the Grams of all factors except `mode`; Vinv = V^-1 by
+// Cholesky (V = L L^T, Vinv = L^-T L^-1), or, when a pivot is not positive,
+// the pseudo-inverse from a Jacobi eigendecomposition.  One CTA, V in
+// dynamic shared memory.  `work` is global scratch of 2 R^2 doubles.
+__global__ void __launch_bounds__(512) k_normal_inverse(NormalArgs a) {
+    extern __shared__ double V[];  // R x R
+    __shared__ int s_fail;
+    const int R = a.R;
+    for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+        double v = 1.0;
+        for (int m = 0; m < a.nG; m++)
+            if (m != a.mode) v *= a.G[m][e];
+        V[e] = v;
+    }
+    if (threadIdx.x == 0) s_fail = 0;
+    __syncthreads();
+    // right-looking Cholesky, lower triangle
+    double maxdiag = 0.0;
+    for (int j = 0; j < R; j++) maxdiag = fmax(maxdiag, fabs(V[j + R * j]));
+    for (int j = 0; j < R; j++) {
+        double d = V[j + R * j];
+        if (!(d > 1e-13 * maxdiag) || !isfinite(d)) {
+            if (threadIdx.x == 0) s_fail = 1;
+            break;
+        }
+        d = sqrt(d);
+        __syncthreads();
+        if (threadIdx.x == 0) V[j + R * j] = d;
+        for (int i = j + 1 + threadIdx.x; i < R; i += blockDim.x) V[i + R * j] /= d;
+        __syncthreads();
+        int w = R - j - 1;
+        for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+            int i = j + 1 + e % w, k = j + 1 + e / w;
+            if (k <= i) V[i + R * k] -= V[i + R * j] * V[k + R * j];
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    double *Linv = a.work;        // R x R
+    double *Q = a.work + R * R;   // R x R (pinv path)
+    if (!s_fail) {
+        // Linv = L^-1 (lower), one column per thread
+        for (int c = threadIdx.x; c < R; c += blockDim.x) {
+            for (int i = 0; i < R; i++) Linv[i + R * c] = 0.0;
+            for (int i = c; i < R; i++) {
+                double s = (i == c) ? 1.0 : 0.0;
+                for (int k = c; k < i; k++) s -= V[i + R * k] * Linv[k + R * c];
+                Linv[i + R * c] = s / V[i + R * i];
+            }
+        }
+        __syncthreads();
+        // Vinv = Linv^T Linv
+        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+            int i = e % R, j = e / R;
+            int k0 = max(i, j);
+            double s = 0.0;
+            for (int k = k0; k < R; k++) s += Linv[k + R * i] * Linv[k + R * j];
+            a.Vinv[e] = s;
+        }
+    } else {
+        // pseudo-inverse: rebuild V, eigendecompose, invert eigenvalues above tol
+        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+            double v = 1.0;
+            for (int m = 0; m < a.nG; m++)
+                if (m != a.mode) v *= a.G[m][e];
+            V[e] = v;
+        }
+        __syncthreads();
+        block_jacobi_smem(V, Q, R, 60, 1e-15);
+        __syncthreads();
+        double lmax = 0.0;
+        for (int j = 0; j < R; j++) lmax = fmax(lmax, fabs(V[j + R * j]));
+        double cut = lmax * (double)R * 2.2e-16;
+        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+            int i = e % R, j = e / R;
+            double s = 0.0;
+            for (int k = 0; k < R; k++) {
+                double l = V[k + R * k];
+                if (l > cut) s += Q[i + R * k] * Q[j + R * k] / l;
+            }
+            a.Vinv[e] = s;
+        }
+        if (threadIdx.x == 0 && a.fallbacks) atomicAdd(a.fallbacks, 1);
+    }
+}
+
+// U (I x R, FP32) = M (I x R, FP32) * Vinv (R x R, FP64), FP64 accumulation.
+__global__ void __launch_bounds__(256) k_apply_inverse(const float *__restrict__ M,
+                                                       const double *__restrict__ Vinv, long I,
+                                                       long R, float *__restrict__ U) {
+    extern __shared__ double sV[];  // R x R when it fits, else read from global
+    const bool in_smem = (R <= 64);
+    if (in_smem) {
+        for (long e = threadIdx.x; e < R * R; e += blockDim.x) sV[e] = Vinv[e];
+        __syncthreads();
+    }
+    const double *Vp = in_smem ? sV : Vinv;
+    long n = I * R;
+    long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long stride = (long)gridDim.x * blockDim.x;
+    for (long e = tid; e < n; e += stride) {
+        long i = e % I, c = e / I;
+        double s = 0.0;
+        for (long r = 0; r < R; r++) s = fma((double)M[i + I * r], Vp[r + R * c], s);
+        U[e] = (float)s;
+    }
+}
+
+// fit = 1 - sqrt(max(||X||^2 - 2<M, U> + sum_{r,s} prod_m G_m[r,s], 0)) / ||X||
+__global__ void __launch_bounds__(256) k_fit(FitArgs a) {
+    __shared__ double sh[2][8];
+    double inner = 0.0, hat = 0.0;
+    for (long e = threadIdx.x; e < a.IR; e += blockDim.x) inner += (double)a.M[e] * (double)a.U[e];
+    for (long e = threadIdx.x; e < (long)a.R * a.R; e += blockDim.x) {
+        double p = 1.0;
+        for (int m = 0; m < a.nG; m++) p *= a.G[m][e];
+        hat += p;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        inner += __shfl_xor_sync(0xffffffffu, inner, o);
+        hat += __shfl_xor_sync(0xffffffffu, hat, o);
+    }
+    int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sh[0][w] = inner; sh[1][w] = hat; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double in = 0.0, h = 0.0;
+        for (int i = 0; i < 8; i++) { in += sh[0][i]; h += sh[1][i]; }
+        double res2 = a.normx2 - 2.0 * in + h;
+        double fit = 1.0 - sqrt(res2 > 0.0 ? res2 : 0.0) / sqrt(a.normx2);
+        a.out[1] = a.out[0];  // previous fit
+        a.out[0] = fit;
+        a.out[2] = in;
+        a.out[3] = h;
+    }
+}
+
+}  // namespace
+
+int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s) {
+    dim3 grid((unsigned)((R + 15) / 16), (unsigned)((R + 15) / 16));
+    k_factor_gram<<<grid, 256, 0, s>>>(U, I, R, G);
+    CUD_CHECK_LAUNCH("factor_gram");
+    return CUD_OK;
+}
+
+int normal_inverse_prepare() {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    CUD_CHECK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        CUD_CHECK(cudaFuncSetAttribute(k_normal_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double) * 160 * 160)));
+        attr_set[dev] = true;
+    }
+    return CUD_OK;
+}
+
+int normal_inverse(const NormalArgs &a, cudaStream_t s) {
+    size_t smem = sizeof(double) * (size_t)a.R * a.R;
+    if (a.R > 160) return CUD_ERR_UNSUPPORTED;
+    int st = normal_inverse_prepare();
+    if (st) return st;
+    k_normal_inverse<<<1, 512, smem, s>>>(a);
+    CUD_CHECK_LAUNCH("normal_inverse");
+    return CUD_OK;
+}
+
+int apply_inverse(const float *M, const double *Vinv, long I, long R, float *U, cudaStream_t s) {
+    size_t smem = (R <= 64) ? sizeof(double) * R * R : 0;
+    k_apply_inverse<<<blocks_for(I * R, 256, 148L * 4), 256, smem, s>>>(M, Vinv, I, R, U);
+    CUD_CHECK_LAUNCH("apply_inverse");
+    return CUD_OK;
+}
+
+int fit_eval(const FitArgs &a, cudaStream_t s) {
+    k_fit<<<1, 256, 0, s>>>(a);
+    CUD_CHECK_LAUNCH("fit_eval");
+    return CUD_OK;
+}
+
+}  // namespace cud

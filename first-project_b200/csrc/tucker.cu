@@ -1,0 +1,161 @@
+// Tucker decompositions: HOSVD (src/tucker_hosvd.cu:3-103,
+// src/tucker4_hosvd.cu:3-141) and HOOI
+// (decomposition/GPU/normal/tucker/tucker_hooi.cu:3-218), any order.
+//
+// Factor n = eigenvectors of the r_n largest eigenvalues of the FP64
+// unfolding Gram, taken as the last r_n columns of the ascending
+// eigendecomposition (the reference copies d_Xn_Xn + (I_n - r_n) I_n).
+// The core is the chain X x_1 U_1^T x_2 U_2^T ... in mode order.
+#include "kernels.cuh"
+
+namespace cud {
+
+namespace {
+
+__global__ void k_take_top(const double *__restrict__ V, long n, long r, float *__restrict__ U) {
+    long total = n * r;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        long i = e % n, j = e / n;
+        U[e] = (float)V[i + n * (n - r + j)];
+    }
+}
+
+struct TuckerWork {
+    double *G = nullptr, *W = nullptr, *V = nullptr;
+    float *buf0 = nullptr, *buf1 = nullptr;
+    size_t bufn = 0;
+};
+
+int alloc_work(int order, const long *dims, const long *ranks, TuckerWork &w) {
+    long maxd = 0;
+    for (int m = 0; m < order; m++) maxd = std::max(maxd, dims[m]);
+    // largest intermediate of any contraction chain: X with one mode reduced
+    size_t maxn = 0;
+    for (int m = 0; m < order; m++) {
+        size_t n = 1;
+        for (int q = 0; q < order; q++) n *= (q == m) ? ranks[q] : dims[q];
+        maxn = std::max(maxn, n);
+    }
+    size_t gbytes = sizeof(double) * (size_t)maxd * maxd;
+    size_t off_W = (gbytes + 255) & ~size_t(255);
+    size_t off_V = off_W + ((sizeof(double) * maxd + 255) & ~size_t(255));
+    size_t off_B = off_V + ((gbytes + 255) & ~size_t(255));
+    size_t bytes = off_B + sizeof(float) * maxn * 2 + 512;
+    int st;
+    char *p = (char *)scratch(kSlotTmp0, bytes, &st);
+    if (!p) return st;
+    w.G = (double *)p;
+    w.W = (double *)(p + off_W);
+    w.V = (double *)(p + off_V);
+    w.buf0 = (float *)(p + off_B);
+    w.buf1 = w.buf0 + maxn;
+    w.bufn = maxn;
+    return CUD_OK;
+}
+
+// U_out (I x r) = top-r eigenvectors of G (I x I, destroyed).
+int top_eigvecs(double *G, long I, long r, const TuckerWork &w, float *U, cudaStream_t s) {
+    int st = syev_jacobi(G, I, w.W, w.V, 60, s);
+    if (st != CUD_OK && st != CUD_ERR_NOT_CONVERGED) return st;
+    k_take_top<<<blocks_for(I * r, 256), 256, 0, s>>>(w.V, I, r, U);
+    CUD_CHECK_LAUNCH("top_eigvecs");
+    return st;
+}
+
+// Y = X x_{m in modes, m != skip} U_m^T, ascending mode order; result dims in
+// `cur`.  Uses the two work buffers; returns the pointer holding Y.
+int project_all_but(const float *X, int order, const long *dims, const long *ranks,
+                    float *const *U, int skip, const TuckerWork &w, long *cur, const float **Y,
+                    float *final_out, cudaStream_t s) {
+    for (int m = 0; m < order; m++) cur[m] = dims[m];
+    const float *src = X;
+    int nsteps = 0;
+    for (int m = 0; m < order; m++)
+        if (m != skip) nsteps++;
+    int step = 0;
+    for (int m = 0; m < order; m++) {
+        if (m == skip) continue;
+        step++;
+        float *dst = (step == nsteps && final_out) ? final_out : ((step & 1) ? w.buf0 : w.buf1);
+        int st = mode_product(src, order, cur, m, U[m], ranks[m], dst, s, true);
+        if (st) return st;
+        cur[m] = ranks[m];
+        src = dst;
+    }
+    *Y = src;
+    return CUD_OK;
+}
+
+bool valid(int order, const long *dims, const long *ranks, float *const *U, const float *X,
+           const float *core) {
+    if (order < 2 || order > kMaxOrder || !dims || !ranks || !U || !X || !core) return false;
+    for (int m = 0; m < order; m++)
+        if (dims[m] <= 0 || ranks[m] <= 0 || ranks[m] > dims[m] || !U[m]) return false;
+    return true;
+}
+
+}  // namespace
+
+}  // namespace cud
+
+using namespace cud;
+
+extern "C" int cud_tucker_hosvd(const float *X, int order, const long *dims, const long *ranks,
+                                float *core, float *const *U, int precision, void *stream) {
+    (void)precision;
+    if (!valid(order, dims, ranks, U, X, core)) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cudaStream_t s = as_stream(stream);
+    TuckerWork w;
+    int st = alloc_work(order, dims, ranks, w);
+    if (st) return set_status(st);
+    int worst = CUD_OK;
+    for (int n = 0; n < order; n++) {
+        if ((st = unfold_gram(X, order, dims, n, w.G, s))) return set_status(st);
+        st = top_eigvecs(w.G, dims[n], ranks[n], w, U[n], s);
+        if (st == CUD_ERR_NOT_CONVERGED) worst = st;
+        else if (st) return set_status(st);
+    }
+    long cur[kMaxOrder];
+    const float *Y;
+    if ((st = project_all_but(X, order, dims, ranks, U, -1, w, cur, &Y, core, s))) return set_status(st);
+    CUD_CHECK(cudaStreamSynchronize(s));
+    return set_status(worst);
+}
+
+extern "C" int cud_tucker_hooi(const float *X, int order, const long *dims, const long *ranks,
+                               float *core, float *const *U, int sweeps, int precision, void *stream) {
+    (void)precision;
+    if (!valid(order, dims, ranks, U, X, core) || sweeps < 0) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cudaStream_t s = as_stream(stream);
+    TuckerWork w;
+    int st = alloc_work(order, dims, ranks, w);
+    if (st) return set_status(st);
+    int worst = CUD_OK;
+    // initial U_2..U_N from the unfolding Grams (tucker_hooi.cu:45-75)
+    for (int n = 1; n < order; n++) {
+        if ((st = unfold_gram(X, order, dims, n, w.G, s))) return set_status(st);
+        st = top_eigvecs(w.G, dims[n], ranks[n], w, U[n], s);
+        if (st == CUD_ERR_NOT_CONVERGED) worst = st;
+        else if (st) return set_status(st);
+    }
+    long cur[kMaxOrder];
+    const float *Y;
+    for (int it = 0; it < sweeps; it++) {
+        for (int n = 0; n < order; n++) {
+            if ((st = project_all_but(X, order, dims, ranks, U, n, w, cur, &Y, nullptr, s))) return set_status(st);
+            if ((st = unfold_gram(Y, order, cur, n, w.G, s))) return set_status(st);
+            st = top_eigvecs(w.G, dims[n], ranks[n], w, U[n], s);
+            if (st == CUD_ERR_NOT_CONVERGED) worst = st;
+            else if (st) return set_status(st);
+        }
+    }
+    if (sweeps == 0) {
+        // no sweep: U_1 from its Gram as in HOSVD
+        if ((st = unfold_gram(X, order, dims, 0, w.G, s))) return set_status(st);
+        st = top_eigvecs(w.G, dims[0], ranks[0], w, U[0], s);
+        if (st && st != CUD_ERR_NOT_CONVERGED) return set_status(st);
+    }
+    if ((st = project_all_but(X, order, dims, ranks, U, -1, w, cur, &Y, core, s))) return set_status(st);
+    CUD_CHECK(cudaStreamSynchronize(s));
+    return set_status(worst);
+}

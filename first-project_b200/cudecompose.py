@@ -1,0 +1,400 @@
+"""Python mirror of the cudecompose API over the library's C ABI.
+
+The reference (891922758/first-project) is a cuBLAS-like C++ library
+(inc/cudecompose.h): every routine takes device pointers and extents.  This
+module exposes the same routines by the same names for PyTorch CUDA tensors
+(column-major data is passed as flat or Fortran-ordered tensors), calling the
+in-tree shared library `libcudecompose_b200.so` through ctypes.  There is no
+fallback: if the library is missing or fails to load, importing this module
+raises.
+
+Conventions: tensors are column-major (mode 1 fastest).  A torch tensor that
+represents an I x J x K tensor is stored as a flat float32 buffer of I*J*K
+elements laid out column-major; `colmajor(t)` / `from_colmajor(buf, shape)`
+convert between a logical torch tensor and that buffer.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcudecompose_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is not built; run `make -C first-project_b200` "
+        "(or __graft_entry__.build()) first")
+_lib = ctypes.CDLL(LIB_PATH)
+
+# status codes (include/cudecompose_c.h)
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_CUDA = 2
+ERR_NO_MEMORY = 3
+ERR_NOT_CONVERGED = 4
+ERR_UNSUPPORTED = 5
+ERR_SINGULAR = 6
+ERR_DEVICE_TIMEOUT = 7
+
+# precisions
+PREC_FP32 = 0
+PREC_BF16 = 1
+PREC_FP16 = 2
+PREC_BF16X3 = 3
+PREC_DEFAULT = 4
+PRECISIONS = {"fp32": PREC_FP32, "bf16": PREC_BF16, "fp16": PREC_FP16,
+              "bf16x3": PREC_BF16X3, "default": PREC_DEFAULT}
+
+_vp = ctypes.c_void_p
+_l = ctypes.c_long
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+
+class CpOptions(ctypes.Structure):
+    _fields_ = [("max_sweeps", _i), ("tol", _d), ("precision", _i),
+                ("use_graph", _i), ("check_every", _i)]
+
+
+class CpResult(ctypes.Structure):
+    _fields_ = [("sweeps", _i), ("fallbacks", _i), ("fit", _d),
+                ("fit_prev", _d), ("seconds", _d), ("kernels_per_sweep", _i)]
+
+
+def _sig(name, argtypes, restype=_i):
+    f = getattr(_lib, name)
+    f.argtypes = argtypes
+    f.restype = restype
+    return f
+
+
+_sig("cud_get_last_error", [])
+_sig("cud_status_string", [_i], ctypes.c_char_p)
+_sig("cud_last_error_detail", [], ctypes.c_char_p)
+_sig("cud_hadmard", [_vp, _vp, _vp, _l, _l, _vp])
+_sig("cud_hadmard3", [_vp, _vp, _vp, _vp, _l, _l, _vp])
+_sig("cud_elepro3", [_vp, _vp, _vp, _vp, _l, _vp])
+_sig("cud_kr", [_vp, _vp, _vp, _l, _l, _l, _vp])
+_sig("cud_tensor_product", [_vp, _vp, _vp, _l, _l, _l, _l, _vp])
+_sig("cud_f2h", [_vp, _vp, _l, _vp])
+_sig("cud_f2bf", [_vp, _vp, _l, _vp])
+_sig("cud_t2m", [_vp, _vp, _l, _l, _l, _l, _vp])
+_sig("cud_tminust", [_vp, _vp, _l, _vp])
+_sig("cud_init_identity", [_vp, _l, _vp])
+_sig("cud_rse", [_vp, _vp, _l, ctypes.POINTER(ctypes.c_float), _vp])
+_sig("cud_norm2", [_vp, _l, ctypes.POINTER(_d), _vp])
+_sig("cud_gencp", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _l, _vp])
+_sig("cud_gentucker", [_vp, _i, ctypes.POINTER(_l), _vp, ctypes.POINTER(_l),
+                       ctypes.POINTER(_vp), _vp])
+_sig("cud_ttm", [_vp, _vp, _vp, _l, _l, _l, _l, _l, _i, _vp])
+_sig("cud_mode_product", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _l, _vp, _i, _vp])
+_sig("cud_mttkrp_legacy", [_vp, _vp, _vp, _vp, _l, _l, _l, _l, _l, _i, _vp])
+_sig("cud_mttkrp", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _vp, _i, _vp])
+_sig("cud_unfold_gram", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _i, _vp])
+_sig("cud_syev_jacobi", [_vp, _l, _vp, _vp, _i, _vp])
+_sig("cud_cp_default_options", [ctypes.POINTER(CpOptions)], None)
+_sig("cud_cp_als", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
+                    ctypes.POINTER(CpOptions), ctypes.POINTER(CpResult), _vp])
+_sig("cud_cp_init_curand", [_i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
+                            ctypes.c_ulonglong, _vp])
+_sig("cud_cp_plan_create", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
+                            ctypes.POINTER(CpOptions), _vp, ctypes.POINTER(_vp)])
+_sig("cud_cp_plan_run", [_vp, _i, _vp])
+_sig("cud_cp_plan_fit", [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), _vp])
+_sig("cud_cp_plan_info", [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)])
+_sig("cud_cp_plan_destroy", [_vp])
+_sig("cud_tucker_hosvd", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp,
+                          ctypes.POINTER(_vp), _i, _vp])
+_sig("cud_tucker_hooi", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp,
+                         ctypes.POINTER(_vp), _i, _i, _vp])
+
+
+class CudError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = _lib.cud_status_string(status).decode()
+        detail = _lib.cud_last_error_detail().decode()
+        super().__init__(f"{where}: status {status} ({msg}) {detail}".strip())
+        self.status = status
+
+
+def library() -> ctypes.CDLL:
+    """The loaded shared library (for raw C-ABI calls)."""
+    return _lib
+
+
+def _check(st: int, where: str, allow=(OK,)):
+    if st not in allow:
+        raise CudError(st, where)
+    return st
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("device tensor required")
+    if not t.is_contiguous():
+        raise ValueError("contiguous tensor required")
+    return t.data_ptr()
+
+
+def _stream(stream=None) -> int | None:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream or None
+    return stream
+
+
+def _longs(xs: Sequence[int]):
+    return (_l * len(xs))(*[int(x) for x in xs])
+
+
+def _ptrs(ts: Sequence[torch.Tensor | None]):
+    return (_vp * len(ts))(*[_ptr(t) if t is not None else None for t in ts])
+
+
+# --------------------------------------------------------------------------
+# layout helpers
+# --------------------------------------------------------------------------
+
+def colmajor(t: torch.Tensor) -> torch.Tensor:
+    """Flat column-major float32 copy of a logical tensor/matrix."""
+    return t.float().permute(*reversed(range(t.dim()))).contiguous().reshape(-1)
+
+
+def from_colmajor(buf: torch.Tensor, shape: Sequence[int]) -> torch.Tensor:
+    """Logical tensor view of a flat column-major buffer."""
+    return buf.reshape(tuple(reversed(shape))).permute(*reversed(range(len(shape))))
+
+
+# --------------------------------------------------------------------------
+# reference-named routines (device tensors in, device tensors out)
+# --------------------------------------------------------------------------
+
+def hadmard(A, B, C, a, b, stream=None):
+    _check(_lib.cud_hadmard(_ptr(A), _ptr(B), _ptr(C), a, b, _stream(stream)), "hadmard")
+
+
+def hadmard3(A, B, C, D, a, b, stream=None):
+    _check(_lib.cud_hadmard3(_ptr(A), _ptr(B), _ptr(C), _ptr(D), a, b, _stream(stream)), "hadmard3")
+
+
+def elepro3(A, B, C, D, n, stream=None):
+    _check(_lib.cud_elepro3(_ptr(A), _ptr(B), _ptr(C), _ptr(D), n, _stream(stream)), "elepro3")
+
+
+def kr(A, B, AkrB, a, b, r, stream=None):
+    _check(_lib.cud_kr(_ptr(A), _ptr(B), _ptr(AkrB), a, b, r, _stream(stream)), "kr")
+
+
+def tensor_product(A, B, C, a, b, c, d, stream=None):
+    _check(_lib.cud_tensor_product(_ptr(A), _ptr(B), _ptr(C), a, b, c, d, _stream(stream)),
+           "tensor_product")
+
+
+def f2h(A, B, n, stream=None):
+    _check(_lib.cud_f2h(_ptr(A), _ptr(B), n, _stream(stream)), "f2h")
+
+
+def f2bf(A, B, n, stream=None):
+    _check(_lib.cud_f2bf(_ptr(A), _ptr(B), n, _stream(stream)), "f2bf")
+
+
+def t2m(T1, T2, flag, m, n, k, stream=None):
+    _check(_lib.cud_t2m(_ptr(T1), _ptr(T2), flag, m, n, k, _stream(stream)), "t2m")
+
+
+def tminust(M, N, m, stream=None):
+    _check(_lib.cud_tminust(_ptr(M), _ptr(N), m, _stream(stream)), "tminust")
+
+
+def initMat(A, m, stream=None):
+    _check(_lib.cud_init_identity(_ptr(A), m, _stream(stream)), "initMat")
+
+
+def rse(X, X1, m, stream=None) -> float:
+    err = ctypes.c_float(0.0)
+    _check(_lib.cud_rse(_ptr(X), _ptr(X1), m, ctypes.byref(err), _stream(stream)), "rse")
+    return err.value
+
+
+def norm2(x, n=None, stream=None) -> float:
+    out = _d(0.0)
+    n = x.numel() if n is None else n
+    _check(_lib.cud_norm2(_ptr(x), n, ctypes.byref(out), _stream(stream)), "norm2")
+    return out.value
+
+
+def gencp(rec, factors, dims, r, stream=None):
+    _check(_lib.cud_gencp(_ptr(rec), len(dims), _longs(dims), _ptrs(factors), r,
+                          _stream(stream)), "gencp")
+
+
+def gentucker(rec, core, factors, dims, ranks, stream=None):
+    _check(_lib.cud_gentucker(_ptr(rec), len(dims), _longs(dims), _ptr(core), _longs(ranks),
+                              _ptrs(factors), _stream(stream)), "gentucker")
+
+
+def ttm(X, U, XU, flag, a, b, c, d, precision=PREC_FP32, stream=None):
+    _check(_lib.cud_ttm(_ptr(X), _ptr(U), _ptr(XU), flag, a, b, c, d, precision,
+                        _stream(stream)), "ttm")
+
+
+def mode_product(X, dims, mode, W, J, Y, precision=PREC_FP32, stream=None):
+    _check(_lib.cud_mode_product(_ptr(X), len(dims), _longs(dims), mode, _ptr(W), J, _ptr(Y),
+                                 precision, _stream(stream)), "mode_product")
+
+
+def mttkrp_legacy(X, left, right, XU, flag, m, n, k, r, precision=PREC_FP16, stream=None):
+    _check(_lib.cud_mttkrp_legacy(_ptr(X), _ptr(left), _ptr(right), _ptr(XU), flag, m, n, k, r,
+                                  precision, _stream(stream)), "mttkrp_legacy")
+
+
+def mttkrp(X, dims, factors, mode, R, out, precision=PREC_DEFAULT, stream=None):
+    """out (dims[mode] x R, column-major) = X_(mode) (KR of the other factors)."""
+    _check(_lib.cud_mttkrp(_ptr(X), len(dims), _longs(dims), _ptrs(factors), mode, R,
+                           _ptr(out), precision, _stream(stream)), "mttkrp")
+
+
+def unfold_gram(X, dims, mode, G, stream=None):
+    _check(_lib.cud_unfold_gram(_ptr(X), len(dims), _longs(dims), mode, _ptr(G), 0,
+                                _stream(stream)), "unfold_gram")
+
+
+def syev_jacobi(A, n, W, V, max_sweeps=60, stream=None):
+    return _check(_lib.cud_syev_jacobi(_ptr(A), n, _ptr(W), _ptr(V), max_sweeps,
+                                       _stream(stream)), "syev_jacobi",
+                  allow=(OK, ERR_NOT_CONVERGED))
+
+
+def cp_default_options() -> CpOptions:
+    o = CpOptions()
+    _lib.cud_cp_default_options(ctypes.byref(o))
+    return o
+
+
+def cp_als(X, dims, R, factors, max_sweeps=500, tol=0.0, precision=PREC_DEFAULT,
+           use_graph=True, check_every=1, stream=None) -> CpResult:
+    """CP-ALS from the given initial factors (updated in place)."""
+    opt = CpOptions(max_sweeps, tol, precision, 1 if use_graph else 0, check_every)
+    res = CpResult()
+    _check(_lib.cud_cp_als(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
+                           ctypes.byref(opt), ctypes.byref(res), _stream(stream)), "cp_als")
+    return res
+
+
+class CpPlan:
+    """Reusable CP-ALS plan (cud_cp_plan_*): workspace plus the captured
+    per-sweep CUDA graph; `run(n)` enqueues n sweeps without synchronising."""
+
+    def __init__(self, X, dims, R, factors, precision=PREC_DEFAULT, use_graph=True, stream=None):
+        self._keep = (X, list(factors))
+        opt = CpOptions(0, 0.0, precision, 1 if use_graph else 0, 1)
+        h = _vp()
+        _check(_lib.cud_cp_plan_create(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
+                                       ctypes.byref(opt), _stream(stream), ctypes.byref(h)),
+               "cp_plan_create")
+        self._h = h
+
+    def run(self, sweeps=1, stream=None):
+        _check(_lib.cud_cp_plan_run(self._h, sweeps, _stream(stream)), "cp_plan_run")
+
+    def fit(self, stream=None):
+        f, fp = _d(0.0), _d(0.0)
+        _check(_lib.cud_cp_plan_fit(self._h, ctypes.byref(f), ctypes.byref(fp), _stream(stream)),
+               "cp_plan_fit")
+        return f.value, fp.value
+
+    def info(self):
+        k, fb = _i(0), _i(0)
+        _check(_lib.cud_cp_plan_info(self._h, ctypes.byref(k), ctypes.byref(fb)), "cp_plan_info")
+        return k.value, fb.value
+
+    def close(self):
+        if self._h:
+            _lib.cud_cp_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cp_init_curand(dims, R, factors, seed=1234, stream=None):
+    _check(_lib.cud_cp_init_curand(len(dims), _longs(dims), R, _ptrs(factors), seed,
+                                   _stream(stream)), "cp_init_curand")
+
+
+def tucker_hosvd(X, dims, ranks, core, factors, precision=PREC_FP32, stream=None):
+    return _check(_lib.cud_tucker_hosvd(_ptr(X), len(dims), _longs(dims), _longs(ranks),
+                                        _ptr(core), _ptrs(factors), precision, _stream(stream)),
+                  "tucker_hosvd", allow=(OK, ERR_NOT_CONVERGED))
+
+
+def tucker_hooi(X, dims, ranks, core, factors, sweeps=10, precision=PREC_FP32, stream=None):
+    return _check(_lib.cud_tucker_hooi(_ptr(X), len(dims), _longs(dims), _longs(ranks),
+                                       _ptr(core), _ptrs(factors), sweeps, precision,
+                                       _stream(stream)),
+                  "tucker_hooi", allow=(OK, ERR_NOT_CONVERGED))
+
+
+# --------------------------------------------------------------------------
+# seeded synthetic workloads (the shapes and value distributions of the
+# reference's benchmark configurations; generated on the device)
+# --------------------------------------------------------------------------
+
+def make_cp_tensor(dims, R, seed=0, noise=1e-3, device="cuda"):
+    """X = sum_r U1[:,r] o U2[:,r] o ... + noise, factors uniform [0,1), noise
+    i.i.d. Gaussian scaled to `noise` * ||X_clean||_F.  Returns the flat
+    column-major X and the list of true factors (dims[m] x R column-major)."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    facs = [torch.rand(int(R) * int(d), generator=g, device=device, dtype=torch.float32)
+            for d in dims]
+    n = 1
+    for d in dims:
+        n *= int(d)
+    X = torch.empty(n, device=device, dtype=torch.float32)
+    gencp(X, facs, dims, R)
+    if noise > 0:
+        nrm = norm2(X) ** 0.5
+        E = torch.randn(n, generator=g, device=device, dtype=torch.float32)
+        enrm = norm2(E) ** 0.5
+        X.add_(E, alpha=noise * nrm / enrm)
+    return X, facs
+
+
+def make_init(dims, R, seed=1, device="cuda"):
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    return [torch.rand(int(R) * int(d), generator=g, device=device, dtype=torch.float32)
+            for d in dims]
+
+
+def make_tucker_tensor(dims, ranks, seed=0, noise=1e-3, device="cuda"):
+    """X = G x_1 U1 x_2 U2 ... + noise; G i.i.d. N(0,1), U_n orthonormal
+    columns (QR of a seeded Gaussian)."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    core = torch.randn(int(torch.tensor(ranks).prod()), generator=g, device=device)
+    facs = []
+    for d, r in zip(dims, ranks):
+        Z = torch.randn(int(d), int(r), generator=g, device=device, dtype=torch.float64)
+        Q, _ = torch.linalg.qr(Z)
+        facs.append(colmajor(Q.float()))
+    n = 1
+    for d in dims:
+        n *= int(d)
+    X = torch.empty(n, device=device, dtype=torch.float32)
+    gentucker(X, core, facs, dims, ranks)
+    if noise > 0:
+        nrm = norm2(X) ** 0.5
+        E = torch.randn(n, generator=g, device=device, dtype=torch.float32)
+        enrm = norm2(E) ** 0.5
+        X.add_(E, alpha=noise * nrm / enrm)
+    return X, core, facs

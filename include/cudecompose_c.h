@@ -1,0 +1,219 @@
+/*
+ * cudecompose_c.h -- C ABI of the B200-native dense CP/Tucker library.
+ *
+ * Every entry point takes plain pointers and sizes: device pointers for
+ * tensors and matrices (column-major, mode 1 fastest; factor matrices are
+ * I_n x R column-major), `long` extents, and an optional CUDA stream passed as
+ * `void *` (NULL = the legacy default stream).  Each returns a cud_status and
+ * also records it as the calling thread's last status (cud_get_last_error),
+ * the side channel the void-returning drop-in functions of cudecompose.h use.
+ *
+ * The comment above each declaration names the reference interface it
+ * replaces (891922758/first-project, file:line).  Entry points marked
+ * "extension" have no reference counterpart.
+ */
+#ifndef CUDECOMPOSE_C_H_
+#define CUDECOMPOSE_C_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ----------------------------------------------------------- */
+
+typedef enum cud_status {
+    CUD_OK = 0,
+    CUD_ERR_INVALID_ARGUMENT = 1, /* bad flag/mode, null pointer, bad extent  */
+    CUD_ERR_CUDA = 2,             /* a CUDA runtime call failed                */
+    CUD_ERR_NO_MEMORY = 3,        /* device workspace allocation failed        */
+    CUD_ERR_NOT_CONVERGED = 4,    /* an iterative solver hit its sweep limit   */
+    CUD_ERR_UNSUPPORTED = 5,      /* shape/precision combination not built     */
+    CUD_ERR_SINGULAR = 6,         /* normal equations fell back to pinv        */
+    CUD_ERR_DEVICE_TIMEOUT = 7    /* a bounded device-side wait gave up        */
+} cud_status;
+
+/* MTTKRP / TTM / Gram arithmetic. */
+typedef enum cud_precision {
+    CUD_PREC_FP32 = 0,   /* FP32 FMA on CUDA cores (plain FP32)                 */
+    CUD_PREC_BF16 = 1,   /* BF16 operands, FP32 accumulate, tensor cores        */
+    CUD_PREC_FP16 = 2,   /* FP16 operands, FP32 accumulate, tensor cores        */
+    CUD_PREC_BF16X3 = 3, /* hi/lo BF16 split, 3 products, FP32-level accuracy   */
+    CUD_PREC_DEFAULT = 4 /* BF16X3 where the tensor-core path applies, else FP32 */
+} cud_precision;
+
+/* Extension: the calling thread's last status (cudecomposeGetLastError). */
+int cud_get_last_error(void);
+/* Extension: a static message for a status code. */
+const char *cud_status_string(int status);
+/* Extension: the detail text (CUDA error name, failing call) of the thread's
+ * last non-OK status, or "" */
+const char *cud_last_error_detail(void);
+
+/* ---- element-wise and permutation primitives -------------------------- */
+
+/* inc/cudecompose.h:23, src/hadmard.cu:10-15: C = A .* B over a*b elements. */
+int cud_hadmard(const float *A, const float *B, float *C, long a, long b, void *stream);
+
+/* inc/cudecompose.h:50, src/hadmard.cu:25-30: D = A .* B .* C. */
+int cud_hadmard3(const float *A, const float *B, const float *C, float *D, long a, long b,
+                 void *stream);
+
+/* inc/cudecompose.h:55, src/kernel.cu:3-9 elepro3: D = A .* B .* C over n. */
+int cud_elepro3(const float *A, const float *B, const float *C, float *D, long n, void *stream);
+
+/* inc/cudecompose.h:24, src/kr.cu:3-11: Khatri-Rao, out (a*b) x r with
+ * out[x + y*b + t*a*b] = B[x,t]*A[y,t]. */
+int cud_kr(const float *A, const float *B, float *AkrB, long a, long b, long r, void *stream);
+
+/* inc/cudecompose.h:25, src/tensorproduct.cu:4-14: Kronecker product,
+ * C (a*c) x (b*d) = A (a x b) (x) B (c x d). */
+int cud_tensor_product(const float *A, const float *B, float *C, long a, long b, long c,
+                       long d, void *stream);
+
+/* inc/cudecompose.h:28, src/float2half.cu:14-18: FP32 -> FP16 (RN). */
+int cud_f2h(const float *A, void *B_half, long n, void *stream);
+
+/* Extension: FP32 -> BF16 (RN). */
+int cud_f2bf(const float *A, void *B_bf16, long n, void *stream);
+
+/* inc/cudecompose.h:35, src/tensor2matrix.cu:38-52: mode-n unfolding of an
+ * m x n x k tensor (flag 1 copy, 2: n x (m*k), 3: k x (m*n)). */
+int cud_t2m(const float *T1, float *T2, long flag, long m, long n, long k, void *stream);
+
+/* inc/cudecompose.h:37, src/tminust.cu:10-15: N = M - N over m elements. */
+int cud_tminust(const float *M, float *N, long m, void *stream);
+
+/* inc/cudecompose.h:47, src/tminust.cu:31-36 initMat: m x m identity. */
+int cud_init_identity(float *A, long m, void *stream);
+
+/* inc/cudecompose.h:38, src/rse.cu:4-15: X1 <- X - X1 and
+ * *err = ||X - X1|| / ||X|| (norms accumulated in FP64). err is a host pointer. */
+int cud_rse(const float *X, float *X1, long n, float *err, void *stream);
+
+/* Extension: sum of squares of x (FP64 accumulation), written to *out (host). */
+int cud_norm2(const float *x, long n, double *out, void *stream);
+
+/* ---- generators / reconstructions ------------------------------------- */
+
+/* inc/cudecompose.h:39,52, src/rse.cu:17-30,53-73 gencp/gencp4, any order:
+ * rec = sum_r U[0][:,r] o U[1][:,r] o ... ; U is a host array of `order`
+ * device pointers, U[m] is dims[m] x R. */
+int cud_gencp(float *rec, int order, const long *dims, const float *const *U, long R,
+              void *stream);
+
+/* inc/cudecompose.h:40,53, src/rse.cu:32-51,75-96 gentucker/gentucker4, any
+ * order: rec = core x_1 U[0] x_2 U[1] ...; core is ranks[0] x ranks[1] x ...,
+ * U[m] is dims[m] x ranks[m]. */
+int cud_gentucker(float *rec, int order, const long *dims, const float *core,
+                  const long *ranks, const float *const *U, void *stream);
+
+/* ---- contractions ------------------------------------------------------ */
+
+/* inc/cudecompose.h:29, src/ttm.cu:4-47: mode-`flag` product of the
+ * a x b x c tensor X with U (d x I_flag, row = new index); XU is d x b x c,
+ * a x d x c or a x b x d. */
+int cud_ttm(const float *X, const float *U, float *XU, long flag, long a, long b, long c,
+            long d, int precision, void *stream);
+
+/* Extension: general-order mode product Y = X x_mode W, W is J x dims[mode]
+ * (row = new index); Y has dims[mode] replaced by J. */
+int cud_mode_product(const float *X, int order, const long *dims, int mode, const float *W,
+                     long J, float *Y, int precision, void *stream);
+
+/* inc/cudecompose.h:30, src/mttkrp.cu:3-80: MTTKRP of the m x n x k tensor
+ * with the reference's operand convention (flag 1: left k x r, right n x r,
+ * XU m x r; flag 2: left k x r, right m x r, XU n x r; flag 3: left n x r,
+ * right m x r, XU k x r). */
+int cud_mttkrp_legacy(const float *X, const float *left, const float *right, float *XU,
+                      long flag, long m, long n, long k, long r, int precision, void *stream);
+
+/* The FP32 MTTKRPs inside src/cp_als.cu:46-52,66-69,85-88 and
+ * src/cp4_als.cu:201-207,225-230,246-251,269-272, any order, native layout:
+ * out (dims[mode] x R) = X_(mode) * (KR of the other factors), with no
+ * unfolding or Khatri-Rao matrix materialised. */
+int cud_mttkrp(const float *X, int order, const long *dims, const float *const *U, int mode,
+               long R, float *out, int precision, void *stream);
+
+/* Extension: the unfolding Gram G = X_(mode) X_(mode)^T (dims[mode]^2),
+ * written in FP64 -- the SGEMMs of src/tucker_hosvd.cu:27-29. */
+int cud_unfold_gram(const float *X, int order, const long *dims, int mode, double *G,
+                    int precision, void *stream);
+
+/* ---- symmetric eigensolver / small solves ------------------------------ */
+
+/* Extension (replaces cusolverDnSsyevdx at src/tucker_hosvd.cu:43-61):
+ * FP64 Jacobi eigensolver of the symmetric n x n matrix A (destroyed).
+ * W receives the n eigenvalues in ascending order and V the eigenvectors
+ * (column j pairs with W[j]).  max_sweeps bounds the iteration. */
+int cud_syev_jacobi(double *A, long n, double *W, double *V, int max_sweeps, void *stream);
+
+/* ---- decompositions ----------------------------------------------------- */
+
+typedef struct cud_cp_options {
+    int max_sweeps;   /* sweep limit (the reference's fixed L, src/cp_als.cu:42) */
+    double tol;       /* stop when |fit - fit_prev| < tol; <= 0 disables       */
+    int precision;    /* cud_precision of the MTTKRPs                          */
+    int use_graph;    /* capture each sweep in a CUDA graph                    */
+    int check_every;  /* read the fit back every this many sweeps (>= 1)       */
+} cud_cp_options;
+
+typedef struct cud_cp_result {
+    int sweeps;       /* sweeps run                                           */
+    int fallbacks;    /* normal-equation solves that fell back to pinv        */
+    double fit;       /* 1 - ||X - Xhat|| / ||X|| after the last sweep         */
+    double fit_prev;  /* fit one sweep earlier                                 */
+    double seconds;   /* wall time of the sweeps on the stream                 */
+    int kernels_per_sweep; /* kernel launches in one sweep (graph kernel nodes) */
+} cud_cp_result;
+
+/* Extension: default options (500 sweeps, tol 0, CUD_PREC_DEFAULT, graph on). */
+void cud_cp_default_options(cud_cp_options *opt);
+
+/* src/cp_als.cu:3-134 (order 3) and src/cp4_als.cu:3-186 (order 4) as one
+ * general-order entry: CP-ALS from the initial factors U (host array of
+ * device pointers, U[m] is dims[m] x R, updated in place).  Update order
+ * U[0], U[1], ...; normal equations (Hadamard of FP64 Grams) solved by FP64
+ * Cholesky with a pseudo-inverse fallback.  res may be NULL. */
+int cud_cp_als(const float *X, int order, const long *dims, long R, float *const *U,
+               const cud_cp_options *opt, cud_cp_result *res, void *stream);
+
+/* Extension: a reusable CP-ALS plan -- the workspace, the Grams and the
+ * captured per-sweep CUDA graph for one (X, dims, R, factors) problem, so
+ * sweeps can be enqueued without synchronisation (what cud_cp_als loops
+ * over).  X and U must stay allocated while the plan lives. */
+typedef struct cud_cp_plan_s *cud_cp_plan;
+
+/* Creates the plan, computes ||X||^2 and the initial Grams on `stream`. */
+int cud_cp_plan_create(const float *X, int order, const long *dims, long R, float *const *U,
+                       const cud_cp_options *opt, void *stream, cud_cp_plan *plan);
+/* Enqueues `sweeps` sweeps on `stream` (no host synchronisation). */
+int cud_cp_plan_run(cud_cp_plan plan, int sweeps, void *stream);
+/* Synchronises `stream` and reads the last two fits (either may be NULL). */
+int cud_cp_plan_fit(cud_cp_plan plan, double *fit, double *fit_prev, void *stream);
+/* Kernel launches per sweep and the pseudo-inverse fallbacks so far. */
+int cud_cp_plan_info(cud_cp_plan plan, int *kernels_per_sweep, int *fallbacks);
+int cud_cp_plan_destroy(cud_cp_plan plan);
+
+/* src/cp_als.cu:20-24: the reference's initialisation -- cuRAND default
+ * pseudo-random generator, seed 1234, uniform [0,1) into U[1], then U[2], ...
+ * (U[0] is left as is; the first update overwrites it). */
+int cud_cp_init_curand(int order, const long *dims, long R, float *const *U,
+                       unsigned long long seed, void *stream);
+
+/* src/tucker_hosvd.cu:3-103 (order 3), src/tucker4_hosvd.cu:3-141 (order 4):
+ * HOSVD.  U[m] (dims[m] x ranks[m]) = eigenvectors of the r_m largest
+ * eigenvalues of the FP64 unfolding Gram, in ascending eigenvalue order as
+ * the reference's syevdx output; core = X x_1 U1^T x_2 U2^T ... */
+int cud_tucker_hosvd(const float *X, int order, const long *dims, const long *ranks,
+                     float *core, float *const *U, int precision, void *stream);
+
+/* decomposition/GPU/normal/tucker/tucker_hooi.cu:3-218: HOOI, `sweeps`
+ * sweeps from the HOSVD initialisation of modes 2..N, then the core. */
+int cud_tucker_hooi(const float *X, int order, const long *dims, const long *ranks,
+                    float *core, float *const *U, int sweeps, int precision, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDECOMPOSE_C_H_ */

@@ -1,0 +1,107 @@
+"""CP-ALS on the GPU against the oracle's restatement of src/cp_als.cu and
+src/cp4_als.cu (same initial factors).
+
+Tolerances: the fit after a fixed number of sweeps within 1e-4 of the FP64
+oracle (the final-fit bar), factors within 1e-3 relative Frobenius norm.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def dev_t(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def low_rank(dims, R, seed, noise=1e-3):
+    rng = np.random.default_rng(seed)
+    true = [rng.random(d * R) for d in dims]
+    X = oracle.gencp(dims, true, R)
+    X = X + noise * np.linalg.norm(X) / np.sqrt(X.size) * rng.standard_normal(X.size)
+    init = [rng.random(d * R).astype(np.float32) for d in dims]
+    return X.astype(np.float32), init
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3", "default"])
+@pytest.mark.parametrize("dims,R", [((30, 25, 20), 4), ((16, 12, 10, 8), 3), ((64, 64, 64), 16)])
+def test_fixed_sweeps_match_oracle(cd, prec, dims, R):
+    X, init = low_rank(dims, R, seed=len(dims) * 100 + R)
+    sweeps = 15
+    facs_or, fits_or, n_or = oracle.cp_als(X, dims, R, init, sweeps)
+    U = [dev_t(f) for f in init]
+    res = cd.cp_als(dev_t(X), dims, R, U, max_sweeps=sweeps, tol=0.0,
+                    precision=cd.PRECISIONS[prec])
+    assert res.sweeps == sweeps
+    assert abs(res.fit - fits_or[-1]) <= 1e-4, (res.fit, fits_or[-1])
+    for u, f in zip(U, facs_or):
+        g = u.cpu().numpy().astype(np.float64)
+        assert np.linalg.norm(g - f) / np.linalg.norm(f) <= 1e-3
+
+
+def test_stopping_rule_matches_oracle(cd):
+    dims, R = (40, 36, 32), 5
+    X, init = low_rank(dims, R, seed=7)
+    facs_or, fits_or, n_or = oracle.cp_als(X, dims, R, init, 50, tol=1e-6)
+    U = [dev_t(f) for f in init]
+    res = cd.cp_als(dev_t(X), dims, R, U, max_sweeps=50, tol=1e-6)
+    assert abs(res.sweeps - n_or) <= 2, (res.sweeps, n_or)
+    assert abs(res.fit - fits_or[-1]) <= 1e-4
+
+
+def test_graph_and_eager_agree(cd):
+    dims, R = (24, 20, 18), 4
+    X, init = low_rank(dims, R, seed=9)
+    Ua = [dev_t(f) for f in init]
+    Ub = [dev_t(f) for f in init]
+    ra = cd.cp_als(dev_t(X), dims, R, Ua, max_sweeps=12, use_graph=True)
+    rb = cd.cp_als(dev_t(X), dims, R, Ub, max_sweeps=12, use_graph=False)
+    assert ra.fit == rb.fit
+    for a, b in zip(Ua, Ub):
+        assert torch.equal(a, b)
+
+
+def test_curand_init_and_500_sweeps_like_reference(cd):
+    """cp_als() of src/cp_als.cu:20-24,42: cuRAND seed 1234 init of B then C,
+    500 sweeps; checked against the oracle from the same initial factors."""
+    dims, R = (12, 10, 8), 3
+    X, _ = low_rank(dims, R, seed=21)
+    U = [torch.zeros(d * R, device="cuda") for d in dims]
+    cd.cp_init_curand(dims, R, U, 1234)
+    init = [u.cpu().numpy() for u in U]
+    assert init[1].min() >= 0 and init[1].max() <= 1 and init[2].std() > 0.1
+    facs_or, fits_or, _ = oracle.cp_als(X, dims, R, init, 500)
+    res = cd.cp_als(dev_t(X), dims, R, U, max_sweeps=500)
+    assert abs(res.fit - fits_or[-1]) <= 1e-4
+
+
+def test_singular_normal_equations_fall_back(cd):
+    """Two identical factor columns make the Hadamard of Grams singular: the
+    Cholesky fails and the pseudo-inverse path must keep the update finite."""
+    dims, R = (10, 9, 8), 2
+    rng = np.random.default_rng(4)
+    X = rng.random(int(np.prod(dims))).astype(np.float32)
+    init = []
+    for d in dims:
+        col = rng.random(d)
+        init.append(np.concatenate([col, col]).astype(np.float32))
+    U = [dev_t(f) for f in init]
+    res = cd.cp_als(dev_t(X), dims, R, U, max_sweeps=3)
+    assert res.fallbacks >= 1
+    for u in U:
+        assert torch.isfinite(u).all()
+
+
+def test_fit_matches_reconstruction(cd):
+    dims, R = (20, 16, 12), 3
+    X, init = low_rank(dims, R, seed=31, noise=1e-2)
+    U = [dev_t(f) for f in init]
+    res = cd.cp_als(dev_t(X), dims, R, U, max_sweeps=20)
+    rec = torch.empty(int(np.prod(dims)), device="cuda")
+    cd.gencp(rec, U, dims, R)
+    Xd = dev_t(X)
+    direct = 1.0 - torch.linalg.norm((Xd - rec).double()) / torch.linalg.norm(Xd.double())
+    assert abs(res.fit - float(direct)) <= 1e-5
