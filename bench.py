@@ -196,6 +196,10 @@ def main():
     ap.add_argument("--cpu-slab", type=int, default=64)
     ap.add_argument("--no-ttf", action="store_true", help="skip the time-to-fit runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--only-mttkrp", action="store_true",
+                    help="time only the MTTKRP kernels (profiling runs) and exit")
+    ap.add_argument("--kreps", type=int, default=10, help="timed MTTKRP launches per mode")
+    ap.add_argument("--kwarm", type=int, default=3, help="untimed MTTKRP launches per mode")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -234,9 +238,9 @@ def main():
     kern = {}
     U = [u.clone() for u in init]
     outs = [torch.empty(d * R, device="cuda") for d in dims]
-    reps = 10
+    reps = max(1, args.kreps)
     for mode in range(len(dims)):
-        for _ in range(3):
+        for _ in range(args.kwarm):
             cd.mttkrp(X, dims, U, mode, R, outs[mode], prec, stream=sptr)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -245,7 +249,12 @@ def main():
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / reps
-        kern[mode] = {"ms": round(ms, 5), "gbs": round(mttkrp_bytes(dims, R, mode) / ms / 1e6, 1)}
+        kern[mode] = {"ms": round(ms, 5), "gbs": round(mttkrp_bytes(dims, R, mode) / ms / 1e6, 1),
+                      "path": cd.mttkrp_path(dims, mode, R, prec)}
+    if args.only_mttkrp:
+        if rank == 0:
+            print(json.dumps({"mttkrp": kern, "dims": dims, "rank": R, "precision": prec_name}), flush=True)
+        return
 
     # ---- timed sweeps through the plan (graph replay)
     plan = cd.CpPlan(X, dims, R, U, precision=prec, stream=sptr)

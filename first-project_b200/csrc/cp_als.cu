@@ -155,6 +155,60 @@ extern "C" int cud_cp_init_curand(int order, const long *dims, long R, float *co
     return set_status(st);
 }
 
+extern "C" int cud_factor_gram(const float *U, long I, long R, double *G, void *stream) {
+    if (I <= 0 || R <= 0 || !U || !G) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    return set_status(factor_gram(U, I, R, G, as_stream(stream)));
+}
+
+extern "C" int cud_cp_solve(const float *M, long I, long R, int order, const double *const *G,
+                            int mode, float *U, double *work, void *stream) {
+    if (I <= 0 || R <= 0 || R > 160 || order < 2 || order > kMaxOrder || mode < 0 || mode >= order ||
+        !M || !G || !U || !work)
+        return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cudaStream_t s = as_stream(stream);
+    NormalArgs na;
+    for (int m = 0; m < order; m++) {
+        if (m != mode && !G[m]) return set_status(CUD_ERR_INVALID_ARGUMENT);
+        na.G[m] = (m == mode) ? G[(mode + 1) % order] : G[m];
+    }
+    na.nG = order;
+    na.mode = mode;
+    na.R = (int)R;
+    na.Vinv = work;
+    na.work = work + R * R;
+    na.fallbacks = reinterpret_cast<int *>(work + 3 * R * R);
+    int st = normal_inverse(na, s);
+    if (st == CUD_OK) st = apply_inverse(M, na.Vinv, I, R, U, s);
+    return set_status(st);
+}
+
+extern "C" int cud_cp_fit_terms(const float *M, const float *U, long IR, int order,
+                                const double *const *G, long R, double *inner, double *norm_hat2,
+                                void *stream) {
+    if (!M || !U || IR <= 0 || order < 1 || order > kMaxOrder || !G || R <= 0 || !inner || !norm_hat2)
+        return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cudaStream_t s = as_stream(stream);
+    int st;
+    double *d = (double *)scratch(kSlotReduce, 8 * sizeof(double), &st);
+    if (!d) return set_status(st);
+    FitArgs fa;
+    fa.M = M;
+    fa.U = U;
+    fa.IR = IR;
+    for (int m = 0; m < order; m++) fa.G[m] = G[m];
+    fa.nG = order;
+    fa.R = (int)R;
+    fa.normx2 = 1.0;
+    fa.out = d;
+    if ((st = fit_eval(fa, s))) return set_status(st);
+    double h[4];
+    CUD_CHECK(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CUD_CHECK(cudaStreamSynchronize(s));
+    *inner = h[2];
+    *norm_hat2 = h[3];
+    return set_status(CUD_OK);
+}
+
 extern "C" int cud_cp_plan_destroy(cud_cp_plan p) {
     if (!p) return set_status(CUD_OK);
     int prev = -1;

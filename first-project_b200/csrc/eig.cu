@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(NT) k_block_jacobi(EigArgs a) {
                     S[e] = (gi < n && gj < n) ? a.A[gi + (long)n * gj] : 0.0;
                 }
                 __syncthreads();
-                inner_jacobi(S, Qs, 1e-15);
+                inner_jacobi(S, Qs, 4e-15 * M2);
                 double *Qg = a.Q + (long)k * M2 * M2;
                 for (int e = threadIdx.x; e < M2 * M2; e += NT) Qg[e] = Qs[e];
                 __syncthreads();
@@ -336,7 +336,9 @@ int syev_jacobi(double *A, long n, double *W, double *V, int max_sweeps, cudaStr
     a.n = (int)n;
     a.nb = nb;
     a.max_sweeps = max_sweeps > 0 ? max_sweeps : 40;
-    a.tol = 1e-15;
+    // off(A) can only be driven to the rounding floor of the rotations,
+    // about n * eps relative to ||A||_F
+    a.tol = 4.0 * 2.22e-16 * (double)std::max(16L, n);
     CUD_CHECK(cudaMemsetAsync(w + off_bar, 0, 128, s));
     void *args[] = {&a};
     CUD_CHECK(cudaLaunchCooperativeKernel((void *)k_block_jacobi, grid, NT, args, 0, s));

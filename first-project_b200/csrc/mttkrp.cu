@@ -14,20 +14,24 @@ int round_mode(int precision) {
 }
 }  // namespace
 
+// Sized for both paths, so a call may fall back (e.g. a misaligned X) with
+// the same workspace.
 size_t mttkrp_ws_bytes(int order, const long *dims, int mode, long R, int precision) {
-    if (precision != CUD_PREC_FP32) {
-        size_t b = 0;
-        if (mttkrp_tc_query(order, dims, mode, R, precision, &b) == CUD_OK) return b;
-    }
-    return mttkrp_simt_ws_bytes(order, dims, mode, R, round_mode(precision));
+    size_t b = mttkrp_simt_ws_bytes(order, dims, mode, R, round_mode(precision));
+    size_t t = 0;
+    if (precision != CUD_PREC_FP32 && mttkrp_tc_query(order, dims, mode, R, precision, &t) == CUD_OK)
+        b = std::max(b, t);
+    return b;
 }
 
 int mttkrp_run(const float *X, int order, const long *dims, const float *const *U, int mode, long R,
                float *out, int precision, void *ws, cudaStream_t s) {
     if (precision != CUD_PREC_FP32) {
         size_t b = 0;
-        if (mttkrp_tc_query(order, dims, mode, R, precision, &b) == CUD_OK)
-            return mttkrp_tc(X, order, dims, U, mode, R, out, precision, ws, s);
+        if (mttkrp_tc_query(order, dims, mode, R, precision, &b) == CUD_OK) {
+            int st = mttkrp_tc(X, order, dims, U, mode, R, out, precision, ws, s);
+            if (st != CUD_ERR_UNSUPPORTED) return st;
+        }
     }
     return mttkrp_simt_rounded(X, order, dims, U, mode, R, out, round_mode(precision), ws, s);
 }
@@ -49,6 +53,13 @@ extern "C" int cud_mttkrp(const float *X, int order, const long *dims, const flo
     void *ws = scratch(kSlotMttkrp, mttkrp_ws_bytes(order, dims, mode, R, precision), &st);
     if (!ws) return set_status(st);
     return set_status(mttkrp_run(X, order, dims, U, mode, R, out, precision, ws, as_stream(stream)));
+}
+
+extern "C" int cud_mttkrp_path(int order, const long *dims, int mode, long R, int precision) {
+    if (order < 2 || order > kMaxOrder || !dims || mode < 0 || mode >= order || R <= 0) return 0;
+    if (precision == CUD_PREC_FP32) return 0;
+    size_t b = 0;
+    return mttkrp_tc_query(order, dims, mode, R, precision, &b) == CUD_OK ? 1 : 0;
 }
 
 extern "C" int cud_mttkrp_legacy(const float *X, const float *left, const float *right, float *XU,

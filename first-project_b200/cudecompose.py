@@ -95,6 +95,7 @@ _sig("cud_mode_product", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _l, _vp, _i, _vp
 _sig("cud_mttkrp_legacy", [_vp, _vp, _vp, _vp, _l, _l, _l, _l, _l, _i, _vp])
 _sig("cud_mttkrp", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _vp, _i, _vp])
 _sig("cud_unfold_gram", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _i, _vp])
+_sig("cud_mttkrp_path", [_i, ctypes.POINTER(_l), _i, _l, _i])
 _sig("cud_syev_jacobi", [_vp, _l, _vp, _vp, _i, _vp])
 _sig("cud_cp_default_options", [ctypes.POINTER(CpOptions)], None)
 _sig("cud_cp_als", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
@@ -107,6 +108,10 @@ _sig("cud_cp_plan_run", [_vp, _i, _vp])
 _sig("cud_cp_plan_fit", [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), _vp])
 _sig("cud_cp_plan_info", [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)])
 _sig("cud_cp_plan_destroy", [_vp])
+_sig("cud_factor_gram", [_vp, _l, _l, _vp, _vp])
+_sig("cud_cp_solve", [_vp, _l, _l, _i, ctypes.POINTER(_vp), _i, _vp, _vp, _vp])
+_sig("cud_cp_fit_terms", [_vp, _vp, _l, _i, ctypes.POINTER(_vp), _l, ctypes.POINTER(_d),
+                          ctypes.POINTER(_d), _vp])
 _sig("cud_tucker_hosvd", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp,
                           ctypes.POINTER(_vp), _i, _vp])
 _sig("cud_tucker_hooi", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp,
@@ -259,6 +264,11 @@ def mttkrp(X, dims, factors, mode, R, out, precision=PREC_DEFAULT, stream=None):
                            _ptr(out), precision, _stream(stream)), "mttkrp")
 
 
+def mttkrp_path(dims, mode, R, precision=PREC_DEFAULT) -> str:
+    """'tensor-core' or 'cuda-core': the kernel mttkrp() runs for this shape."""
+    return "tensor-core" if _lib.cud_mttkrp_path(len(dims), _longs(dims), mode, R, precision) else "cuda-core"
+
+
 def unfold_gram(X, dims, mode, G, stream=None):
     _check(_lib.cud_unfold_gram(_ptr(X), len(dims), _longs(dims), mode, _ptr(G), 0,
                                 _stream(stream)), "unfold_gram")
@@ -323,6 +333,27 @@ class CpPlan:
             self.close()
         except Exception:
             pass
+
+
+def factor_gram(U, I, R, G, stream=None):
+    """G (R x R, float64 device tensor) = U^T U for U (I x R column-major)."""
+    _check(_lib.cud_factor_gram(_ptr(U), I, R, _ptr(G), _stream(stream)), "factor_gram")
+
+
+def cp_solve(M, I, R, grams, mode, U, work, stream=None):
+    """U = M * inv(Hadamard of the Grams other than `mode`); work: float64
+    device tensor of at least 3 R^2 + 2 elements."""
+    _check(_lib.cud_cp_solve(_ptr(M), I, R, len(grams), _ptrs(grams), mode, _ptr(U), _ptr(work),
+                             _stream(stream)), "cp_solve")
+
+
+def cp_fit_terms(M, U, grams, R, stream=None):
+    """(<M, U>, sum_{r,s} prod_m G_m[r, s]) computed on the device."""
+    inner, nh = _d(0.0), _d(0.0)
+    _check(_lib.cud_cp_fit_terms(_ptr(M), _ptr(U), M.numel(), len(grams), _ptrs(grams), R,
+                                 ctypes.byref(inner), ctypes.byref(nh), _stream(stream)),
+           "cp_fit_terms")
+    return inner.value, nh.value
 
 
 def cp_init_curand(dims, R, factors, seed=1234, stream=None):

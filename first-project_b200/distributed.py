@@ -1,0 +1,105 @@
+"""CP-ALS across ranks (one process per GPU) with the tensor sharded along
+its last mode.
+
+Each rank holds a slab X_r = X[..., k0_r:k1_r] and the full factor matrices
+of the other modes; the last factor is sharded like X.  Per sweep, for every
+mode n:
+  * n < N-1: the local MTTKRP over the slab is a partial sum of the global
+    one; an all-reduce (sum) makes it global, then every rank computes the
+    same solve, so the replicated factors stay identical;
+  * n = N-1: the MTTKRP rows are local; each rank solves its own rows and
+    the Gram of the last factor is all-reduced.
+The fit needs <M_{N-1}, U_{N-1}> (all-reduced) and the Grams.  The collective
+is a real exchange of I_n x R partial sums; nothing else moves.
+
+The sweep logic is backend-neutral: `ops` supplies the per-rank compute
+(the CUDA library for GPUs, see CudaOps) and `comm` the all-reduce
+(torch.distributed over NCCL on GPUs, gloo on CPU in the tests).
+"""
+from __future__ import annotations
+
+import math
+
+
+class ShardedCP:
+    def __init__(self, ops, comm, X, local_dims, R, factors):
+        """factors[m] for m < N-1 are the full I_m x R factors (identical on
+        every rank); factors[N-1] holds this rank's rows of the last factor."""
+        self.ops, self.comm = ops, comm
+        self.X, self.dims, self.R = X, list(local_dims), R
+        self.U = list(factors)
+        self.N = len(local_dims)
+        self.G = [ops.gram(u, d) for u, d in zip(self.U, self.dims)]
+        self.G[-1] = comm.all_reduce(self.G[-1])
+        self.normx2 = comm.all_reduce_scalar(ops.norm2(X))
+        self.M_last = None
+
+    def sweep(self):
+        N = self.N
+        for n in range(N):
+            M = self.ops.mttkrp(self.X, self.dims, self.U, n, self.R)
+            if n < N - 1:
+                M = self.comm.all_reduce(M)
+            self.U[n] = self.ops.solve(M, self.dims[n], self.R, self.G, n)
+            G = self.ops.gram(self.U[n], self.dims[n])
+            self.G[n] = self.comm.all_reduce(G) if n == N - 1 else G
+            if n == N - 1:
+                self.M_last = M
+
+    def fit(self):
+        inner, nh = self.ops.fit_terms(self.M_last, self.U[-1], self.G, self.R)
+        inner = self.comm.all_reduce_scalar(inner)
+        res2 = self.normx2 - 2.0 * inner + nh
+        return 1.0 - math.sqrt(max(res2, 0.0)) / math.sqrt(self.normx2)
+
+
+class TorchComm:
+    """all-reduce (sum) through torch.distributed (NCCL on GPUs, gloo on CPU)."""
+
+    def __init__(self, dist):
+        self.dist = dist
+
+    def all_reduce(self, t):
+        self.dist.all_reduce(t)
+        return t
+
+    def all_reduce_scalar(self, x):
+        import torch
+        dev = "cuda" if self.dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t)
+        return float(t.item())
+
+
+class CudaOps:
+    """Per-rank compute on the GPU through the library's C ABI."""
+
+    def __init__(self, cd, precision, stream=None):
+        import torch
+        self.cd, self.precision, self.stream = cd, precision, stream
+        self.torch = torch
+        self._work = None
+
+    def mttkrp(self, X, dims, U, mode, R):
+        out = self.torch.empty(dims[mode] * R, device="cuda")
+        self.cd.mttkrp(X, dims, U, mode, R, out, self.precision, stream=self.stream)
+        return out
+
+    def solve(self, M, I, R, G, mode):
+        if self._work is None or self._work.numel() < 3 * R * R + 2:
+            self._work = self.torch.zeros(3 * R * R + 2, dtype=self.torch.float64, device="cuda")
+        U = self.torch.empty(I * R, device="cuda")
+        self.cd.cp_solve(M, I, R, G, mode, U, self._work, stream=self.stream)
+        return U
+
+    def gram(self, U, I):
+        R = U.numel() // I
+        G = self.torch.empty(R * R, dtype=self.torch.float64, device="cuda")
+        self.cd.factor_gram(U, I, R, G, stream=self.stream)
+        return G
+
+    def fit_terms(self, M, U, G, R):
+        return self.cd.cp_fit_terms(M, U, G, R, stream=self.stream)
+
+    def norm2(self, X):
+        return self.cd.norm2(X, stream=self.stream)

@@ -134,6 +134,10 @@ int cud_mttkrp_legacy(const float *X, const float *left, const float *right, flo
 int cud_mttkrp(const float *X, int order, const long *dims, const float *const *U, int mode,
                long R, float *out, int precision, void *stream);
 
+/* Extension: the kernel cud_mttkrp runs for these arguments (given a
+ * 16-byte-aligned X): 1 = tcgen05 tensor cores, 0 = CUDA cores. */
+int cud_mttkrp_path(int order, const long *dims, int mode, long R, int precision);
+
 /* Extension: the unfolding Gram G = X_(mode) X_(mode)^T (dims[mode]^2),
  * written in FP64 -- the SGEMMs of src/tucker_hosvd.cu:27-29. */
 int cud_unfold_gram(const float *X, int order, const long *dims, int mode, double *G,
@@ -193,6 +197,21 @@ int cud_cp_plan_fit(cud_cp_plan plan, double *fit, double *fit_prev, void *strea
 /* Kernel launches per sweep and the pseudo-inverse fallbacks so far. */
 int cud_cp_plan_info(cud_cp_plan plan, int *kernels_per_sweep, int *fallbacks);
 int cud_cp_plan_destroy(cud_cp_plan plan);
+
+/* Extension: the pieces of one CP-ALS mode update, for callers that
+ * orchestrate sweeps themselves (e.g. one process per GPU with the tensor
+ * sharded along its last mode and the partial MTTKRPs summed by NCCL).
+ * G = U^T U (R x R, FP64) for U (I x R). */
+int cud_factor_gram(const float *U, long I, long R, double *G, void *stream);
+/* U (I x R) = M (I x R) * V^-1 with V = Hadamard_{m != mode} G[m] (FP64
+ * Cholesky, pseudo-inverse fallback).  G is a host array of `order` device
+ * pointers (R x R each); work holds 3 R^2 doubles + 16 bytes. */
+int cud_cp_solve(const float *M, long I, long R, int order, const double *const *G, int mode,
+                 float *U, double *work, void *stream);
+/* Host results of the fit terms: inner = <M, U> (FP64) and
+ * norm_hat2 = sum_{r,s} prod_m G[m][r,s]. */
+int cud_cp_fit_terms(const float *M, const float *U, long IR, int order, const double *const *G,
+                     long R, double *inner, double *norm_hat2, void *stream);
 
 /* src/cp_als.cu:20-24: the reference's initialisation -- cuRAND default
  * pseudo-random generator, seed 1234, uniform [0,1) into U[1], then U[2], ...

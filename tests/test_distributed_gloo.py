@@ -1,0 +1,107 @@
+"""Host logic of the sharded (multi-GPU) CP-ALS, run as two gloo ranks on the
+CPU: the tensor is split along its last mode, the partial MTTKRPs of the
+other modes are all-reduced, the last factor stays sharded.  Per-rank
+compute comes from the oracle here (on GPUs it is the CUDA library, see
+distributed.CudaOps); the result must equal the single-process oracle ALS
+from the same start."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import oracle
+
+DIMS = (9, 8, 12)
+R = 3
+SWEEPS = 6
+
+
+class OracleOps:
+    def mttkrp(self, X, dims, U, mode, R):
+        return torch.from_numpy(oracle.mttkrp(X, dims, [u.numpy() for u in U], mode, R))
+
+    def solve(self, M, I, R, G, mode):
+        V = np.ones((R, R))
+        for m, g in enumerate(G):
+            if m != mode:
+                V = V * g.numpy().reshape(R, R, order="F")
+        Mm = M.numpy().reshape(I, R, order="F")
+        return torch.from_numpy(np.linalg.solve(V.T, Mm.T).T.reshape(-1, order="F").copy())
+
+    def gram(self, U, I):
+        Um = U.numpy().reshape(I, -1, order="F")
+        return torch.from_numpy((Um.T @ Um).reshape(-1, order="F").copy())
+
+    def fit_terms(self, M, U, G, R):
+        nh = np.ones((R, R))
+        for g in G:
+            nh = nh * g.numpy().reshape(R, R, order="F")
+        return float(np.dot(M.numpy(), U.numpy())), float(nh.sum())
+
+    def norm2(self, X):
+        return float(np.dot(X.astype(np.float64), X))
+
+
+def problem():
+    rng = np.random.default_rng(0)
+    true = [rng.random(d * R) for d in DIMS]
+    X = oracle.gencp(DIMS, true, R).astype(np.float32)
+    init = [rng.random(d * R) for d in DIMS]
+    return X, init
+
+
+def worker(rank, world, port, outdir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                    "first-project_b200"))
+    from distributed import ShardedCP, TorchComm
+    X, init = problem()
+    K = DIMS[-1]
+    k0, k1 = rank * K // world, (rank + 1) * K // world
+    Xg = X.reshape(DIMS, order="F")
+    Xl = np.asfortranarray(Xg[:, :, k0:k1]).reshape(-1, order="F")
+    ldims = (DIMS[0], DIMS[1], k1 - k0)
+    U = [torch.from_numpy(f.copy()) for f in init[:-1]]
+    Cl = init[-1].reshape(K, R, order="F")[k0:k1].reshape(-1, order="F").copy()
+    U.append(torch.from_numpy(Cl))
+    cp = ShardedCP(OracleOps(), TorchComm(dist), Xl, ldims, R, U)
+    fits = []
+    for _ in range(SWEEPS):
+        cp.sweep()
+        fits.append(cp.fit())
+    np.savez(os.path.join(outdir, f"rank{rank}.npz"), fits=np.array(fits),
+             *[u.numpy() for u in cp.U])
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_cp_matches_single_process(tmp_path, world):
+    mp.start_processes(worker, args=(world, free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    X, init = problem()
+    facs, fits, _ = oracle.cp_als(X, DIMS, R, init, SWEEPS, use_lu=True)
+    K = DIMS[-1]
+    parts = [np.load(tmp_path / f"rank{r}.npz") for r in range(world)]
+    for r, p in enumerate(parts):
+        np.testing.assert_allclose(p["fits"], fits, rtol=0, atol=1e-9)
+        for m in range(len(DIMS) - 1):
+            np.testing.assert_allclose(p[f"arr_{m}"], facs[m], rtol=1e-8, atol=1e-10)
+    # the sharded last factor, reassembled
+    C = np.concatenate([p[f"arr_{len(DIMS) - 1}"].reshape(-1, R, order="F") for p in parts])
+    np.testing.assert_allclose(C.reshape(-1, order="F"), facs[-1], rtol=1e-8, atol=1e-10)
