@@ -183,6 +183,105 @@ def config_dict(dims, R, precision, world=1):
             "l2": "inputs (512 MiB per tensor) exceed the 126 MB L2; no flush between steps"}
 
 
+def run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_name):
+    """N > 1: the global tensor is dims[0] x ... x (dims[-1] * N), sharded
+    along its last mode (one dims-sized slab per rank, weak scaling); the
+    partial MTTKRPs of the other modes are all-reduced over NCCL each sweep
+    (distributed.ShardedCP)."""
+    from distributed import CudaOps, ShardedCP, TorchComm
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1000)                      # shared factors of the other modes
+        shared = [torch.rand(R * d, generator=g, device="cuda") for d in dims[:-1]]
+        g.manual_seed(5000 + rank)               # this rank's rows of the last factor
+        last = torch.rand(R * dims[-1], generator=g, device="cuda")
+        n = 1
+        for d in dims:
+            n *= d
+        X = torch.empty(n, device="cuda")
+        cd.gencp(X, shared + [last], dims, R)
+        E = torch.randn(n, generator=g, device="cuda")
+        X.add_(E, alpha=1e-3 * (cd.norm2(X) / cd.norm2(E)) ** 0.5)
+        del E
+        g.manual_seed(2000)
+        init = [torch.rand(R * d, generator=g, device="cuda") for d in dims[:-1]]
+        g.manual_seed(6000 + rank)
+        init.append(torch.rand(R * dims[-1], generator=g, device="cuda"))
+    stream.synchronize()
+    comm = TorchComm(dist)
+    with torch.cuda.stream(stream):
+        cp = ShardedCP(CudaOps(cd, prec, stream=sptr), comm, X, dims, R, [u.clone() for u in init])
+        for _ in range(args.warmup):
+            cp.sweep()
+    torch.cuda.synchronize()
+    dist.barrier()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.steps):
+                cp.sweep()
+            e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_total = float(t.item())
+    with torch.cuda.stream(stream):
+        fit = cp.fit()
+    value = world * sweep_bytes(dims, R) * args.steps / (ms_total * 1e-3) / 1e9
+    # e2e: H2D of each rank's slab and factors, 10 sweeps, D2H of the factors
+    hX = torch.empty(X.numel(), dtype=torch.float32, pin_memory=True)
+    hX.copy_(X)
+    hU = [u.cpu().pin_memory() for u in init]
+    times = []
+    for it in range(3):
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            dX = hX.to("cuda", non_blocking=True)
+            dU = [u.to("cuda", non_blocking=True) for u in hU]
+            c2 = ShardedCP(CudaOps(cd, prec, stream=sptr), comm, dX, dims, R, dU)
+            for _ in range(args.e2e_sweeps):
+                c2.sweep()
+            outs = [u.to("cpu", non_blocking=True) for u in c2.U]
+            e1.record(stream)
+        e1.synchronize()
+        tt = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        if it > 0:
+            times.append(float(tt.item()) * 1e-3)
+    e2e_s = sum(times) / len(times)
+    peak, peak_kind = load_peaks()
+    per_sweep_launches = 5 * len(dims)
+    result = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_total / args.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic",
+        "config": dict(config_dict(dims, R, prec_name, world),
+                       workload=f"cp_als_sweep_{'x'.join(map(str, dims[:-1]))}x{dims[-1]}N_r{R}",
+                       parallelism=f"sharded along the last mode over {world} ranks, NCCL all-reduce"),
+        "gpu_launches": per_sweep_launches * args.steps * world,
+        "fit_after_timed_sweeps": round(fit, 8),
+        "clocks": clk.summary(),
+        "e2e": {"value": round(world * sweep_bytes(dims, R) * args.e2e_sweeps / e2e_s / 1e9, 3),
+                "unit": "GB/s", "h2d_bytes_per_step": 4 * (X.numel() + sum(u.numel() for u in init)),
+                "d2h_bytes_per_step": 4 * sum(u.numel() for u in init),
+                "step": f"sharded CP-ALS, {args.e2e_sweeps} sweeps, from pinned host buffers"},
+        "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                     "traffic": None, "note": "kernel roofline reported by the 1-GPU run"},
+    }
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -227,6 +326,9 @@ def main():
     R = args.rank
     prec = cd.PRECISIONS[args.precision]
     prec_name = "bf16x3" if prec in (cd.PREC_DEFAULT, cd.PREC_BF16X3) else args.precision
+    if world > 1 and not args.only_mttkrp:
+        run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_name)
+        return
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     with torch.cuda.stream(stream):

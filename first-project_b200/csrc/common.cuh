@@ -56,6 +56,7 @@ enum ScratchSlot {
     kSlotTmp1 = 3,
     kSlotTmp2 = 4,
     kSlotEig = 5,       // eigensolver work
+    kSlotGram = 6,      // factor Gram partials
     kNumSlots = 8
 };
 

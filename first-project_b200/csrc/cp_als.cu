@@ -31,10 +31,16 @@ struct cud_cp_plan_s {
     float *M = nullptr;
     double *G = nullptr, *Vinv = nullptr, *work = nullptr, *fit = nullptr;
     int *fallbacks = nullptr;
+    unsigned *counter = nullptr;  // ticket of the fused update's last-CTA reduction
+    double *gpart = nullptr;      // its per-CTA partial Grams
     void *ws = nullptr;
     double *hbuf = nullptr;  // pinned
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // the R x R inverse of mode n depends only on the other modes' Grams, so
+    // it runs on a second stream beside the mode-n MTTKRP
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int kernels_per_sweep = -1;
 };
 
@@ -64,9 +70,9 @@ int enqueue_sweep(cud_cp_plan_s *p, cudaStream_t s) {
     int st;
     const long R = p->R;
     for (int n = 0; n < p->order; n++) {
-        st = mttkrp_run(p->X, p->order, p->dims, (const float *const *)p->U, n, R, p->M,
-                        p->opt.precision, p->ws, s);
-        if (st) return st;
+        // fork: V^-1 of mode n on the side stream, concurrent with the MTTKRP
+        CUD_CHECK(cudaEventRecord(p->ev_fork, s));
+        CUD_CHECK(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
         NormalArgs na;
         for (int m = 0; m < p->order; m++) na.G[m] = p->G + (size_t)m * R * R;
         na.nG = p->order;
@@ -75,20 +81,32 @@ int enqueue_sweep(cud_cp_plan_s *p, cudaStream_t s) {
         na.Vinv = p->Vinv;
         na.work = p->work;
         na.fallbacks = p->fallbacks;
-        if ((st = normal_inverse(na, s))) return st;
-        if ((st = apply_inverse(p->M, p->Vinv, p->dims[n], R, p->U[n], s))) return st;
-        if ((st = factor_gram(p->U[n], p->dims[n], R, p->G + (size_t)n * R * R, s))) return st;
+        if ((st = normal_inverse(na, p->side))) return st;
+        CUD_CHECK(cudaEventRecord(p->ev_join, p->side));
+        st = mttkrp_run(p->X, p->order, p->dims, (const float *const *)p->U, n, R, p->M,
+                        p->opt.precision, p->ws, s);
+        if (st) return st;
+        CUD_CHECK(cudaStreamWaitEvent(s, p->ev_join, 0));
+        // join: U_n = M V^-1, its Gram, and after the last mode the fit
+        UpdateArgs ua;
+        ua.M = p->M;
+        ua.Vinv = p->Vinv;
+        ua.U = p->U[n];
+        ua.I = p->dims[n];
+        ua.R = (int)R;
+        ua.G_out = p->G + (size_t)n * R * R;
+        ua.gpart = p->gpart;
+        ua.counter = p->counter;
+        if (n == p->order - 1) {
+            for (int m = 0; m < p->order; m++) ua.Gall[m] = p->G + (size_t)m * R * R;
+            ua.nG = p->order;
+            ua.mode = n;
+            ua.normx2 = p->normx2;
+            ua.fit_out = p->fit;
+        }
+        if ((st = factor_update(ua, s))) return st;
     }
-    FitArgs fa;
-    fa.M = p->M;
-    fa.U = p->U[p->order - 1];
-    fa.IR = p->dims[p->order - 1] * R;
-    for (int m = 0; m < p->order; m++) fa.G[m] = p->G + (size_t)m * R * R;
-    fa.nG = p->order;
-    fa.R = (int)R;
-    fa.normx2 = p->normx2;
-    fa.out = p->fit;
-    return fit_eval(fa, s);
+    return CUD_OK;
 }
 
 // Capture needs a stream other than the legacy default one.
@@ -216,6 +234,12 @@ extern "C" int cud_cp_plan_destroy(cud_cp_plan p) {
     cudaSetDevice(p->device);
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->side) {
+        cudaStreamSynchronize(p->side);
+        cudaStreamDestroy(p->side);
+    }
+    if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+    if (p->ev_join) cudaEventDestroy(p->ev_join);
     if (p->mem) cudaFree(p->mem);
     if (p->hbuf) cudaFreeHost(p->hbuf);
     if (prev >= 0) cudaSetDevice(prev);
@@ -260,8 +284,9 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     size_t off_V = off_G + up(sizeof(double) * order * R * R);
     size_t off_W = off_V + up(sizeof(double) * R * R);
     size_t off_F = off_W + up(sizeof(double) * 2 * R * R);
-    size_t off_C = off_F + up(sizeof(double) * 4);
-    size_t off_S = off_C + 256;
+    size_t off_C = off_F + up(sizeof(double) * 4);  // fallbacks (int) + counter
+    size_t off_P = off_C + 256;
+    size_t off_S = off_P + up(sizeof(double) * update_ws_doubles(maxd, R));
     size_t bytes = off_S + up(wsb);
     cudaError_t e = cudaMalloc((void **)&p->mem, bytes);
     if (e != cudaSuccess) {
@@ -280,7 +305,16 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     p->work = (double *)(p->mem + off_W);
     p->fit = (double *)(p->mem + off_F);
     p->fallbacks = (int *)(p->mem + off_C);
+    p->counter = (unsigned *)(p->mem + off_C + 64);
+    p->gpart = (double *)(p->mem + off_P);
     p->ws = p->mem + off_S;
+    if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        cud_cp_plan_destroy(p);
+        return set_status(CUD_ERR_CUDA);
+    }
 
     SideStream ss;
     int st = ss.open(as_stream(stream));
@@ -289,7 +323,8 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
         st = residual_norms(X, nullptr, total, 0, o, ss.s);
         p->normx2 = o[1];
     }
-    if (st == CUD_OK && cudaMemsetAsync(p->fit, 0, sizeof(double) * 4 + 256, ss.s) != cudaSuccess)
+    // fit scalars, fallback count and the update ticket start at zero
+    if (st == CUD_OK && cudaMemsetAsync(p->fit, 0, off_P - off_F, ss.s) != cudaSuccess)
         st = CUD_ERR_CUDA;
     for (int m = 0; m < order && st == CUD_OK; m++)
         st = factor_gram(U[m], dims[m], R, p->G + (size_t)m * R * R, ss.s);

@@ -10,10 +10,14 @@
 //     swizzle);
 //   * four converter warps read their rows, split each value into BF16
 //     hi + lo (x = hi + lo + O(2^-16 x)), and store both into tensor memory
-//     as the MMA's A operand (one TMEM lane per row);
-//   * the same warps form the 32 Khatri-Rao rows of the stage from the factor
-//     matrices, split them the same way, and write them to shared memory in
-//     the K-major canonical layout (the B operand);
+//     as the MMA's A operand (one TMEM lane per row), so X crosses shared
+//     memory only once;
+//   * the same warps form the stage's 32 Khatri-Rao rows: the stage's kappa
+//     run over 32 consecutive rows of the fastest generating factor while
+//     the other factors contribute one constant row, so each thread loads
+//     two 128-bit vectors of one factor column (prefetched a stage ahead),
+//     scales them, splits them and stores 16 bytes per operand into the
+//     K-major canonical B layout;
 //   * one thread issues tcgen05.mma (kind::f16, FP32 accumulation in TMEM):
 //     D += Xhi*KRhi + Xhi*KRlo + Xlo*KRhi  (BF16X3), or one product for
 //     BF16 / FP16.
@@ -23,8 +27,8 @@
 // over the contraction splits in FP64.
 //
 // Every wait is bounded: an expired wait raises a CTA-wide abort flag, the
-// roles drain and the TMEM is freed before the CTA exits; the host sees the
-// error flag and returns CUD_ERR_DEVICE_TIMEOUT.
+// roles drain and the TMEM is freed before the CTA exits, and the kernel's
+// error flag is set.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -35,36 +39,37 @@ namespace cud {
 
 namespace {
 
-constexpr int BQ = 128;      // rows per CTA tile (MMA M)
-constexpr int BKS = 32;      // contraction depth per stage (two MMA K-steps of 16)
-constexpr int NST = 4;       // pipeline stages
-constexpr int NTHREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2..5 converters
+constexpr int BQ = 128;          // rows per CTA tile (MMA M)
+constexpr int BKS = 32;          // contraction depth per stage (two MMA K-steps of 16)
+constexpr int NST = 4;           // pipeline stages
+constexpr int NTHREADS = 192;    // warp 0 TMA, warp 1 MMA, warps 2..5 converters
 constexpr int NCONV = 128;
 constexpr uint32_t TMEM_COLS = 256;
 constexpr uint32_t A_COL0 = 128;  // A stages start at this TMEM column
 constexpr int X_STAGE_BYTES = BQ * BKS * 4;  // 16 KB
+constexpr int RPAD_MAX = 128;
 
 struct TcArgs {
     long P, Q, S, R;
     int Rpad;          // R rounded up to a multiple of 16 (MMA N)
     int kind;          // 0: mode 0 (rows contiguous); 1: other modes (kappa contiguous)
-    int prec;          // CUD_PREC_BF16 / FP16 / BF16X3
+    int prec;          // CUD_PREC_BF16 / FP16 / BF16X3 / DEFAULT
+    int fast;          // stages never cross a row block of the fastest generating factor
     long psteps;       // stages per s (kind 1) = ceil(P / 32)
     long stages;       // total stages
     long chunk;        // stages per CTA
     long qtiles;
     KrFactors gen;     // kind 0: factors after mode 0; kind 1: factors before the mode
-    KrFactors outer;   // kind 1: factors after the mode (per-stage constant row)
+    KrFactors outer;   // kind 1: factors after the mode (one constant row per stage)
     float *part;       // [split][R][Q]
     int *error;        // device flag
 };
 
-// Shared memory: control block first, then (1024-byte aligned) the NST X
-// stages of 16 KB, then the NST pairs of B tiles of Rpad x 32 16-bit values.
 struct TcCtrl {
     uint64_t full_x[NST], empty_x[NST], full_a[NST], empty_a[NST], done;
-    int tab[BKS][kMaxOrder];   // KR row indices of the current stage
-    int rt[kMaxOrder];         // row index of the outer factors (per stage constant)
+    const float *gU[kMaxOrder];
+    const float *oU[kMaxOrder];
+    long grows[kMaxOrder], orows[kMaxOrder];
     uint32_t tmem_base;
     int abort;
 };
@@ -95,12 +100,96 @@ __device__ __forceinline__ void split_pair(float a, float b, uint32_t &hi, uint3
     lo = pack_bf16(a - f.x, b - f.y);
 }
 
-// Byte offset of element (n, k) (16-bit) in a K-major, no-swizzle B tile of
-// 32 columns: core matrix (n/8, k/8) at (n/8)*512 + (k/8)*128.
-__device__ __forceinline__ uint32_t b_offset(int n, int k) {
-    return (uint32_t)((n >> 3) * 512 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2);
+// B tile (Rpad x 32 16-bit values, K-major, no swizzle): core matrix
+// (n/8, k/8) -- 8 rows x 16 bytes -- at (n/8)*128 + (k/8)*Rpad*16, so the
+// 8 values k = 8c..8c+7 of row n form one 16-byte chunk at n*16 + c*Rpad*16.
+// Descriptor: SBO (8-row groups) = 128 B, LBO (K chunks) = Rpad*16 B.
+
+// The Khatri-Rao values one converter thread produces per stage: IPT items,
+// each (row r, chunk kc) = 8 consecutive kappa of one column r.
+template <int IPT>
+struct KrRegs {
+    float f[IPT][8];
+    float c[IPT];
+};
+
+struct StageInfo {
+    long k0;    // first contraction index of the stage (s for kind 0, p for kind 1)
+    long kmax;  // contraction extent (S or P)
+    long s;     // kind 1: the slab index
+};
+
+__device__ __forceinline__ StageInfo stage_info(const TcArgs &a, long g) {
+    StageInfo si;
+    if (a.kind == 0) {
+        si.k0 = g * BKS;
+        si.kmax = a.S;
+        si.s = 0;
+    } else {
+        si.s = g / a.psteps;
+        si.k0 = (g % a.psteps) * BKS;
+        si.kmax = a.P;
+    }
+    return si;
 }
 
+// Loads (fast path) or computes (general path) this thread's KR items for
+// stage g into registers.
+template <int IPT>
+__device__ __forceinline__ void kr_load(const TcArgs &a, const TcCtrl &sm, long g, int ct,
+                                        KrRegs<IPT> &o) {
+    StageInfo si = stage_info(a, g);
+    const int ng = a.gen.n, no = a.outer.n;
+    // constant-row indices for this stage
+    long gidx[kMaxOrder], oidx[kMaxOrder];
+    long rest = si.k0 / sm.grows[0];
+    const long i0 = si.k0 % sm.grows[0];
+    for (int f = 1; f < ng; f++) {
+        gidx[f] = rest % sm.grows[f];
+        rest /= sm.grows[f];
+    }
+    long srest = si.s;
+    for (int f = 0; f < no; f++) {
+        oidx[f] = srest % sm.orows[f];
+        srest /= sm.orows[f];
+    }
+#pragma unroll
+    for (int it = 0; it < IPT; it++) {
+        const int id = ct + NCONV * it;
+        const int kc = id & 3;
+        const int r = id >> 2;
+#pragma unroll
+        for (int j = 0; j < 8; j++) o.f[it][j] = 0.f;
+        o.c[it] = 0.f;
+        if (r >= a.R) continue;
+        float c = 1.f;
+        for (int f = 0; f < no; f++) c *= __ldg(sm.oU[f] + oidx[f] + r * sm.orows[f]);
+        if (a.fast) {
+            for (int f = 1; f < ng; f++) c *= __ldg(sm.gU[f] + gidx[f] + r * sm.grows[f]);
+            const float4 *src = reinterpret_cast<const float4 *>(sm.gU[0] + i0 + kc * 8 + r * sm.grows[0]);
+            float4 v0 = __ldg(src), v1 = __ldg(src + 1);
+            o.f[it][0] = v0.x; o.f[it][1] = v0.y; o.f[it][2] = v0.z; o.f[it][3] = v0.w;
+            o.f[it][4] = v1.x; o.f[it][5] = v1.y; o.f[it][6] = v1.z; o.f[it][7] = v1.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                long k = si.k0 + kc * 8 + j;
+                if (k >= si.kmax) continue;
+                float v = 1.f;
+                long lin = k;
+                for (int f = 0; f < ng; f++) {
+                    long d = sm.grows[f];
+                    v *= __ldg(sm.gU[f] + (lin % d) + r * d);
+                    lin /= d;
+                }
+                o.f[it][j] = v;
+            }
+        }
+        o.c[it] = c;
+    }
+}
+
+template <int IPT>
 __global__ void __launch_bounds__(NTHREADS, 2)
     k_mttkrp_tc(const __grid_constant__ CUtensorMap tmap, TcArgs a) {
     extern __shared__ uint8_t smem_raw[];
@@ -108,7 +197,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     TcCtrl &sm = *reinterpret_cast<TcCtrl *>(base);
     float *xst = reinterpret_cast<float *>(base + CTRL_BYTES);
     uint8_t *bst = base + CTRL_BYTES + (size_t)NST * X_STAGE_BYTES;
-    const size_t bbytes = b_tile_bytes(a.Rpad);
+    const uint32_t bbytes = (uint32_t)b_tile_bytes(a.Rpad);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long qtile = blockIdx.x % a.qtiles;
     const long z = blockIdx.x / a.qtiles;
@@ -127,6 +216,12 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         }
         ptx::mbar_init(&sm.done, 1);
         sm.abort = 0;
+        for (int f = 0; f < kMaxOrder; f++) {
+            sm.gU[f] = f < a.gen.n ? a.gen.U[f] : nullptr;
+            sm.grows[f] = f < a.gen.n ? a.gen.rows[f] : 1;
+            sm.oU[f] = f < a.outer.n ? a.outer.U[f] : nullptr;
+            sm.orows[f] = f < a.outer.n ? a.outer.rows[f] : 1;
+        }
         ptx::fence_mbar_init();
         ptx::prefetch_tmap(&tmap);
     }
@@ -153,11 +248,12 @@ __global__ void __launch_bounds__(NTHREADS, 2)
                 long g = st_beg + i;
                 issued = i + 1;
                 ptx::mbar_arrive_expect_tx(&sm.full_x[slot], X_STAGE_BYTES);
+                float *dst = xst + (size_t)slot * BQ * BKS;
                 if (a.kind == 0) {
-                    ptx::tma_load_2d((xst + (size_t)slot * BQ * BKS), &tmap, &sm.full_x[slot], (int)q0, (int)(g * BKS));
+                    ptx::tma_load_2d(dst, &tmap, &sm.full_x[slot], (int)q0, (int)(g * BKS));
                 } else {
                     long s = g / a.psteps, p0 = (g % a.psteps) * BKS;
-                    ptx::tma_load_3d((xst + (size_t)slot * BQ * BKS), &tmap, &sm.full_x[slot], (int)p0, (int)q0, (int)s);
+                    ptx::tma_load_3d(dst, &tmap, &sm.full_x[slot], (int)p0, (int)q0, (int)s);
                 }
             }
         }
@@ -165,6 +261,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t idesc = ptx::idesc_f16(f16 ? 0u : 1u, BQ, (uint32_t)a.Rpad);
+            const uint32_t lbo = (uint32_t)a.Rpad * 16u;
             uint32_t acc = 0;
             for (long i = 0; i < nst; i++) {
                 int slot = (int)(i % NST);
@@ -174,14 +271,14 @@ __global__ void __launch_bounds__(NTHREADS, 2)
                 const uint32_t a_hi = tbase + A_COL0 + (uint32_t)slot * 32u;
                 const uint32_t a_lo = a_hi + 16u;
                 const uint32_t b_hi = ptx::smem_addr(bst + (size_t)(2 * slot) * bbytes);
-                const uint32_t b_lo = ptx::smem_addr(bst + (size_t)(2 * slot + 1) * bbytes);
+                const uint32_t b_lo = b_hi + bbytes;
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
-                    uint64_t dh = ptx::smem_desc_kmajor_noswizzle(b_hi + j * 256, 128, 512);
+                    uint64_t dh = ptx::smem_desc_kmajor_noswizzle(b_hi + 2 * j * lbo, lbo, 128);
                     ptx::mma_ts_f16(tbase, a_hi + j * 8, dh, idesc, acc);
                     acc = 1;
                     if (three) {
-                        uint64_t dl = ptx::smem_desc_kmajor_noswizzle(b_lo + j * 256, 128, 512);
+                        uint64_t dl = ptx::smem_desc_kmajor_noswizzle(b_lo + 2 * j * lbo, lbo, 128);
                         ptx::mma_ts_f16(tbase, a_hi + j * 8, dl, idesc, 1);
                         ptx::mma_ts_f16(tbase, a_lo + j * 8, dh, idesc, 1);
                     }
@@ -199,57 +296,64 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         const int row = sub * 32 + lane;          // row within the tile (= TMEM lane)
         const int ct = threadIdx.x - 64;          // 0..127 among converters
         const uint32_t lane_off = (uint32_t)(sub * 32) << 16;
+        KrRegs<IPT> nxt;
+        if (nst > 0) kr_load<IPT>(a, sm, st_beg, ct, nxt);
         for (long i = 0; i < nst; i++) {
-            int slot = (int)(i % NST);
-            long use = i / NST;
-            long g = st_beg + i;
-            // stage decode
-            long s = 0, p0 = 0;
-            if (a.kind == 1) { s = g / a.psteps; p0 = (g % a.psteps) * BKS; }
-            long k0 = (a.kind == 0) ? g * BKS : p0;  // first contraction index of the stage
-            long kmax = (a.kind == 0) ? a.S : a.P;
-            // KR index table for this stage (threads 0..31), outer row (thread 32)
-            if (ct < BKS) {
-                long k = k0 + ct;
-                if (k < kmax) {
-                    long lin = k;
-                    for (int f = 0; f < a.gen.n; f++) {
-                        sm.tab[ct][f] = (int)(lin % a.gen.rows[f]);
-                        lin /= a.gen.rows[f];
-                    }
-                } else {
-                    sm.tab[ct][0] = -1;
-                }
-            } else if (ct == BKS && a.kind == 1) {
-                long lin = s;
-                for (int f = 0; f < a.outer.n; f++) {
-                    sm.rt[f] = (int)(lin % a.outer.rows[f]);
-                    lin /= a.outer.rows[f];
-                }
-            }
+            const int slot = (int)(i % NST);
+            const long use = i / NST;
+            KrRegs<IPT> cur = nxt;
+            if (i + 1 < nst) kr_load<IPT>(a, sm, st_beg + i + 1, ct, nxt);
             // The slot's TMEM A stage and B tile are free once the MMAs of its
             // previous use completed.  After an abort the loop keeps running
             // (without waiting) so every converter thread reaches the same
-            // warp-aligned tcgen05 instructions and named barriers.
+            // warp-aligned tcgen05 instructions.
             if (use > 0 && !*abort) ptx::mbar_wait(&sm.empty_a[slot], (uint32_t)((use - 1) & 1), abort);
-            if (!*abort) ptx::mbar_wait(&sm.full_x[slot], (uint32_t)(use & 1), abort);
-            __syncwarp();
-            // ---- A operand: this thread's row, 32 values
-            float x[BKS];
-            const float *xs = (xst + (size_t)slot * BQ * BKS);
-            if (a.kind == 0) {
+            // ---- B operand: this thread's KR items -> 16-byte chunks
+            {
+                uint8_t *bh = bst + (size_t)(2 * slot) * bbytes;
+                uint8_t *bl = bh + bbytes;
 #pragma unroll
-                for (int k = 0; k < BKS; k++) x[k] = xs[k * BQ + row];
-            } else {
-                const float4 *r4 = reinterpret_cast<const float4 *>(xs + row * BKS);
+                for (int it = 0; it < IPT; it++) {
+                    const int id = ct + NCONV * it;
+                    const int r = id >> 2, kc = id & 3;
+                    if (r >= a.Rpad) continue;
+                    const uint32_t off = (uint32_t)r * 16u + (uint32_t)kc * (uint32_t)a.Rpad * 16u;
+                    float v[8];
 #pragma unroll
-                for (int c = 0; c < 8; c++) {
-                    float4 v = r4[c ^ (row & 7)];
-                    x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+                    for (int j = 0; j < 8; j++) v[j] = cur.f[it][j] * cur.c[it];
+                    uint4 h, l;
+                    if (f16) {
+                        h.x = pack_f16(v[0], v[1]); h.y = pack_f16(v[2], v[3]);
+                        h.z = pack_f16(v[4], v[5]); h.w = pack_f16(v[6], v[7]);
+                    } else if (three) {
+                        split_pair(v[0], v[1], h.x, l.x); split_pair(v[2], v[3], h.y, l.y);
+                        split_pair(v[4], v[5], h.z, l.z); split_pair(v[6], v[7], h.w, l.w);
+                        *reinterpret_cast<uint4 *>(bl + off) = l;
+                    } else {
+                        h.x = pack_bf16(v[0], v[1]); h.y = pack_bf16(v[2], v[3]);
+                        h.z = pack_bf16(v[4], v[5]); h.w = pack_bf16(v[6], v[7]);
+                    }
+                    *reinterpret_cast<uint4 *>(bh + off) = h;
                 }
             }
-            ptx::mbar_arrive(&sm.empty_x[slot]);
+            if (!*abort) ptx::mbar_wait(&sm.full_x[slot], (uint32_t)(use & 1), abort);
+            __syncwarp();
+            // ---- A operand: this thread's row, 32 values -> TMEM (hi, lo)
             {
+                float x[BKS];
+                const float *xs = xst + (size_t)slot * BQ * BKS;
+                if (a.kind == 0) {
+#pragma unroll
+                    for (int k = 0; k < BKS; k++) x[k] = xs[k * BQ + row];
+                } else {
+                    const float4 *r4 = reinterpret_cast<const float4 *>(xs + row * BKS);
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        float4 v = r4[c ^ (row & 7)];
+                        x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+                    }
+                }
+                ptx::mbar_arrive(&sm.empty_x[slot]);
                 uint32_t hi[16], lo[16];
                 if (f16) {
 #pragma unroll
@@ -265,51 +369,10 @@ __global__ void __launch_bounds__(NTHREADS, 2)
                 ptx::tmem_st16(ta, hi);
                 if (three) ptx::tmem_st16(ta + 16, lo);
             }
-            // ---- B operand: the stage's 32 KR rows, Rpad columns
-            ptx::named_bar_sync(1, NCONV);  // index table ready
-            {
-                uint8_t *bh = bst + (size_t)(2 * slot) * bbytes;
-                uint8_t *bl = bst + (size_t)(2 * slot + 1) * bbytes;
-                const int npairs = a.Rpad * (BKS / 2);
-                for (int e = ct; e < npairs; e += NCONV) {
-                    int r = e % a.Rpad, kp = e / a.Rpad;
-                    float v0 = 0.f, v1 = 0.f;
-                    if (r < a.R) {
-                        float w = 1.0f;
-                        if (a.kind == 1)
-                            for (int f = 0; f < a.outer.n; f++)
-                                w *= __ldg(a.outer.U[f] + sm.rt[f] + r * a.outer.rows[f]);
-                        const int *t0 = sm.tab[2 * kp];
-                        const int *t1 = sm.tab[2 * kp + 1];
-                        if (t0[0] >= 0) {
-                            v0 = 1.0f;
-                            for (int f = 0; f < a.gen.n; f++) v0 *= __ldg(a.gen.U[f] + t0[f] + r * a.gen.rows[f]);
-                            v0 *= w;
-                        }
-                        if (t1[0] >= 0) {
-                            v1 = 1.0f;
-                            for (int f = 0; f < a.gen.n; f++) v1 *= __ldg(a.gen.U[f] + t1[f] + r * a.gen.rows[f]);
-                            v1 *= w;
-                        }
-                    }
-                    uint32_t off = b_offset(r, 2 * kp);
-                    if (f16) {
-                        *reinterpret_cast<uint32_t *>(bh + off) = pack_f16(v0, v1);
-                    } else if (three) {
-                        uint32_t h, l;
-                        split_pair(v0, v1, h, l);
-                        *reinterpret_cast<uint32_t *>(bh + off) = h;
-                        *reinterpret_cast<uint32_t *>(bl + off) = l;
-                    } else {
-                        *reinterpret_cast<uint32_t *>(bh + off) = pack_bf16(v0, v1);
-                    }
-                }
-            }
             ptx::fence_proxy_async_smem();  // generic-proxy B writes -> tensor core
             ptx::tmem_wait_st();
             ptx::tc_fence_before();
             ptx::mbar_arrive(&sm.full_a[slot]);
-            ptx::named_bar_sync(2, NCONV);  // table slot reuse guard
         }
         // ---- epilogue: D (128 x Rpad FP32) -> partial
         if (!*abort) ptx::mbar_wait(&sm.done, 0, abort);
@@ -351,15 +414,19 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     if (warp == 0) ptx::tmem_dealloc(tbase, TMEM_COLS);
 }
 
-__global__ void k_sum_tc_partials(const float *__restrict__ part, int splits, long n,
-                                  float *__restrict__ out) {
-    long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    long stride = (long)gridDim.x * blockDim.x;
-    for (long e = tid; e < n; e += stride) {
-        double s = 0.0;
-        for (int z = 0; z < splits; z++) s += (double)part[(long)z * n + e];
-        out[e] = (float)s;
-    }
+// out[e] = sum_z part[z][e] in FP64: 64 outputs per CTA, the splits spread
+// over 4 lanes per output (coalesced rows of 64), combined in fixed order.
+__global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict__ part, int splits,
+                                                         long n, float *__restrict__ out) {
+    __shared__ double red[4][64];
+    const int o = threadIdx.x & 63, lanez = threadIdx.x >> 6;
+    const long e = blockIdx.x * 64L + o;
+    double s = 0.0;
+    if (e < n)
+        for (int z = lanez; z < splits; z += 4) s += (double)__ldcs(part + (long)z * n + e);
+    red[lanez][o] = s;
+    __syncthreads();
+    if (lanez == 0 && e < n) out[e] = (float)(((red[0][o] + red[1][o]) + red[2][o]) + red[3][o]);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -383,7 +450,7 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     if (!(precision == CUD_PREC_BF16 || precision == CUD_PREC_FP16 || precision == CUD_PREC_BF16X3 ||
           precision == CUD_PREC_DEFAULT))
         return false;
-    if (order < 2 || R <= 0 || R > 128) return false;
+    if (order < 2 || order > kMaxOrder || R <= 0 || R > RPAD_MAX) return false;
     ModeView v = mode_view(order, dims, mode);
     p.P = v.P; p.Q = v.Q; p.S = v.S;
     p.kind = (mode == 0) ? 0 : 1;
@@ -402,6 +469,21 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     p.chunk = (p.stages + p.splits - 1) / p.splits;
     p.splits = (p.stages + p.chunk - 1) / p.chunk;
     return true;
+}
+
+template <int IPT>
+int launch_tc(const CUtensorMap &tmap, const TcArgs &a, unsigned grid, cudaStream_t s) {
+    static bool attr[64] = {false};
+    int dev = 0;
+    CUD_CHECK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !attr[dev]) {
+        CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_tc<IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)tc_smem_bytes(RPAD_MAX)));
+        attr[dev] = true;
+    }
+    k_mttkrp_tc<IPT><<<grid, NTHREADS, tc_smem_bytes(a.Rpad), s>>>(tmap, a);
+    CUD_CHECK_LAUNCH("mttkrp_tc");
+    return CUD_OK;
 }
 
 }  // namespace
@@ -460,22 +542,26 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
         f.rows[f.n] = dims[m];
         f.n++;
     }
+    // Fast KR path: every stage covers 32 consecutive rows of the fastest
+    // generating factor (its row count is a multiple of 32) and that
+    // factor's columns can be read as aligned 128-bit vectors.
+    a.fast = (a.gen.rows[0] % BKS == 0) && ((reinterpret_cast<uintptr_t>(a.gen.U[0]) & 15) == 0);
     char *w = static_cast<char *>(ws);
     a.error = reinterpret_cast<int *>(w);
     a.part = reinterpret_cast<float *>(w + 256);
-    size_t smem = tc_smem_bytes(a.Rpad);
-    static bool attr[64] = {false};
-    int dev = 0;
-    CUD_CHECK(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !attr[dev]) {
-        CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr[dev] = true;
-    }
     CUD_CHECK(cudaMemsetAsync(a.error, 0, sizeof(int), s));
-    k_mttkrp_tc<<<(unsigned)(p.qtiles * p.splits), NTHREADS, smem, s>>>(tmap, a);
-    CUD_CHECK_LAUNCH("mttkrp_tc");
+    unsigned grid = (unsigned)(p.qtiles * p.splits);
+    int ipt = std::max(1, (int)((p.Rpad + 31) / 32));
+    int st;
+    switch (ipt) {
+        case 1: st = launch_tc<1>(tmap, a, grid, s); break;
+        case 2: st = launch_tc<2>(tmap, a, grid, s); break;
+        case 3: st = launch_tc<3>(tmap, a, grid, s); break;
+        default: st = launch_tc<4>(tmap, a, grid, s); break;
+    }
+    if (st) return st;
     long n = R * p.Q;
-    k_sum_tc_partials<<<blocks_for(n, 256), 256, 0, s>>>(a.part, (int)p.splits, n, out);
+    k_sum_tc_partials<<<(unsigned)((n + 63) / 64), 256, 0, s>>>(a.part, (int)p.splits, n, out);
     CUD_CHECK_LAUNCH("mttkrp_tc reduce");
     return CUD_OK;
 }

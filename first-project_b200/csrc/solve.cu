@@ -110,12 +110,16 @@ __device__ int block_jacobi_smem(double *A, double *Q, int n, int max_sweeps, do
 }
 
 // V = Hadamard of the Grams of all factors except `mode`; Vinv = V^-1 by
-// Cholesky (V = L L^T, Vinv = L^-T L^-1), or, when a pivot is not positive,
-// the pseudo-inverse from a Jacobi eigendecomposition.  One CTA, V in
-// dynamic shared memory.  `work` is global scratch of 2 R^2 doubles.
+// in-place Gauss-Jordan elimination without pivoting (V is symmetric
+// positive definite, so every pivot is a positive Schur complement -- the
+// same pivots as its Cholesky factorisation), or, when a pivot is not
+// positive, the pseudo-inverse from a Jacobi eigendecomposition.  One CTA,
+// V in dynamic shared memory, two barriers per pivot.  `work` is global
+// scratch of 2 R^2 doubles.
 __global__ void __launch_bounds__(512) k_normal_inverse(NormalArgs a) {
     extern __shared__ double V[];  // R x R
     __shared__ int s_fail;
+    __shared__ double rowk[160], colk[160];
     const int R = a.R;
     for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
         double v = 1.0;
@@ -125,48 +129,33 @@ __global__ void __launch_bounds__(512) k_normal_inverse(NormalArgs a) {
     }
     if (threadIdx.x == 0) s_fail = 0;
     __syncthreads();
-    // right-looking Cholesky, lower triangle
     double maxdiag = 0.0;
     for (int j = 0; j < R; j++) maxdiag = fmax(maxdiag, fabs(V[j + R * j]));
-    for (int j = 0; j < R; j++) {
-        double d = V[j + R * j];
-        if (!(d > 1e-13 * maxdiag) || !isfinite(d)) {
+    for (int k = 0; k < R; k++) {
+        const double piv = V[k + R * k];
+        if (!(piv > 1e-13 * maxdiag) || !isfinite(piv)) {  // same decision in every thread
             if (threadIdx.x == 0) s_fail = 1;
             break;
         }
-        d = sqrt(d);
+        const double inv = 1.0 / piv;
+        for (int j = threadIdx.x; j < R; j += blockDim.x) {
+            rowk[j] = (j == k ? 1.0 : V[k + R * j]) * inv;
+            colk[j] = V[j + R * k];
+        }
         __syncthreads();
-        if (threadIdx.x == 0) V[j + R * j] = d;
-        for (int i = j + 1 + threadIdx.x; i < R; i += blockDim.x) V[i + R * j] /= d;
-        __syncthreads();
-        int w = R - j - 1;
-        for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-            int i = j + 1 + e % w, k = j + 1 + e / w;
-            if (k <= i) V[i + R * k] -= V[i + R * j] * V[k + R * j];
+        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+            const int i = e % R, j = e / R;
+            const double old = (j == k) ? 0.0 : V[e];
+            V[e] = (i == k) ? rowk[j] : old - colk[i] * rowk[j];
         }
         __syncthreads();
     }
     __syncthreads();
-    double *Linv = a.work;        // R x R
     double *Q = a.work + R * R;   // R x R (pinv path)
     if (!s_fail) {
-        // Linv = L^-1 (lower), one column per thread
-        for (int c = threadIdx.x; c < R; c += blockDim.x) {
-            for (int i = 0; i < R; i++) Linv[i + R * c] = 0.0;
-            for (int i = c; i < R; i++) {
-                double s = (i == c) ? 1.0 : 0.0;
-                for (int k = c; k < i; k++) s -= V[i + R * k] * Linv[k + R * c];
-                Linv[i + R * c] = s / V[i + R * i];
-            }
-        }
-        __syncthreads();
-        // Vinv = Linv^T Linv
         for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-            int i = e % R, j = e / R;
-            int k0 = max(i, j);
-            double s = 0.0;
-            for (int k = k0; k < R; k++) s += Linv[k + R * i] * Linv[k + R * j];
-            a.Vinv[e] = s;
+            const int i = e % R, j = e / R;
+            a.Vinv[e] = 0.5 * (V[e] + V[j + R * i]);  // symmetrise the rounding
         }
     } else {
         // pseudo-inverse: rebuild V, eigendecompose, invert eigenvalues above tol
@@ -246,13 +235,154 @@ __global__ void __launch_bounds__(256) k_fit(FitArgs a) {
     }
 }
 
+// Fused factor update:  U = M * Vinv (FP64 accumulation; skipped when Vinv
+// is null, then U = M), G = U^T U, and optionally the fit.  Each CTA owns a
+// contiguous block of rows, walks it 16 rows at a time (the rows staged in
+// shared memory as doubles), keeps its share of the R x R Gram in
+// registers, and writes one partial Gram (+ its part of <M, U>).  The last
+// CTA to finish (atomic ticket) sums the partials in CTA order --
+// deterministic -- writes G, resets the ticket and, if asked, the fit.
+constexpr int UPD_RB = 16;
+
+template <int NT, int NACC>
+__global__ void __launch_bounds__(NT) k_update(UpdateArgs a) {
+    extern __shared__ double sU[];  // UPD_RB x R
+    __shared__ int s_last;
+    __shared__ double s_red[NT / 32];
+    const int R = a.R;
+    const long I = a.I;
+    const long rpb = (I + gridDim.x - 1) / gridDim.x;
+    const long r0 = blockIdx.x * rpb, r1 = min(I, r0 + rpb);
+    double acc[NACC];
+#pragma unroll
+    for (int k = 0; k < NACC; k++) acc[k] = 0.0;
+    double inner = 0.0;
+    for (long c0 = r0; c0 < r1; c0 += UPD_RB) {
+        const int nr = (int)min((long)UPD_RB, r1 - c0);
+        for (int e = threadIdx.x; e < UPD_RB * R; e += NT) {
+            const int i = e % UPD_RB, c = e / UPD_RB;
+            double u = 0.0;
+            if (i < nr) {
+                const long gi = c0 + i;
+                if (a.Vinv) {
+                    double s = 0.0;
+                    for (int r = 0; r < R; r++) s = fma((double)a.M[gi + I * r], a.Vinv[r + R * c], s);
+                    float uf = (float)s;
+                    a.U[gi + I * c] = uf;
+                    u = (double)uf;
+                } else {
+                    u = (double)a.M[gi + I * c];
+                }
+                if (a.fit_out) inner += (double)a.M[gi + I * c] * u;
+            }
+            sU[i + UPD_RB * c] = u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NACC; k++) {
+            const int e = threadIdx.x + NT * k;
+            if (e < R * R) {
+                const int p = e % R, q = e / R;
+                double s = acc[k];
+#pragma unroll
+                for (int i = 0; i < UPD_RB; i++) s = fma(sU[i + UPD_RB * p], sU[i + UPD_RB * q], s);
+                acc[k] = s;
+            }
+        }
+        __syncthreads();
+    }
+    const long stride = (long)R * R + 1;
+    double *mine = a.gpart + blockIdx.x * stride;
+#pragma unroll
+    for (int k = 0; k < NACC; k++) {
+        const int e = threadIdx.x + NT * k;
+        if (e < R * R) mine[e] = acc[k];
+    }
+    for (int o = 16; o > 0; o >>= 1) inner += __shfl_xor_sync(0xffffffffu, inner, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = inner;
+    __threadfence();  // every thread's partial-Gram stores, device-wide
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < NT / 32; w++) t += s_red[w];
+        mine[R * R] = t;
+        __threadfence();
+        unsigned ticket = atomicAdd(a.counter, 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // last CTA: fixed-order sum of the partials
+    for (long e = threadIdx.x; e < stride; e += NT) {
+        double s = 0.0;
+        for (unsigned b = 0; b < gridDim.x; b++) s += __ldcg(a.gpart + b * stride + e);
+        if (e < (long)R * R) a.G_out[e] = s;
+        else s_red[0] = s;  // inner product (written by exactly one thread)
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) atomicExch(a.counter, 0u);
+    if (!a.fit_out) return;
+    const double in = s_red[0];
+    __syncthreads();
+    double hat = 0.0;
+    for (int e = threadIdx.x; e < R * R; e += NT) {
+        double p = 1.0;
+        for (int m = 0; m < a.nG; m++) p *= (m == a.mode) ? __ldcg(a.G_out + e) : a.Gall[m][e];
+        hat += p;
+    }
+    for (int o = 16; o > 0; o >>= 1) hat += __shfl_xor_sync(0xffffffffu, hat, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = hat;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double h = 0.0;
+        for (int w = 0; w < NT / 32; w++) h += s_red[w];
+        double res2 = a.normx2 - 2.0 * in + h;
+        double fit = 1.0 - sqrt(res2 > 0.0 ? res2 : 0.0) / sqrt(a.normx2);
+        a.fit_out[1] = a.fit_out[0];
+        a.fit_out[0] = fit;
+        a.fit_out[2] = in;
+        a.fit_out[3] = h;
+    }
+}
+
 }  // namespace
 
-int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s) {
-    dim3 grid((unsigned)((R + 15) / 16), (unsigned)((R + 15) / 16));
-    k_factor_gram<<<grid, 256, 0, s>>>(U, I, R, G);
-    CUD_CHECK_LAUNCH("factor_gram");
+int update_blocks(long I) { return (int)std::max(1L, std::min((long)kNumSMs, (I + UPD_RB - 1) / UPD_RB)); }
+
+size_t update_ws_doubles(long I, long R) { return (size_t)update_blocks(I) * (size_t)(R * R + 1); }
+
+int factor_update(const UpdateArgs &a, cudaStream_t s) {
+    const int nb = update_blocks(a.I);
+    const size_t smem = sizeof(double) * UPD_RB * a.R;
+    if (a.R <= 32) k_update<256, 4><<<nb, 256, smem, s>>>(a);
+    else if (a.R <= 64) k_update<256, 16><<<nb, 256, smem, s>>>(a);
+    else if (a.R <= 160) k_update<512, 50><<<nb, 512, smem, s>>>(a);
+    else return CUD_ERR_UNSUPPORTED;
+    CUD_CHECK_LAUNCH("factor_update");
     return CUD_OK;
+}
+
+int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s) {
+    if (R > 160) {
+        dim3 grid((unsigned)((R + 15) / 16), (unsigned)((R + 15) / 16));
+        k_factor_gram<<<grid, 256, 0, s>>>(U, I, R, G);
+        CUD_CHECK_LAUNCH("factor_gram");
+        return CUD_OK;
+    }
+    int st;
+    size_t nd = update_ws_doubles(I, R);
+    char *w = (char *)scratch(kSlotGram, 256 + sizeof(double) * nd, &st);
+    if (!w) return st;
+    UpdateArgs a;
+    a.M = U;
+    a.I = I;
+    a.R = (int)R;
+    a.G_out = G;
+    a.counter = reinterpret_cast<unsigned *>(w);
+    a.gpart = reinterpret_cast<double *>(w + 256);
+    CUD_CHECK(cudaMemsetAsync(w, 0, 256, s));
+    return factor_update(a, s);
 }
 
 int normal_inverse_prepare() {

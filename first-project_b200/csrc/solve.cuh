@@ -26,6 +26,25 @@ struct FitArgs {
     double *out = nullptr;       // [fit, fit_prev, inner, ||Xhat||^2]
 };
 
+struct UpdateArgs {
+    const float *M = nullptr;      // I x R
+    const double *Vinv = nullptr;  // R x R, or null: U = M, Gram only
+    float *U = nullptr;            // I x R out (when Vinv is set)
+    long I = 0;
+    int R = 0;
+    double *G_out = nullptr;       // R x R Gram of U
+    double *gpart = nullptr;       // update_ws_doubles(I, R) doubles
+    unsigned *counter = nullptr;   // zero; left zero on return
+    // optional fit (when fit_out is set): Gall[m] for m != mode, G_out for mode
+    const double *Gall[kMaxOrder];
+    int nG = 0, mode = 0;
+    double normx2 = 0.0;
+    double *fit_out = nullptr;     // [fit, fit_prev, inner, ||Xhat||^2]
+};
+// Fused U = M Vinv, G = U^T U (+ fit), deterministic multi-CTA reduction.
+int factor_update(const UpdateArgs &a, cudaStream_t s);
+size_t update_ws_doubles(long I, long R);
+
 int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s);
 int normal_inverse(const NormalArgs &a, cudaStream_t s);
 // Per-device kernel attributes for normal_inverse; call before stream capture.
