@@ -112,6 +112,36 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def mttkrp_sample_errors(cd, torch, X, dims, R, U, sptr, rows=(0, 77, 300)):
+    """Relative error of each MTTKRP precision against an FP64 evaluation of
+    a few output rows of every mode (3rd-order workloads)."""
+    import numpy as np
+    if len(dims) != 3:
+        return None
+    X3 = X.cpu().numpy().reshape(tuple(reversed(dims))).transpose(2, 1, 0).astype(np.float64)
+    F = [u.cpu().numpy().reshape(R, d).T.astype(np.float64) for u, d in zip(U, dims)]
+    out = {}
+    for name in ("fp32", "bf16x3", "bf16", "fp16"):
+        errs = {}
+        for mode in range(3):
+            got = torch.empty(dims[mode] * R, device="cuda")
+            cd.mttkrp(X, dims, U, mode, R, got, cd.PRECISIONS[name], stream=sptr)
+            torch.cuda.synchronize()
+            g = got.cpu().numpy().reshape(R, dims[mode]).T.astype(np.float64)
+            num = den = 0.0
+            for q in rows:
+                if q >= dims[mode]:
+                    continue
+                sl = np.take(X3, q, axis=mode)          # the other two modes, in order
+                a, b = [F[m] for m in range(3) if m != mode]
+                want = np.einsum("ij,ir,jr->r", sl, a, b)
+                num += float(np.sum((g[q] - want) ** 2))
+                den += float(np.sum(want ** 2))
+            errs[str(mode)] = float(f"{(num / den) ** 0.5:.3e}")
+        out[name] = errs
+    return out
+
+
 def cpu_sweep_gbs(X3, factors, sweeps=1):
     """Times NumPy ALS sweeps (oracle port of mycp.py) -> (GB/s, seconds)."""
     import numpy as np
@@ -412,20 +442,31 @@ def main():
         "clocks": clk.summary(),
     }
 
-    # ---- time to fit (<= 50 sweeps or delta fit < 1e-6), per precision
+    # ---- MTTKRP error against FP64 on sampled output rows (NumPy on the host)
+    result["mttkrp_error_vs_fp64"] = mttkrp_sample_errors(cd, torch, X, dims, R, init, sptr)
+
+    # ---- time to fit: the plain FP32 path (CUDA cores) runs to convergence
+    # (delta fit < 1e-7, <= 200 sweeps); every variant then runs from the same
+    # start until it is within 1e-4 of that fit.
     if not args.no_ttf:
-        ttf = {}
+        Ut = [u.clone() for u in init]
+        torch.cuda.synchronize()
+        ref = cd.cp_als(X, dims, R, Ut, max_sweeps=200, tol=1e-7, precision=cd.PREC_FP32, stream=sptr)
+        target = ref.fit - 1e-4
+        ttf = {"reference_fp32": {"seconds": round(ref.seconds, 5), "sweeps": ref.sweeps,
+                                  "fit": round(ref.fit, 8)},
+               "target_fit": round(target, 8)}
         for name in ("fp32", "bf16x3", "bf16"):
             Ut = [u.clone() for u in init]
             torch.cuda.synchronize()
-            res = cd.cp_als(X, dims, R, Ut, max_sweeps=50, tol=1e-6,
+            res = cd.cp_als(X, dims, R, Ut, max_sweeps=200, target_fit=target,
                             precision=cd.PRECISIONS[name], stream=sptr)
             ttf[name] = {"seconds": round(res.seconds, 5), "sweeps": res.sweeps,
-                         "fit": round(res.fit, 8)}
+                         "fit": round(res.fit, 8), "reached": bool(res.fit >= target)}
         base = ttf["fp32"]["seconds"]
-        for name in ttf:
-            ttf[name]["speedup_vs_fp32"] = round(base / ttf[name]["seconds"], 3) if ttf[name]["seconds"] else None
-            ttf[name]["fit_delta_vs_fp32"] = round(abs(ttf[name]["fit"] - ttf["fp32"]["fit"]), 8)
+        for name in ("fp32", "bf16x3", "bf16"):
+            s = ttf[name]["seconds"]
+            ttf[name]["speedup_vs_fp32"] = round(base / s, 3) if s else None
         result["time_to_fit"] = ttf
 
     # ---- end to end through the C ABI with host buffers: H2D of X and the

@@ -20,6 +20,9 @@ constexpr int kNumSMs = 148;  // B200: 2 dies x 74 SMs
 // returns it unchanged, so entry points can `return set_status(...)`.
 int set_status(int st);
 
+// Records `st` with a detail message (read by cud_last_error_detail).
+int set_status_msg(int st, const char *msg);
+
 // Maps a CUDA runtime error to a library status, recording the CUDA message.
 int cuda_status(cudaError_t e, const char *where);
 

@@ -152,6 +152,7 @@ extern "C" void cud_cp_default_options(cud_cp_options *opt) {
     opt->precision = CUD_PREC_DEFAULT;
     opt->use_graph = 1;
     opt->check_every = 1;
+    opt->target_fit = 0.0;
 }
 
 extern "C" int cud_cp_init_curand(int order, const long *dims, long R, float *const *U,
@@ -407,15 +408,16 @@ extern "C" int cud_cp_als(const float *X, int order, const long *dims, long R, f
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
         cudaEventRecord(t0, ss.s);
-        int chunk = (opt.tol > 0) ? opt.check_every : opt.max_sweeps;
+        int chunk = (opt.tol > 0 || opt.target_fit > 0) ? opt.check_every : opt.max_sweeps;
         if (chunk <= 0) chunk = 1;
         while (sweeps < opt.max_sweeps && st == CUD_OK) {
             int n = std::min(chunk, opt.max_sweeps - sweeps);
             st = cud_cp_plan_run(p, n, ss.s);
             sweeps += n;
-            if (st == CUD_OK && opt.tol > 0) {
+            if (st == CUD_OK && (opt.tol > 0 || opt.target_fit > 0)) {
                 st = cud_cp_plan_fit(p, &fit, &fit_prev, ss.s);
-                if (st == CUD_OK && sweeps >= 2 && fabs(fit - fit_prev) < opt.tol) break;
+                if (st == CUD_OK && opt.tol > 0 && sweeps >= 2 && fabs(fit - fit_prev) < opt.tol) break;
+                if (st == CUD_OK && opt.target_fit > 0 && fit >= opt.target_fit) break;
             }
         }
         cudaEventRecord(t1, ss.s);

@@ -16,6 +16,12 @@ int set_status(int st) {
     return st;
 }
 
+int set_status_msg(int st, const char *msg) {
+    t_last_status = st;
+    snprintf(t_last_detail, sizeof(t_last_detail), "%s", msg ? msg : "");
+    return st;
+}
+
 int cuda_status(cudaError_t e, const char *where) {
     snprintf(t_last_detail, sizeof(t_last_detail), "%s: %s", where, cudaGetErrorString(e));
     int st = (e == cudaErrorMemoryAllocation) ? CUD_ERR_NO_MEMORY : CUD_ERR_CUDA;

@@ -45,20 +45,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+// try_wait with a suspend-time hint: the thread sleeps in hardware until the
+// phase completes or about `hint_ns` elapse, instead of spinning.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t *bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait: returns false (and raises *abort) when the phase with the
-// given parity has not completed after `limit` polls, or when another role
-// has already raised *abort.
+// given parity has not completed after `limit` hinted polls (~0.1 ms each,
+// so the default gives up after a few seconds), or when another role has
+// already raised *abort.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
-                                          long limit = (1L << 26)) {
+                                          long limit = 40000) {
+    if (mbar_try_wait(bar, parity)) return true;
     for (long i = 0;; i++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 63) == 63) {
-            if (*abort) return false;
-            if (i > limit) {
-                *abort = 1;
-                return false;
-            }
-            __nanosleep(32);
+        if (mbar_try_wait_hint(bar, parity, 100000u)) return true;
+        if (*abort) return false;
+        if (i > limit) {
+            *abort = 1;
+            return false;
         }
     }
 }

@@ -57,7 +57,7 @@ _d = ctypes.c_double
 
 class CpOptions(ctypes.Structure):
     _fields_ = [("max_sweeps", _i), ("tol", _d), ("precision", _i),
-                ("use_graph", _i), ("check_every", _i)]
+                ("use_graph", _i), ("check_every", _i), ("target_fit", _d)]
 
 
 class CpResult(ctypes.Structure):
@@ -287,9 +287,11 @@ def cp_default_options() -> CpOptions:
 
 
 def cp_als(X, dims, R, factors, max_sweeps=500, tol=0.0, precision=PREC_DEFAULT,
-           use_graph=True, check_every=1, stream=None) -> CpResult:
-    """CP-ALS from the given initial factors (updated in place)."""
-    opt = CpOptions(max_sweeps, tol, precision, 1 if use_graph else 0, check_every)
+           use_graph=True, check_every=1, target_fit=0.0, stream=None) -> CpResult:
+    """CP-ALS from the given initial factors (updated in place).  Stops after
+    max_sweeps, when |fit - fit_prev| < tol (tol > 0), or when fit >=
+    target_fit (target_fit > 0)."""
+    opt = CpOptions(max_sweeps, tol, precision, 1 if use_graph else 0, check_every, target_fit)
     res = CpResult()
     _check(_lib.cud_cp_als(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
                            ctypes.byref(opt), ctypes.byref(res), _stream(stream)), "cp_als")
@@ -302,7 +304,7 @@ class CpPlan:
 
     def __init__(self, X, dims, R, factors, precision=PREC_DEFAULT, use_graph=True, stream=None):
         self._keep = (X, list(factors))
-        opt = CpOptions(0, 0.0, precision, 1 if use_graph else 0, 1)
+        opt = CpOptions(0, 0.0, precision, 1 if use_graph else 0, 1, 0.0)
         h = _vp()
         _check(_lib.cud_cp_plan_create(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
                                        ctypes.byref(opt), _stream(stream), ctypes.byref(h)),

@@ -159,6 +159,7 @@ typedef struct cud_cp_options {
     int precision;    /* cud_precision of the MTTKRPs                          */
     int use_graph;    /* capture each sweep in a CUDA graph                    */
     int check_every;  /* read the fit back every this many sweeps (>= 1)       */
+    double target_fit; /* also stop once fit >= target_fit (<= 0 disables)     */
 } cud_cp_options;
 
 typedef struct cud_cp_result {
