@@ -134,6 +134,19 @@ int cud_mttkrp_legacy(const float *X, const float *left, const float *right, flo
 int cud_mttkrp(const float *X, int order, const long *dims, const float *const *U, int mode,
                long R, float *out, int precision, void *stream);
 
+/* No counterpart in the reference.  cud_mttkrp for callers that cannot
+ * allocate device memory (code running inside host callbacks or allocator
+ * hooks, or under a framework that owns all device memory): same arguments,
+ * kernels and results, but its workspace is a fixed 32 MiB __device__ array
+ * inside the library, so it calls no cudaMalloc/cudaFree.  A call needing
+ * more workspace is rejected (CUD_ERR_INVALID_ARGUMENT, message in
+ * cud_last_error_detail).  All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first
+ * call on a device resolves the array's address; make it before any stream
+ * capture. */
+int cud_mttkrp_noalloc(const float *X, int order, const long *dims, const float *const *U,
+                       int mode, long R, float *out, int precision, void *stream);
+
 /* Extension: the kernel cud_mttkrp runs for these arguments (given a
  * 16-byte-aligned X): 1 = tcgen05 tensor cores, 0 = CUDA cores. */
 int cud_mttkrp_path(int order, const long *dims, int mode, long R, int precision);
