@@ -1,0 +1,584 @@
+// Batched CP-ALS: thousands of small, independent 3rd-order tensors of uneven
+// shape and rank, one persistent kernel launch per ALS sweep for the whole
+// batch (sized for 4096 tensors with dims in [16, 96] and ranks in [4, 16]).
+//
+// Each CTA pulls tensors from a work queue (largest first) and runs one full
+// sweep of that tensor on its own, everything on-chip except X:
+//   * the three factor matrices live in shared memory (<= 96 x 16 each);
+//   * each MTTKRP streams X through shared memory one frontal slice
+//     (I x J) at a time and contracts it with register-blocked FMA (the
+//     ranks are too small for tensor cores to pay): mode 1 over j, modes 2
+//     and 3 over i, with the slice's C row as the per-slice weight (mode 3
+//     reduces the slice to one row of M);
+//   * the R x R normal equations (Hadamard of the FP64 Grams) are inverted
+//     by Gauss-Jordan in shared memory (FP64), with a tiny diagonal shift
+//     retried when a pivot is not positive;
+//   * the fit comes from ||X||^2 - 2 <M_3, C> + sum prod G (FP64), per
+//     tensor; a tensor whose fit changed by less than `tol` is marked
+//     converged and skipped by later sweeps.
+// The host captures `sweeps_per_graph` sweeps (queue reset + kernel) in one
+// CUDA graph and replays it until every tensor has converged or hit the
+// sweep limit.  The CTA size and the CTAs per SM come from a small autotuner
+// (batched_tune) that times one sweep per candidate on the batch itself and
+// caches the winner per batch shape class.
+#include <map>
+#include <mutex>
+#include <vector>
+#include <algorithm>
+
+#include "kernels.cuh"
+
+namespace cud {
+
+namespace {
+
+constexpr int BMAXD = 96;    // largest mode size handled (smem sizing)
+constexpr int BMAXR = 16;    // largest rank handled
+
+struct TensorMeta {
+    long xoff;          // offset of X (elements) in the packed tensor buffer
+    long uoff[3];       // offsets of the factors in the packed factor buffer
+    int dims[3];
+    int R;
+    int done;
+    int sweeps;
+    double normx2;
+    double fit, fit_prev;
+    double G[3][BMAXR * BMAXR];  // factor Grams (FP64)
+};
+
+struct BatchArgs {
+    TensorMeta *meta;
+    const int *order;   // processing order (largest first)
+    int ntensors;
+    const float *X;
+    float *U;
+    unsigned *queue;    // work counter, zero at kernel start
+    int *ndone;         // tensors marked converged so far
+    int max_sweeps;
+    double tol;
+    int *fallbacks;
+};
+
+// shared memory layout (floats / doubles), sized for BMAXD x BMAXR
+struct BatchSmem {
+    float F[3][BMAXD * BMAXR];       // factors, column-major I_m x R
+    float slice[BMAXD * (BMAXD + 1)];// one frontal slice, row stride I + 1
+    float M[BMAXD * BMAXR];          // MTTKRP result of the current mode
+    float red3[BMAXR * (BMAXD / 2)]; // mode-3 per-slice partials (rank x row pair)
+    double V[BMAXR * BMAXR];         // normal matrix / its inverse
+    double rowk[BMAXR], colk[BMAXR];
+    double red[32];
+    int tensor;
+    int fail;
+};
+
+template <int NT>
+__device__ void load_factors(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t) {
+    for (int m = 0; m < 3; m++) {
+        const float *src = a.U + t.uoff[m];
+        const int n = t.dims[m] * t.R;
+        for (int e = threadIdx.x; e < n; e += NT) sm.F[m][e] = src[e];
+    }
+}
+
+// M (I_mode x R) = MTTKRP of mode `mode` with the factors in shared memory.
+// Thread items: (row pair, 4 ranks) with rows = i (mode 1) or j (modes 2, 3);
+// at most (96 / 2) * 4 = 192 items, IPB = ceil(192 / NT) per thread.
+template <int NT>
+__device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
+    constexpr int IPB = (BMAXD / 2 * (BMAXR / 4) + NT - 1) / NT;
+    const int I = t.dims[0], J = t.dims[1], K = t.dims[2], R = t.R;
+    const int ld = I + 1;
+    const float *X = a.X + t.xoff;
+    const int Q = t.dims[mode];
+    const int rows = (mode == 0) ? I : J;
+    const int npair = (rows + 1) / 2;
+    const int rq = (R + 3) / 4;
+    const int items = npair * rq;
+    float acc[IPB][2][4];
+#pragma unroll
+    for (int u = 0; u < IPB; u++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) { acc[u][0][c] = 0.f; acc[u][1][c] = 0.f; }
+    for (int k = 0; k < K; k++) {
+        __syncthreads();
+        const float *src = X + (long)k * I * J;
+        for (int e = threadIdx.x; e < I * J; e += NT) {
+            const int i = e % I, j = e / I;
+            sm.slice[i + ld * j] = src[e];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < IPB; u++) {
+            const int it = threadIdx.x + NT * u;
+            if (it >= items) continue;
+            const int rp = (it % npair) * 2;
+            const int r0 = (it / npair) * 4;
+            float t2[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+            if (mode == 0) {
+                // T[i, r] = sum_j X[i, j] B[j, r]
+                const float *Bf = sm.F[1];
+                for (int j = 0; j < J; j++) {
+                    const float x0 = sm.slice[rp + ld * j];
+                    const float x1 = (rp + 1 < I) ? sm.slice[rp + 1 + ld * j] : 0.f;
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int r = r0 + c;
+                        const float b = (r < R) ? Bf[j + J * r] : 0.f;
+                        t2[0][c] = fmaf(x0, b, t2[0][c]);
+                        t2[1][c] = fmaf(x1, b, t2[1][c]);
+                    }
+                }
+            } else {
+                // T[j, r] = sum_i X[i, j] A[i, r]
+                const float *Af = sm.F[0];
+                for (int i = 0; i < I; i++) {
+                    const float x0 = sm.slice[i + ld * rp];
+                    const float x1 = (rp + 1 < J) ? sm.slice[i + ld * (rp + 1)] : 0.f;
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int r = r0 + c;
+                        const float av = (r < R) ? Af[i + I * r] : 0.f;
+                        t2[0][c] = fmaf(x0, av, t2[0][c]);
+                        t2[1][c] = fmaf(x1, av, t2[1][c]);
+                    }
+                }
+            }
+            if (mode < 2) {
+                const float *Cf = sm.F[2];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int r = r0 + c;
+                    const float w = (r < R) ? Cf[k + K * r] : 0.f;
+                    acc[u][0][c] = fmaf(t2[0][c], w, acc[u][0][c]);
+                    acc[u][1][c] = fmaf(t2[1][c], w, acc[u][1][c]);
+                }
+            } else {
+                // this pair's share of M[k, r] = sum_j T[j, r] B[j, r]
+                const float *Bf = sm.F[1];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int r = r0 + c;
+                    float v = 0.f;
+                    if (r < R) {
+                        v = t2[0][c] * Bf[rp + J * r];
+                        if (rp + 1 < J) v = fmaf(t2[1][c], Bf[rp + 1 + J * r], v);
+                    }
+                    sm.red3[(r0 + c) * (BMAXD / 2) + rp / 2] = v;
+                }
+            }
+        }
+        if (mode == 2) {
+            // fixed-order sum over the row pairs (deterministic)
+            __syncthreads();
+            for (int r = threadIdx.x; r < R; r += NT) {
+                float v = 0.f;
+                for (int p2 = 0; p2 < npair; p2++) v += sm.red3[r * (BMAXD / 2) + p2];
+                sm.M[k + K * r] = v;
+            }
+        }
+    }
+    if (mode < 2) {
+#pragma unroll
+        for (int u = 0; u < IPB; u++) {
+            const int it = threadIdx.x + NT * u;
+            if (it >= items) continue;
+            const int rp = (it % npair) * 2;
+            const int r0 = (it / npair) * 4;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int r = r0 + c;
+                if (r < R) {
+                    sm.M[rp + Q * r] = acc[u][0][c];
+                    if (rp + 1 < Q) sm.M[rp + 1 + Q * r] = acc[u][1][c];
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// V = Hadamard of the Grams other than `mode`; V <- V^-1 (Gauss-Jordan).
+// Leaves sm.fail set when both attempts met a non-positive pivot (V is then
+// not an inverse and the caller keeps the old factor).
+template <int NT>
+__device__ void normal_inverse_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
+    const int R = t.R;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        for (int e = threadIdx.x; e < R * R; e += NT) {
+            double v = 1.0;
+            for (int m = 0; m < 3; m++)
+                if (m != mode) v *= t.G[m][e];
+            sm.V[e] = v;
+        }
+        if (threadIdx.x == 0) sm.fail = 0;
+        __syncthreads();
+        double maxdiag = 0.0;
+        for (int j = 0; j < R; j++) maxdiag = fmax(maxdiag, fabs(sm.V[j + R * j]));
+        if (attempt == 1) {
+            __syncthreads();
+            for (int j = threadIdx.x; j < R; j += NT) sm.V[j + R * j] += 1e-10 * maxdiag + 1e-300;
+            __syncthreads();
+        }
+        for (int k = 0; k < R; k++) {
+            const double piv = sm.V[k + R * k];
+            if (!(piv > 1e-14 * maxdiag) || !isfinite(piv)) {
+                if (threadIdx.x == 0) sm.fail = 1;
+                break;
+            }
+            const double inv = 1.0 / piv;
+            for (int j = threadIdx.x; j < R; j += NT) {
+                sm.rowk[j] = (j == k ? 1.0 : sm.V[k + R * j]) * inv;
+                sm.colk[j] = sm.V[j + R * k];
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < R * R; e += NT) {
+                const int i = e % R, j = e / R;
+                const double old = (j == k) ? 0.0 : sm.V[e];
+                sm.V[e] = (i == k) ? sm.rowk[j] : old - sm.colk[i] * sm.rowk[j];
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+        if (!sm.fail) return;
+        if (threadIdx.x == 0 && attempt == 0) atomicAdd(a.fallbacks, 1);
+        __syncthreads();
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_batch_sweep(BatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BatchSmem &sm = *reinterpret_cast<BatchSmem *>(smem_raw);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            unsigned w = atomicAdd(a.queue, 1u);
+            sm.tensor = (w < (unsigned)a.ntensors) ? a.order[w] : -1;
+        }
+        __syncthreads();
+        const int ti = sm.tensor;
+        __syncthreads();
+        if (ti < 0) return;
+        TensorMeta &t = a.meta[ti];
+        if (t.done) continue;
+        const int R = t.R;
+        load_factors<NT>(sm, a, t);
+        __syncthreads();
+        double inner = 0.0;
+        for (int mode = 0; mode < 3; mode++) {
+            mttkrp_small<NT>(sm, a, t, mode);
+            normal_inverse_small<NT>(sm, a, t, mode);
+            // U_mode = M V^-1 (FP64 accumulation), into shared and global memory
+            const int Q = t.dims[mode];
+            float *Ug = a.U + t.uoff[mode];
+            const bool keep = sm.fail != 0;  // singular twice: keep the old factor
+            double part = 0.0;
+            for (int e = threadIdx.x; e < Q * R; e += NT) {
+                const int q = e % Q, c = e / Q;
+                float u = sm.F[mode][e];
+                if (!keep) {
+                    double s = 0.0;
+                    for (int r = 0; r < R; r++) s = fma((double)sm.M[q + Q * r], sm.V[r + R * c], s);
+                    u = (float)s;
+                    sm.F[mode][e] = u;
+                    Ug[e] = u;
+                }
+                if (mode == 2) part += (double)sm.M[e] * (double)u;
+            }
+            __syncthreads();
+            // Gram of the new factor
+            for (int e = threadIdx.x; e < R * R; e += NT) {
+                const int p = e % R, q2 = e / R;
+                double s = 0.0;
+                for (int i = 0; i < Q; i++) s = fma((double)sm.F[mode][i + Q * p], (double)sm.F[mode][i + Q * q2], s);
+                t.G[mode][e] = s;
+            }
+            if (mode == 2) {
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = part;
+            }
+            __syncthreads();
+            if (mode == 2 && threadIdx.x == 0) {
+                for (int w = 0; w < NT / 32; w++) inner += sm.red[w];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double hat = 0.0;
+            for (int e = 0; e < R * R; e++) hat += t.G[0][e] * t.G[1][e] * t.G[2][e];
+            const double res2 = t.normx2 - 2.0 * inner + hat;
+            const double fit = 1.0 - sqrt(res2 > 0.0 ? res2 : 0.0) / sqrt(t.normx2);
+            t.fit_prev = t.fit;
+            t.fit = fit;
+            t.sweeps += 1;
+            if ((a.tol > 0 && t.sweeps >= 2 && fabs(t.fit - t.fit_prev) < a.tol) || t.sweeps >= a.max_sweeps) {
+                t.done = 1;
+                atomicAdd(a.ndone, 1);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Per-tensor ||X||^2 and the initial Grams.
+__global__ void __launch_bounds__(256) k_batch_setup(TensorMeta *meta, int ntensors, const float *X,
+                                                     const float *U) {
+    __shared__ double red[8];
+    for (int ti = blockIdx.x; ti < ntensors; ti += gridDim.x) {
+        TensorMeta &t = meta[ti];
+        const long n = (long)t.dims[0] * t.dims[1] * t.dims[2];
+        double s = 0.0;
+        for (long e = threadIdx.x; e < n; e += 256) {
+            const double x = X[t.xoff + e];
+            s += x * x;
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < 8; w++) tot += red[w];
+            t.normx2 = tot;
+            t.fit = 0.0;
+            t.fit_prev = 0.0;
+            t.sweeps = 0;
+            t.done = 0;
+        }
+        const int R = t.R;
+        for (int m = 0; m < 3; m++) {
+            const float *F = U + t.uoff[m];
+            const int I = t.dims[m];
+            for (int e = threadIdx.x; e < R * R; e += 256) {
+                const int p = e % R, q = e / R;
+                double g = 0.0;
+                for (int i = 0; i < I; i++) g = fma((double)F[i + I * p], (double)F[i + I * q], g);
+                t.G[m][e] = g;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+struct BatchState {
+    TensorMeta *meta = nullptr;
+    int *order = nullptr;
+    unsigned *queue = nullptr;
+    int *fallbacks = nullptr;
+};
+
+template <int NT>
+int launch_sweep(const BatchArgs &a, int ctas_per_sm, cudaStream_t s) {
+    static bool attr[64] = {false};
+    int dev = 0;
+    CUD_CHECK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !attr[dev]) {
+        CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(BatchSmem)));
+        attr[dev] = true;
+    }
+    CUD_CHECK(cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s));
+    k_batch_sweep<NT><<<kNumSMs * ctas_per_sm, NT, sizeof(BatchSmem), s>>>(a);
+    CUD_CHECK_LAUNCH("batched sweep");
+    return CUD_OK;
+}
+
+int launch_cfg(const BatchArgs &a, int threads, int ctas_per_sm, cudaStream_t s) {
+    return threads == 128 ? launch_sweep<128>(a, ctas_per_sm, s) : launch_sweep<256>(a, ctas_per_sm, s);
+}
+
+// Autotuner cache: shape class -> (threads, CTAs per SM)
+std::mutex g_tune_mu;
+std::map<long, std::pair<int, int>> g_tune;
+
+long shape_class(int n, const int *dims, const int *ranks) {
+    // bucket the mean element count and mean rank; plus the batch size order
+    double e = 0.0, r = 0.0;
+    for (int t = 0; t < n; t++) {
+        e += (double)dims[3 * t] * dims[3 * t + 1] * dims[3 * t + 2];
+        r += ranks[t];
+    }
+    e /= std::max(1, n);
+    r /= std::max(1, n);
+    long eb = (long)log2(std::max(1.0, e)), rb = (long)r / 4, nb = (long)log2(std::max(1, n));
+    return eb * 10000 + rb * 100 + nb;
+}
+
+}  // namespace
+
+}  // namespace cud
+
+using namespace cud;
+
+extern "C" int cud_cp_als_batched(int ntensors, const long *dims, const long *ranks, const float *X,
+                                  const long *x_offsets, float *U, const long *u_offsets,
+                                  const cud_cp_options *opt_in, double *fits, int *sweeps,
+                                  int *kernel_launches, void *stream) {
+    if (ntensors <= 0 || !dims || !ranks || !X || !x_offsets || !U || !u_offsets)
+        return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cud_cp_options opt;
+    cud_cp_default_options(&opt);
+    if (opt_in) opt = *opt_in;
+    if (opt.max_sweeps < 1) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    cudaStream_t s = as_stream(stream);
+    std::vector<TensorMeta> hm(ntensors);
+    std::vector<int> hd(3 * ntensors), hr(ntensors);
+    std::vector<std::pair<double, int>> work(ntensors);
+    for (int t = 0; t < ntensors; t++) {
+        TensorMeta &m = hm[t];
+        memset(&m, 0, sizeof(TensorMeta));
+        for (int k = 0; k < 3; k++) {
+            if (dims[3 * t + k] < 1 || dims[3 * t + k] > BMAXD) return set_status(CUD_ERR_UNSUPPORTED);
+            m.dims[k] = (int)dims[3 * t + k];
+            m.uoff[k] = u_offsets[3 * t + k];
+            hd[3 * t + k] = m.dims[k];
+        }
+        if (ranks[t] < 1 || ranks[t] > BMAXR) return set_status(CUD_ERR_UNSUPPORTED);
+        m.R = (int)ranks[t];
+        hr[t] = m.R;
+        m.xoff = x_offsets[t];
+        work[t] = {-(double)m.dims[0] * m.dims[1] * m.dims[2] * m.R, t};
+    }
+    std::sort(work.begin(), work.end());
+    std::vector<int> order(ntensors);
+    for (int t = 0; t < ntensors; t++) order[t] = work[t].second;
+
+    int st;
+    size_t bytes = sizeof(TensorMeta) * ntensors + sizeof(int) * ntensors + 256;
+    char *w = (char *)scratch(kSlotTmp1, bytes, &st);
+    if (!w) return set_status(st);
+    BatchArgs a;
+    a.meta = reinterpret_cast<TensorMeta *>(w);
+    a.order = reinterpret_cast<int *>(w + sizeof(TensorMeta) * ntensors);
+    a.queue = reinterpret_cast<unsigned *>(w + sizeof(TensorMeta) * ntensors + sizeof(int) * ntensors);
+    a.fallbacks = reinterpret_cast<int *>(a.queue + 16);
+    a.ndone = reinterpret_cast<int *>(a.queue + 32);
+    a.ntensors = ntensors;
+    a.X = X;
+    a.U = U;
+    a.max_sweeps = opt.max_sweeps;
+    a.tol = opt.tol;
+    CUD_CHECK(cudaMemcpyAsync(a.meta, hm.data(), sizeof(TensorMeta) * ntensors, cudaMemcpyHostToDevice, s));
+    CUD_CHECK(cudaMemcpyAsync(const_cast<int *>(a.order), order.data(), sizeof(int) * ntensors,
+                              cudaMemcpyHostToDevice, s));
+    CUD_CHECK(cudaMemsetAsync(a.queue, 0, 256, s));
+    k_batch_setup<<<std::min(ntensors, kNumSMs * 4), 256, 0, s>>>(a.meta, ntensors, X, U);
+    CUD_CHECK_LAUNCH("batched setup");
+
+    // tile shape from the autotuner (threads per CTA, CTAs per SM)
+    long key = shape_class(ntensors, hd.data(), hr.data());
+    std::pair<int, int> cfg(256, 2);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) cfg = it->second;
+    }
+    // sweeps: graph of `per` sweeps replayed; the done-count read back between
+    const int per = std::max(1, std::min(opt.check_every > 1 ? opt.check_every : 5, opt.max_sweeps));
+    cudaStream_t cs = s;
+    bool own = false;
+    if (s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
+        CUD_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        own = true;
+        CUD_CHECK(cudaStreamSynchronize(s));
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    st = CUD_OK;
+    if (opt.use_graph) {
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) st = CUD_ERR_CUDA;
+        for (int i = 0; i < per && st == CUD_OK; i++) st = launch_cfg(a, cfg.first, cfg.second, cs);
+        cudaError_t e = cudaStreamEndCapture(cs, &graph);
+        if (st == CUD_OK && e != cudaSuccess) st = cuda_status(e, "batched capture");
+        if (st == CUD_OK) {
+            e = cudaGraphInstantiate(&exec, graph, 0);
+            if (e != cudaSuccess) st = cuda_status(e, "batched instantiate");
+        }
+    }
+    int launched = 0, done_sweeps = 0;
+    double *hs = pinned_scalars();  // slot 63: the converged count
+    int *ndone_h = hs ? reinterpret_cast<int *>(hs + 63) : nullptr;
+    while (st == CUD_OK && done_sweeps < opt.max_sweeps) {
+        if (exec) {
+            if (cudaGraphLaunch(exec, cs) != cudaSuccess) { st = CUD_ERR_CUDA; break; }
+        } else {
+            for (int i = 0; i < per && st == CUD_OK; i++) st = launch_cfg(a, cfg.first, cfg.second, cs);
+        }
+        launched += per;
+        done_sweeps += per;
+        // convergence check: the count of converged tensors (4 bytes)
+        if (!ndone_h || cudaMemcpyAsync(ndone_h, a.ndone, sizeof(int), cudaMemcpyDeviceToHost, cs) != cudaSuccess ||
+            cudaStreamSynchronize(cs) != cudaSuccess) { st = CUD_ERR_CUDA; break; }
+        if (*ndone_h >= ntensors) break;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    std::vector<TensorMeta> out;
+    if (st == CUD_OK && (fits || sweeps)) {
+        out.resize(ntensors);
+        if (cudaMemcpyAsync(out.data(), a.meta, sizeof(TensorMeta) * ntensors, cudaMemcpyDeviceToHost, cs) != cudaSuccess ||
+            cudaStreamSynchronize(cs) != cudaSuccess)
+            st = CUD_ERR_CUDA;
+    }
+    if (st == CUD_OK) {
+        for (int t = 0; t < ntensors; t++) {
+            if (fits) fits[t] = out[t].fit;
+            if (sweeps) sweeps[t] = out[t].sweeps;
+        }
+        if (kernel_launches) *kernel_launches = launched;
+    }
+    if (own) {
+        cudaStreamSynchronize(cs);
+        cudaStreamDestroy(cs);
+    }
+    return set_status(st);
+}
+
+extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *ranks, const float *X,
+                                   const long *x_offsets, float *U_scratch, const long *u_offsets,
+                                   int *threads, int *ctas_per_sm, void *stream) {
+    if (ntensors <= 0 || !dims || !ranks) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    std::vector<int> hd(3 * ntensors), hr(ntensors);
+    for (int t = 0; t < ntensors; t++) {
+        for (int k = 0; k < 3; k++) hd[3 * t + k] = (int)dims[3 * t + k];
+        hr[t] = (int)ranks[t];
+    }
+    long key = shape_class(ntensors, hd.data(), hr.data());
+    const int cand[][2] = {{128, 2}, {128, 3}, {128, 4}, {256, 1}, {256, 2}, {256, 3}};
+    float best = 1e30f;
+    std::pair<int, int> bestc(256, 2);
+    cudaStream_t s = as_stream(stream);
+    cudaEvent_t e0, e1;
+    CUD_CHECK(cudaEventCreate(&e0));
+    CUD_CHECK(cudaEventCreate(&e1));
+    for (auto &c : cand) {
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune[key] = {c[0], c[1]};
+        }
+        cud_cp_options opt;
+        cud_cp_default_options(&opt);
+        opt.max_sweeps = 2;
+        opt.tol = 0.0;
+        opt.use_graph = 0;
+        opt.check_every = 2;
+        cudaEventRecord(e0, s);
+        int st = cud_cp_als_batched(ntensors, dims, ranks, X, x_offsets, U_scratch, u_offsets, &opt,
+                                    nullptr, nullptr, nullptr, stream);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return set_status(st); }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; bestc = {c[0], c[1]}; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = bestc;
+    }
+    if (threads) *threads = bestc.first;
+    if (ctas_per_sm) *ctas_per_sm = bestc.second;
+    return set_status(CUD_OK);
+}

@@ -380,6 +380,16 @@ extern "C" int cud_cp_plan_fit(cud_cp_plan p, double *fit, double *fit_prev, voi
     return set_status(CUD_OK);
 }
 
+extern "C" int cud_cp_plan_true_fit(cud_cp_plan p, double *fit, void *stream) {
+    if (!p) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    double res2 = 0.0, x2 = 0.0;
+    int st = cud_cp_residual(p->X, p->order, p->dims, const_cast<const float *const *>(p->U), p->R, &res2, &x2,
+                             stream);
+    if (st) return st;
+    if (fit) *fit = 1.0 - sqrt(res2) / sqrt(x2 > 0.0 ? x2 : 1.0);
+    return set_status(CUD_OK);
+}
+
 extern "C" int cud_cp_plan_info(cud_cp_plan p, int *kernels_per_sweep, int *fallbacks) {
     if (!p) return set_status(CUD_ERR_INVALID_ARGUMENT);
     if (kernels_per_sweep) *kernels_per_sweep = p->kernels_per_sweep;
@@ -403,7 +413,7 @@ extern "C" int cud_cp_als(const float *X, int order, const long *dims, long R, f
     st = ss.open(as_stream(stream));
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     int sweeps = 0;
-    double fit = 0.0, fit_prev = 0.0;
+    double fit = 0.0, fit_prev = 0.0, true_fit = 0.0;
     if (st == CUD_OK) {
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
@@ -417,17 +427,24 @@ extern "C" int cud_cp_als(const float *X, int order, const long *dims, long R, f
             if (st == CUD_OK && (opt.tol > 0 || opt.target_fit > 0)) {
                 st = cud_cp_plan_fit(p, &fit, &fit_prev, ss.s);
                 if (st == CUD_OK && opt.tol > 0 && sweeps >= 2 && fabs(fit - fit_prev) < opt.tol) break;
-                if (st == CUD_OK && opt.target_fit > 0 && fit >= opt.target_fit) break;
+                // the target is judged on the exact fit: the estimate's
+                // cancellation error can exceed the distance to the target
+                if (st == CUD_OK && opt.target_fit > 0) {
+                    st = cud_cp_plan_true_fit(p, &true_fit, ss.s);
+                    if (st == CUD_OK && true_fit >= opt.target_fit) break;
+                }
             }
         }
         cudaEventRecord(t1, ss.s);
         if (st == CUD_OK) st = cud_cp_plan_fit(p, &fit, &fit_prev, ss.s);
+        if (st == CUD_OK) st = cud_cp_plan_true_fit(p, &true_fit, ss.s);
     }
     if (st == CUD_OK && res) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, t0, t1);
         res->sweeps = sweeps;
-        res->fit = fit;
+        res->fit = true_fit;
+        res->fit_estimate = fit;
         res->fit_prev = fit_prev;
         res->seconds = ms * 1e-3;
         cud_cp_plan_info(p, &res->kernels_per_sweep, &res->fallbacks);

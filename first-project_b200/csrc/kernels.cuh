@@ -45,6 +45,12 @@ inline ModeView mode_view(int order, const long *dims, int mode) {
 
 constexpr int kMaxOrder = 8;
 
+// ||X - [[U]]||^2 and ||X||^2 into out2[0..1] (device, FP64), one pass
+// over X (residual.cu); ws holds cp_residual_ws_bytes.
+size_t cp_residual_ws_bytes(int order, const long *dims);
+int cp_residual(const float *X, int order, const long *dims, const float *const *U, long R, double *out2,
+                void *ws, cudaStream_t s);
+
 // Factor set for on-the-fly Khatri-Rao rows: up to kMaxOrder-1 factor
 // matrices (column-major rows x R) listed fastest-first.
 struct KrFactors {

@@ -24,10 +24,12 @@
 //     D += Xhi*KRhi + Xhi*KRlo + Xlo*KRhi  (BF16X3), or one product (BF16,
 //     FP16).
 // The tensor core's FP32 accumulation truncates, so long accumulation chains
-// drift low; the CTA's stage range is therefore cut into segments of F
+// drift low; the CTA's stage range is therefore cut into segments of SEG
 // stages, each accumulated in its own TMEM buffer (two, alternating), and
 // the A converters add each finished segment into the CTA's FP32 partial in
-// global memory with round-to-nearest adds.  A small second kernel sums the
+// global memory with round-to-nearest reductions (`red.add`, fire and
+// forget; each partial element has one owning thread, so the order of the
+// adds is fixed and the result deterministic).  A small second kernel sums the
 // partials over the contraction splits in FP64.  The unfolding and the KR
 // matrix are never materialised: X is read from HBM exactly once.
 //
@@ -47,7 +49,10 @@ namespace {
 constexpr int BQ = 128;          // rows per CTA tile (MMA M)
 constexpr int BKS = 32;          // contraction depth per stage (two MMA K-steps of 16)
 constexpr int NST = 4;           // pipeline stages
-constexpr int SEG = 16;          // stages per TMEM accumulation segment
+#ifndef CUD_TC_SEG
+#define CUD_TC_SEG 16
+#endif
+constexpr int SEG = CUD_TC_SEG;  // stages per TMEM accumulation segment
 constexpr int NTHREADS = 256;    // w0 TMA, w1 MMA, w2-5 A converters, w6-7 KR producers
 constexpr int NCONV = 128;       // A converter threads
 constexpr int NKR = 64;          // KR producer threads
@@ -137,13 +142,6 @@ __device__ __forceinline__ void kr_load(const TcArgs &a, const TcCtrl &sm, long 
     const long key = rest * 2147483647L + s;
     const bool refresh = (key != cache_key);
     cache_key = key;
-    long gidx[kMaxOrder], oidx[kMaxOrder];
-    if (refresh) {
-        long lin = rest;
-        for (int f = 1; f < ng; f++) { gidx[f] = lin % sm.grows[f]; lin /= sm.grows[f]; }
-        lin = s;
-        for (int f = 0; f < no; f++) { oidx[f] = lin % sm.orows[f]; lin /= sm.orows[f]; }
-    }
 #pragma unroll
     for (int it = 0; it < KIPT; it++) {
         const int id = kt + NKR * it;
@@ -154,10 +152,26 @@ __device__ __forceinline__ void kr_load(const TcArgs &a, const TcCtrl &sm, long 
         o.c[it] = 0.f;
         if (r >= a.R) continue;
         if (refresh) {
+            // the constant row: the digits of s over the outer factors and
+            // (fast path) of `rest` over the slower generating factors,
+            // recomputed per item so no index array lives in local memory
             float c = 1.f;
-            for (int f = 0; f < no; f++) c *= __ldg(sm.oU[f] + oidx[f] + r * sm.orows[f]);
-            if (a.fast)
-                for (int f = 1; f < ng; f++) c *= __ldg(sm.gU[f] + gidx[f] + r * sm.grows[f]);
+            long lin = s;
+            for (int f = 0; f < no; f++) {
+                const long d = sm.orows[f];
+                const long idx = lin % d;
+                lin /= d;
+                c *= __ldg(sm.oU[f] + idx + r * d);
+            }
+            if (a.fast) {
+                lin = rest;
+                for (int f = 1; f < ng; f++) {
+                    const long d = sm.grows[f];
+                    const long idx = lin % d;
+                    lin /= d;
+                    c *= __ldg(sm.gU[f] + idx + r * d);
+                }
+            }
             cc[it] = c;
         }
         o.c[it] = cc[it];
@@ -316,18 +330,20 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             if (ok) {
                 ptx::tc_fence_after();
                 const uint32_t d = tbase + lane_off + (uint32_t)b * (uint32_t)a.Rpad;
-                for (int c0 = 0; c0 < a.Rpad; c0 += 16) {
-                    uint32_t v[16];
-                    ptx::tmem_ld16(d + (uint32_t)c0, v);
+                for (int c0 = 0; c0 < a.Rpad; c0 += 32) {
+                    uint32_t v[2][16];
+                    const bool two = c0 + 16 < a.Rpad;  // warp-uniform
+                    ptx::tmem_ld16(d + (uint32_t)c0, v[0]);
+                    if (two) ptx::tmem_ld16(d + (uint32_t)c0 + 16u, v[1]);
                     ptx::tmem_wait_ld();
                     if (q < a.Q) {
+                        float *p = P + q + a.Q * c0;
 #pragma unroll
-                        for (int j = 0; j < 16; j++) {
-                            const int r = c0 + j;
-                            if (r < a.R) {
-                                float *p = P + q + a.Q * r;
-                                float val = __uint_as_float(v[j]);
-                                *p = (seg == 0) ? val : __fadd_rn(*p, val);
+                        for (int j = 0; j < 32; j++) {
+                            if (c0 + j < a.R) {
+                                const float val = __uint_as_float(v[j >> 4][j & 15]);
+                                if (seg == 0) p[a.Q * j] = val;
+                                else atomicAdd(p + a.Q * j, val);  // red.global.add.f32, RN
                             }
                         }
                     }

@@ -22,7 +22,7 @@ from typing import Sequence
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libcudecompose_b200.so")
+LIB_PATH = os.environ.get("CUDECOMPOSE_B200_LIB") or os.path.join(_HERE, "libcudecompose_b200.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
@@ -62,7 +62,8 @@ class CpOptions(ctypes.Structure):
 
 class CpResult(ctypes.Structure):
     _fields_ = [("sweeps", _i), ("fallbacks", _i), ("fit", _d),
-                ("fit_prev", _d), ("seconds", _d), ("kernels_per_sweep", _i)]
+                ("fit_prev", _d), ("seconds", _d), ("kernels_per_sweep", _i),
+                ("fit_estimate", _d)]
 
 
 def _sig(name, argtypes, restype=_i):
@@ -106,8 +107,16 @@ _sig("cud_cp_plan_create", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp)
                             ctypes.POINTER(CpOptions), _vp, ctypes.POINTER(_vp)])
 _sig("cud_cp_plan_run", [_vp, _i, _vp])
 _sig("cud_cp_plan_fit", [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), _vp])
+_sig("cud_cp_plan_true_fit", [_vp, ctypes.POINTER(_d), _vp])
 _sig("cud_cp_plan_info", [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)])
+_sig("cud_cp_residual", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _l, ctypes.POINTER(_d),
+                         ctypes.POINTER(_d), _vp])
 _sig("cud_cp_plan_destroy", [_vp])
+_sig("cud_cp_als_batched", [_i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ctypes.POINTER(_l), _vp,
+                            ctypes.POINTER(_l), ctypes.POINTER(CpOptions), ctypes.POINTER(_d),
+                            ctypes.POINTER(_i), ctypes.POINTER(_i), _vp])
+_sig("cud_cp_batched_tune", [_i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ctypes.POINTER(_l), _vp,
+                             ctypes.POINTER(_l), ctypes.POINTER(_i), ctypes.POINTER(_i), _vp])
 _sig("cud_factor_gram", [_vp, _l, _l, _vp, _vp])
 _sig("cud_cp_solve", [_vp, _l, _l, _i, ctypes.POINTER(_vp), _i, _vp, _vp, _vp])
 _sig("cud_cp_fit_terms", [_vp, _vp, _l, _i, ctypes.POINTER(_vp), _l, ctypes.POINTER(_d),
@@ -320,6 +329,12 @@ class CpPlan:
                "cp_plan_fit")
         return f.value, fp.value
 
+    def true_fit(self, stream=None):
+        """Exact fit of the current factors (cud_cp_plan_true_fit)."""
+        f = _d(0.0)
+        _check(_lib.cud_cp_plan_true_fit(self._h, ctypes.byref(f), _stream(stream)), "cp_plan_true_fit")
+        return f.value
+
     def info(self):
         k, fb = _i(0), _i(0)
         _check(_lib.cud_cp_plan_info(self._h, ctypes.byref(k), ctypes.byref(fb)), "cp_plan_info")
@@ -335,6 +350,20 @@ class CpPlan:
             self.close()
         except Exception:
             pass
+
+
+def cp_residual(X, dims, factors, R, stream=None):
+    """(||X - [[factors]]||^2, ||X||^2) in FP64 (src/rse.cu:4 + gencp)."""
+    r2, x2 = _d(0.0), _d(0.0)
+    _check(_lib.cud_cp_residual(_ptr(X), len(dims), _longs(dims), _ptrs(factors), R,
+                                ctypes.byref(r2), ctypes.byref(x2), _stream(stream)), "cp_residual")
+    return r2.value, x2.value
+
+
+def cp_true_fit(X, dims, factors, R, stream=None):
+    """1 - ||X - [[factors]]|| / ||X||, from cp_residual."""
+    r2, x2 = cp_residual(X, dims, factors, R, stream)
+    return 1.0 - (r2 ** 0.5) / (x2 ** 0.5 if x2 > 0 else 1.0)
 
 
 def factor_gram(U, I, R, G, stream=None):
@@ -356,6 +385,64 @@ def cp_fit_terms(M, U, grams, R, stream=None):
                                  ctypes.byref(inner), ctypes.byref(nh), _stream(stream)),
            "cp_fit_terms")
     return inner.value, nh.value
+
+
+class Batch:
+    """A packed batch of small 3rd-order tensors for cp_als_batched: X and
+    all factors in two device buffers, with per-tensor offsets (16-byte
+    aligned)."""
+
+    def __init__(self, dims, ranks, device="cuda"):
+        self.dims = [tuple(int(x) for x in d) for d in dims]
+        self.ranks = [int(r) for r in ranks]
+        self.n = len(self.dims)
+        xo, uo, xs, us = [], [], 0, 0
+        for d, r in zip(self.dims, self.ranks):
+            xo.append(xs)
+            xs += (d[0] * d[1] * d[2] + 3) // 4 * 4
+            for m in range(3):
+                uo.append(us)
+                us += (d[m] * r + 3) // 4 * 4
+        self.x_offsets, self.u_offsets = xo, uo
+        self.X = torch.zeros(max(xs, 4), device=device)
+        self.U = torch.zeros(max(us, 4), device=device)
+
+    def x_view(self, t):
+        d = self.dims[t]
+        return self.X[self.x_offsets[t]: self.x_offsets[t] + d[0] * d[1] * d[2]]
+
+    def u_view(self, t, m):
+        o = self.u_offsets[3 * t + m]
+        return self.U[o: o + self.dims[t][m] * self.ranks[t]]
+
+    def _args(self):
+        flat = [x for d in self.dims for x in d]
+        return (_longs(flat), _longs(self.ranks), _longs(self.x_offsets), _longs(self.u_offsets))
+
+
+def cp_als_batched(batch, max_sweeps=50, tol=1e-6, use_graph=True, sweeps_per_graph=5, stream=None):
+    """Batched CP-ALS (one persistent kernel per sweep).  Returns (fits,
+    sweeps, kernel_launches) per tensor; the factors in batch.U are updated."""
+    d, r, xo, uo = batch._args()
+    opt = CpOptions(max_sweeps, tol, PREC_FP32, 1 if use_graph else 0, sweeps_per_graph, 0.0)
+    fits = (_d * batch.n)()
+    sw = (_i * batch.n)()
+    launches = _i(0)
+    _check(_lib.cud_cp_als_batched(batch.n, d, r, _ptr(batch.X), xo, _ptr(batch.U), uo,
+                                   ctypes.byref(opt), fits, sw, ctypes.byref(launches),
+                                   _stream(stream)), "cp_als_batched")
+    return list(fits), list(sw), launches.value
+
+
+def cp_batched_tune(batch, stream=None):
+    """Autotunes the batched sweep's launch shape; returns (threads, ctas_per_sm)."""
+    d, r, xo, uo = batch._args()
+    Ucopy = batch.U.clone()
+    th, cps = _i(0), _i(0)
+    _check(_lib.cud_cp_batched_tune(batch.n, d, r, _ptr(batch.X), xo, _ptr(Ucopy), uo,
+                                    ctypes.byref(th), ctypes.byref(cps), _stream(stream)),
+           "cp_batched_tune")
+    return th.value, cps.value
 
 
 def cp_init_curand(dims, R, factors, seed=1234, stream=None):

@@ -10,7 +10,7 @@ mode n:
   * n = N-1: the MTTKRP rows are local; each rank solves its own rows and
     the Gram of the last factor is all-reduced.
 The fit needs <M_{N-1}, U_{N-1}> (all-reduced) and the Grams.  The collective
-is a real exchange of I_n x R partial sums (SURVEY §8e); nothing else moves.
+is a real exchange of I_n x R partial sums; nothing else moves.
 
 The sweep logic is backend-neutral: `ops` supplies the per-rank compute
 (the CUDA library for GPUs, see CudaOps) and `comm` the all-reduce

@@ -172,16 +172,21 @@ typedef struct cud_cp_options {
     int precision;    /* cud_precision of the MTTKRPs                          */
     int use_graph;    /* capture each sweep in a CUDA graph                    */
     int check_every;  /* read the fit back every this many sweeps (>= 1)       */
-    double target_fit; /* also stop once fit >= target_fit (<= 0 disables)     */
+    double target_fit; /* also stop once the exact fit >= target_fit, checked */
+                       /* every check_every sweeps (<= 0 disables)            */
 } cud_cp_options;
 
 typedef struct cud_cp_result {
     int sweeps;       /* sweeps run                                           */
     int fallbacks;    /* normal-equation solves that fell back to pinv        */
-    double fit;       /* 1 - ||X - Xhat|| / ||X|| after the last sweep         */
-    double fit_prev;  /* fit one sweep earlier                                 */
+    double fit;       /* 1 - ||X - Xhat|| / ||X|| of the returned factors,     */
+                      /* exact (cud_cp_residual, src/rse.cu:4)                 */
+    double fit_prev;  /* sweep estimate of the fit one sweep earlier           */
     double seconds;   /* wall time of the sweeps on the stream                 */
     int kernels_per_sweep; /* kernel launches in one sweep (graph kernel nodes) */
+    double fit_estimate; /* the last sweep's estimate ||X||^2 - 2<M,U> + ||Xhat||^2 */
+                      /* (cheap, but it cancels when fit -> 1 and inherits the */
+                      /* MTTKRP's rounding)                                    */
 } cud_cp_result;
 
 /* Extension: default options (500 sweeps, tol 0, CUD_PREC_DEFAULT, graph on). */
@@ -226,6 +231,40 @@ int cud_cp_solve(const float *M, long I, long R, int order, const double *const 
  * norm_hat2 = sum_{r,s} prod_m G[m][r,s]. */
 int cud_cp_fit_terms(const float *M, const float *U, long IR, int order, const double *const *G,
                      long R, double *inner, double *norm_hat2, void *stream);
+
+/* Extension (the reference runs one tensor per cp_als call,
+ * src/cp_als.cu:3): CP-ALS of `ntensors` independent 3rd-order tensors
+ * in one persistent kernel launch per sweep.  Tensor t is dims[3t..3t+2]
+ * (each in [1, 96]) of rank ranks[t] (in [1, 16]), stored column-major at
+ * X + x_offsets[t]; its factor m is dims[3t+m] x ranks[t] at
+ * U + u_offsets[3t+m] (initial values in, result out).  opt: max_sweeps, tol
+ * (per tensor), use_graph, check_every (= sweeps per captured graph).
+ * fits / sweeps (host arrays of ntensors, may be NULL) receive each tensor's
+ * final fit and sweep count; kernel_launches (may be NULL) the number of
+ * sweep kernels launched. */
+int cud_cp_als_batched(int ntensors, const long *dims, const long *ranks, const float *X,
+                       const long *x_offsets, float *U, const long *u_offsets,
+                       const cud_cp_options *opt, double *fits, int *sweeps, int *kernel_launches,
+                       void *stream);
+
+/* Extension: autotunes the batched sweep's launch shape (threads per CTA,
+ * CTAs per SM) for this batch's shape class by timing two sweeps per
+ * candidate; U_scratch is a copy of the factors (overwritten).  The choice
+ * is cached per shape class and used by later cud_cp_als_batched calls. */
+int cud_cp_batched_tune(int ntensors, const long *dims, const long *ranks, const float *X,
+                        const long *x_offsets, float *U_scratch, const long *u_offsets, int *threads,
+                        int *ctas_per_sm, void *stream);
+
+/* src/rse.cu:4-29 (gencp + rse, called from src/cp_als.cu:104-111): the
+ * CP model's residual ||X - [[U_0..U_{order-1}]]||^2 and ||X||^2 (FP64, host
+ * outputs; synchronous), computed in one pass over X without materialising
+ * the reconstruction.  fit = 1 - sqrt(res_norm2 / x_norm2). */
+int cud_cp_residual(const float *X, int order, const long *dims, const float *const *U, long R,
+                    double *res_norm2, double *x_norm2, void *stream);
+
+/* Extension: the exact fit (cud_cp_residual) of the plan's current factors,
+ * independent of the fit estimate the sweep derives from its last MTTKRP. */
+int cud_cp_plan_true_fit(cud_cp_plan plan, double *fit, void *stream);
 
 /* src/cp_als.cu:20-24: the reference's initialisation -- cuRAND default
  * pseudo-random generator, seed 1234, uniform [0,1) into U[1], then U[2], ...

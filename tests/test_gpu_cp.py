@@ -105,3 +105,35 @@ def test_fit_matches_reconstruction(cd):
     Xd = dev_t(X)
     direct = 1.0 - torch.linalg.norm((Xd - rec).double()) / torch.linalg.norm(Xd.double())
     assert abs(res.fit - float(direct)) <= 1e-5
+
+
+@pytest.mark.parametrize("dims,R", [((20, 16, 12), 3), ((37, 23, 11), 70), ((6, 5, 4, 7), 3),
+                                    ((130, 9, 5), 129)])
+def test_cp_residual_matches_reconstruction(cd, dims, R):
+    """src/rse.cu:4 (norm of X - gencp(U)) against an FP64 reconstruction;
+    ranks above 64 take the multi-pass branch, mode 0 above 64 several
+    row tiles."""
+    rng = np.random.default_rng(len(dims) * 100 + R)
+    X = rng.random(int(np.prod(dims))).astype(np.float32)
+    facs = [rng.random(d * R).astype(np.float32) for d in dims]
+    rec = oracle.gencp(dims, [f.astype(np.float64) for f in facs], R)
+    want_r2 = float(np.sum((X.astype(np.float64) - rec) ** 2))
+    want_x2 = float(np.sum(X.astype(np.float64) ** 2))
+    r2, x2 = cd.cp_residual(dev_t(X), dims, [dev_t(f) for f in facs], R)
+    assert abs(x2 - want_x2) <= 1e-12 * want_x2
+    assert abs(r2 - want_r2) <= 1e-5 * want_r2
+
+
+def test_plan_true_fit_matches_direct(cd):
+    dims, R = (40, 32, 24), 5
+    X, init = low_rank(dims, R, seed=41, noise=1e-2)
+    U = [dev_t(f) for f in init]
+    Xd = dev_t(X)
+    plan = cd.CpPlan(Xd, dims, R, U, precision=cd.PREC_FP32)
+    plan.run(15)
+    tf = plan.true_fit()
+    rec = torch.empty(int(np.prod(dims)), device="cuda")
+    cd.gencp(rec, U, dims, R)
+    direct = 1.0 - torch.linalg.norm((Xd - rec).double()) / torch.linalg.norm(Xd.double())
+    assert abs(tf - float(direct)) <= 1e-6
+    plan.close()
