@@ -45,6 +45,13 @@ inline ModeView mode_view(int order, const long *dims, int mode) {
 
 constexpr int kMaxOrder = 8;
 
+// BF16 tensor-core GEMM with fused epilogue (gemm_tc.cu); ws holds
+// gemm_tc_ws_bytes (split-contraction partials + error flag).
+using GemmEpi = cud_gemm_epilogue;
+size_t gemm_tc_ws_bytes(long M, long N, long K);
+int gemm_tc_bf16(const __nv_bfloat16 *A, long lda, const __nv_bfloat16 *B, long ldb, long M, long N, long K,
+                 const GemmEpi &e, void *ws, cudaStream_t s);
+
 // ||X - [[U]]||^2 and ||X||^2 into out2[0..1] (device, FP64), one pass
 // over X (residual.cu); ws holds cp_residual_ws_bytes.
 size_t cp_residual_ws_bytes(int order, const long *dims);

@@ -221,13 +221,15 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     if (threadIdx.x == 0) {
         for (int i = 0; i < NST; i++) {
             ptx::mbar_init(&sm.full_x[i], 1);
-            ptx::mbar_init(&sm.empty_x[i], NCONV);
-            ptx::mbar_init(&sm.full_a[i], NCONV + NKR);
+            // producer barriers count warps: lane 0 arrives for its warp
+            // after __syncwarp, so each stage costs 6 arrivals, not 192
+            ptx::mbar_init(&sm.empty_x[i], NCONV / 32);
+            ptx::mbar_init(&sm.full_a[i], (NCONV + NKR) / 32);
             ptx::mbar_init(&sm.empty_a[i], 1);
         }
         for (int b = 0; b < 2; b++) {
             ptx::mbar_init(&sm.d_full[b], 1);
-            ptx::mbar_init(&sm.d_free[b], NCONV);
+            ptx::mbar_init(&sm.d_free[b], NCONV / 32);
         }
         ptx::mbar_init(&sm.done, 1);
         sm.abort = 0;
@@ -350,7 +352,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
                 }
                 ptx::tc_fence_before();
             }
-            ptx::mbar_arrive(&sm.d_free[b]);
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.d_free[b]);
         };
         for (long i = 0; i < nst; i++) {
             const int slot = (int)(i % NST);
@@ -373,7 +376,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
                     x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
                 }
             }
-            ptx::mbar_arrive(&sm.empty_x[slot]);
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.empty_x[slot]);
             uint32_t hi[16], lo[16];
             if (f16) {
 #pragma unroll
@@ -390,7 +394,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             if (three) ptx::tmem_st16(ta + 16, lo);
             ptx::tmem_wait_st();
             ptx::tc_fence_before();
-            ptx::mbar_arrive(&sm.full_a[slot]);
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.full_a[slot]);
             // a segment just ended: drain the one before it (long finished)
             if ((i % SEG) == SEG - 1 && i / SEG >= 1) flush(flushed++);
         }
@@ -436,7 +441,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
                 *reinterpret_cast<uint4 *>(bh + off) = h;
             }
             ptx::fence_proxy_async_smem();  // generic-proxy B writes -> tensor core
-            ptx::mbar_arrive(&sm.full_a[slot]);
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.full_a[slot]);
         }
     }
 

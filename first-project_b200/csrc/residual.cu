@@ -4,12 +4,13 @@
 // The reference measures a CP model's error by reconstructing the full
 // tensor and taking the norm of the difference (src/rse.cu:4-15 with
 // gencp, src/rse.cu:17-29; the call sits in src/cp_als.cu:104-111).  Here
-// the reconstruction is formed tile by tile in registers: a CTA owns TI = 64
+// the reconstruction is formed tile by tile in registers: a CTA owns TI = 128
 // rows of mode 0 and walks chunks of TJ = 32 consecutive "rest" indices (the
 // other modes, mode 1 fastest).  Per chunk it builds the Khatri-Rao rows
-// W[r][j] = prod_{m>=1} U_m[digit_m(rest0 + j), r] in shared memory, each
-// thread forms 8 reconstructed entries xh = sum_r U_0[i, r] W[r][j] in FP32
-// and accumulates (x - xh)^2 and x^2 in FP64.  X is read once, coalesced
+// W[r][j] = prod_{m>=1} U_m[digit_m(rest0 + j), r] in shared memory (each
+// thread decomposes one rest index and fills 8 ranks of it), each thread
+// forms 2 x 8 reconstructed entries xh = sum_r U_0[i, r] W[r][j] in FP32 and
+// accumulates (x - xh)^2 and x^2 in FP64.  X is read once, coalesced
 // along mode 0.  Per-CTA partials are summed in a fixed order by a second
 // kernel, so the result is deterministic.
 //
@@ -23,10 +24,10 @@ namespace cud {
 
 namespace {
 
-constexpr int TI = 64;      // mode-0 rows per CTA
+constexpr int TI = 128;     // mode-0 rows per CTA (two per thread)
 constexpr int TJ = 32;      // rest indices per chunk
 constexpr int RC = 64;      // ranks per shared-memory pass
-constexpr int NT = 256;     // TI x 4 lanes, each lane 8 rest indices
+constexpr int NT = 256;     // 64 row pairs x 4 lanes, each lane 8 rest indices
 
 struct ResArgs {
     const float *X;
@@ -53,9 +54,11 @@ __global__ void __launch_bounds__(NT) k_cp_residual(ResArgs a) {
         }
     }
     __syncthreads();
-    const int ti = threadIdx.x % TI;
-    const int rl = threadIdx.x / TI;  // 0..3, warp-uniform
-    const long i0 = blockIdx.x * (long)TI + ti;
+    const int ti = threadIdx.x % 64;  // rows ti and ti + 64 of the tile
+    const int rl = threadIdx.x / 64;  // 0..3, warp-uniform
+    const long i0 = blockIdx.x * (long)TI + ti, i1 = i0 + 64;
+    // KR-row builder role of this thread: rest index wj, ranks wg + 8t
+    const int wj = threadIdx.x % TJ, wg = threadIdx.x / TJ;
     const long nchunks = (a.rest + TJ - 1) / TJ;
     const bool one_pass = a.R <= RC;  // U_0's tile fits: load it once
     double acc = 0.0, xx = 0.0;
@@ -68,12 +71,33 @@ __global__ void __launch_bounds__(NT) k_cp_residual(ResArgs a) {
     }
     for (long ch = blockIdx.y; ch < nchunks; ch += gridDim.y) {
         const long rest0 = ch * TJ;
-        float x[8], xh[8];
+        float x0[8], x1[8], h0[8], h1[8];
 #pragma unroll
         for (int c = 0; c < 8; c++) {
             const long j = rest0 + rl * 8 + c;
-            x[c] = (i0 < a.I0 && j < a.rest) ? __ldcs(a.X + i0 + a.I0 * j) : 0.f;
-            xh[c] = 0.f;
+            const bool okj = j < a.rest;
+            x0[c] = (okj && i0 < a.I0) ? __ldcs(a.X + i0 + a.I0 * j) : 0.f;
+            x1[c] = (okj && i1 < a.I0) ? __ldcs(a.X + i1 + a.I0 * j) : 0.f;
+            h0[c] = 0.f;
+            h1[c] = 0.f;
+        }
+        // this thread's factor rows for rest index rest0 + wj (digits once)
+        const float *wb[kMaxOrder];
+        long ws[kMaxOrder];
+        const bool wok = rest0 + wj < a.rest;
+        {
+            long lin = rest0 + wj;
+#pragma unroll
+            for (int m = 0; m < kMaxOrder; m++) {
+                wb[m] = nullptr;
+                ws[m] = 0;
+                if (m < nf) {
+                    const long d = fRows[m];
+                    wb[m] = fU[m] + (lin % d);
+                    ws[m] = d;
+                    lin /= d;
+                }
+            }
         }
         for (long rc = 0; rc < a.R; rc += RC) {
             __syncthreads();
@@ -84,38 +108,39 @@ __global__ void __launch_bounds__(NT) k_cp_residual(ResArgs a) {
                     U0s[r][t] = (rc + r < a.R && i < a.I0) ? a.U0[i + a.I0 * (rc + r)] : 0.f;
                 }
             }
-            for (int e = threadIdx.x; e < RC * TJ; e += NT) {
-                const int r = e / TJ, j = e % TJ;
+#pragma unroll
+            for (int t = 0; t < RC / 8; t++) {
+                const int r = wg + 8 * t;
                 const long rr = rc + r;
                 float w = 0.f;
-                if (rr < a.R && rest0 + j < a.rest) {
+                if (wok && rr < a.R) {
                     w = 1.f;
-                    long lin = rest0 + j;
-                    for (int m = 0; m < nf; m++) {
-                        const long d = fRows[m];
-                        w *= __ldg(fU[m] + (lin % d) + d * rr);
-                        lin /= d;
-                    }
+#pragma unroll
+                    for (int m = 0; m < kMaxOrder; m++)
+                        if (m < nf) w *= __ldg(wb[m] + ws[m] * rr);
                 }
-                Ws[r][j] = w;
+                Ws[r][wj] = w;
             }
             __syncthreads();
-#pragma unroll 8
+#pragma unroll 4
             for (int r = 0; r < RC; r++) {
-                const float u = U0s[r][ti];
+                const float u0 = U0s[r][ti], u1 = U0s[r][ti + 64];
                 const float4 w0 = *reinterpret_cast<const float4 *>(&Ws[r][rl * 8]);
                 const float4 w1 = *reinterpret_cast<const float4 *>(&Ws[r][rl * 8 + 4]);
-                xh[0] = fmaf(u, w0.x, xh[0]); xh[1] = fmaf(u, w0.y, xh[1]);
-                xh[2] = fmaf(u, w0.z, xh[2]); xh[3] = fmaf(u, w0.w, xh[3]);
-                xh[4] = fmaf(u, w1.x, xh[4]); xh[5] = fmaf(u, w1.y, xh[5]);
-                xh[6] = fmaf(u, w1.z, xh[6]); xh[7] = fmaf(u, w1.w, xh[7]);
+                const float w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    h0[c] = fmaf(u0, w[c], h0[c]);
+                    h1[c] = fmaf(u1, w[c], h1[c]);
+                }
             }
         }
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-            const double d = (double)x[c] - (double)xh[c];
-            acc = fma(d, d, acc);
-            xx = fma((double)x[c], (double)x[c], xx);
+            const double d0 = (double)x0[c] - (double)h0[c];
+            const double d1 = (double)x1[c] - (double)h1[c];
+            acc = fma(d0, d0, fma(d1, d1, acc));
+            xx = fma((double)x0[c], (double)x0[c], fma((double)x1[c], (double)x1[c], xx));
         }
     }
     for (int o = 16; o > 0; o >>= 1) {

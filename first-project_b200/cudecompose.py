@@ -60,6 +60,14 @@ class CpOptions(ctypes.Structure):
                 ("use_graph", _i), ("check_every", _i), ("target_fit", _d)]
 
 
+class GemmEpilogue(ctypes.Structure):
+    _fields_ = [("alpha", ctypes.c_float), ("bias", _vp), ("relu", _i),
+                ("mask", _vp), ("mask_ldm", _l), ("mask_ldn", _l),
+                ("out_f32", _vp), ("f32_ldm", _l), ("f32_ldn", _l), ("f32_accumulate", _i),
+                ("out_bf16", _vp), ("bf16_ldm", _l), ("bf16_ldn", _l),
+                ("out_bf16_2", _vp), ("bf16_2_ldm", _l), ("bf16_2_ldn", _l)]
+
+
 class CpResult(ctypes.Structure):
     _fields_ = [("sweeps", _i), ("fallbacks", _i), ("fit", _d),
                 ("fit_prev", _d), ("seconds", _d), ("kernels_per_sweep", _i),
@@ -109,6 +117,7 @@ _sig("cud_cp_plan_run", [_vp, _i, _vp])
 _sig("cud_cp_plan_fit", [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), _vp])
 _sig("cud_cp_plan_true_fit", [_vp, ctypes.POINTER(_d), _vp])
 _sig("cud_cp_plan_info", [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)])
+_sig("cud_gemm_bf16", [_vp, _l, _vp, _l, _l, _l, _l, ctypes.POINTER(GemmEpilogue), _vp])
 _sig("cud_cp_residual", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _l, ctypes.POINTER(_d),
                          ctypes.POINTER(_d), _vp])
 _sig("cud_cp_plan_destroy", [_vp])
@@ -350,6 +359,46 @@ class CpPlan:
             self.close()
         except Exception:
             pass
+
+
+def _mat_strides(t):
+    """(ldm, ldn) of a 2-D tensor seen as out[m, n], or of out.T when
+    passed as ('T', tensor)."""
+    if isinstance(t, tuple):
+        _, t = t
+        return t, t.stride(1), t.stride(0)
+    return t, t.stride(0), t.stride(1)
+
+
+def gemm_bf16(A, B, alpha=1.0, bias=None, relu=False, mask=None, out_f32=None, accumulate=False,
+              out_bf16=None, out_bf16_2=None, stream=None):
+    """C[m, n] = epilogue(alpha * A[m, :] . B[n, :]) on the tensor cores
+    (cud_gemm_bf16).  A (M x K) and B (N x K) are contiguous BF16 tensors.
+    Each output / the mask is a 2-D tensor indexed [m, n], or ('T', t) for a
+    tensor indexed [n, m] (a transposed copy)."""
+    assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16
+    M, K = A.shape
+    N, K2 = B.shape
+    assert K == K2 and A.stride(1) == 1 and B.stride(1) == 1
+    e = GemmEpilogue()
+    e.alpha = alpha
+    e.bias = _ptr(bias) if bias is not None else None
+    e.relu = 1 if relu else 0
+    if mask is not None:
+        t, e.mask_ldm, e.mask_ldn = _mat_strides(mask)
+        e.mask = _ptr(t)
+    if out_f32 is not None:
+        t, e.f32_ldm, e.f32_ldn = _mat_strides(out_f32)
+        e.out_f32 = _ptr(t)
+        e.f32_accumulate = 1 if accumulate else 0
+    if out_bf16 is not None:
+        t, e.bf16_ldm, e.bf16_ldn = _mat_strides(out_bf16)
+        e.out_bf16 = _ptr(t)
+    if out_bf16_2 is not None:
+        t, e.bf16_2_ldm, e.bf16_2_ldn = _mat_strides(out_bf16_2)
+        e.out_bf16_2 = _ptr(t)
+    _check(_lib.cud_gemm_bf16(_ptr(A), A.stride(0), _ptr(B), B.stride(0), M, N, K, ctypes.byref(e),
+                              _stream(stream)), "gemm_bf16")
 
 
 def cp_residual(X, dims, factors, R, stream=None):

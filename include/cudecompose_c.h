@@ -255,6 +255,33 @@ int cud_cp_batched_tune(int ntensors, const long *dims, const long *ranks, const
                         const long *x_offsets, float *U_scratch, const long *u_offsets, int *threads,
                         int *ctas_per_sm, void *stream);
 
+/* Extension (the reference calls cublasGemmEx with FP16 operands,
+ * src/mttkrp.cu:40-72 and src/ttm.cu:20-39): BF16 tensor-core GEMM
+ *     C[m, n] = epilogue(alpha * sum_k A[m, k] * B[n, k])
+ * with A (M x K, row stride lda) and B (N x K, row stride ldb) BF16, K
+ * contiguous, lda and ldb multiples of 8, A and B 16-byte aligned; FP32
+ * accumulation.  The epilogue applies, in order: alpha, + bias[n], zero where
+ * mask[m, n] <= 0 (a BF16 matrix, e.g. a ReLU output; NULL = none), ReLU,
+ * then writes each non-NULL output at out + m * ldm + n * ldn (FP32, with
+ * f32_accumulate adding to the old value; BF16 rounded to nearest).  */
+typedef struct {
+    float alpha;
+    const float *bias;
+    int relu;
+    const void *mask;        /* BF16 */
+    long mask_ldm, mask_ldn;
+    float *out_f32;
+    long f32_ldm, f32_ldn;
+    int f32_accumulate;
+    void *out_bf16;          /* BF16 */
+    long bf16_ldm, bf16_ldn;
+    void *out_bf16_2;        /* BF16, e.g. the transposed copy */
+    long bf16_2_ldm, bf16_2_ldn;
+} cud_gemm_epilogue;
+
+int cud_gemm_bf16(const void *A, long lda, const void *B, long ldb, long M, long N, long K,
+                  const cud_gemm_epilogue *epilogue, void *stream);
+
 /* src/rse.cu:4-29 (gencp + rse, called from src/cp_als.cu:104-111): the
  * CP model's residual ||X - [[U_0..U_{order-1}]]||^2 and ||X||^2 (FP64, host
  * outputs; synchronous), computed in one pass over X without materialising
