@@ -206,6 +206,177 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Side workloads, reported as extra keys of the same JSON line (each leg is
+# timed with CUDA events on the bench stream; a failing leg records its error
+# instead of stopping the bench).
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def leg_cp_small(cd, torch, stream, sptr):
+    """Plain CP-ALS, 128^3, rank 16, <= 50 sweeps or delta fit < 1e-6."""
+    dims, R = (128, 128, 128), 16
+    with torch.cuda.stream(stream):
+        X, _ = cd.make_cp_tensor(dims, R, seed=10)
+        init = cd.make_init(dims, R, seed=11)
+    stream.synchronize()
+    out = {"dims": dims, "rank": R}
+    for name in ("fp32", "bf16x3"):
+        U = [u.clone() for u in init]
+        torch.cuda.synchronize()
+        res = cd.cp_als(X, dims, R, U, max_sweeps=50, tol=1e-6, precision=cd.PRECISIONS[name], stream=sptr)
+        out[name] = {"seconds": round(res.seconds, 5), "sweeps": res.sweeps, "fit": round(res.fit, 8),
+                     "ms_per_sweep": round(1e3 * res.seconds / max(1, res.sweeps), 4)}
+    return out
+
+
+def leg_order4(cd, torch, stream, sptr):
+    """4th-order 96^4, rank 32: MTTKRP per mode (BF16x3 tensor cores) and
+    sweep time from the plan's graph."""
+    dims, R = (96, 96, 96, 96), 32
+    with torch.cuda.stream(stream):
+        X, _ = cd.make_cp_tensor(dims, R, seed=12)
+        init = cd.make_init(dims, R, seed=13)
+    stream.synchronize()
+    kern = {}
+    outm = [torch.empty(d * R, device="cuda") for d in dims]
+    for mode in range(4):
+        for _ in range(2):
+            cd.mttkrp(X, dims, init, mode, R, outm[mode], cd.PREC_BF16X3, stream=sptr)
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        for _ in range(5):
+            cd.mttkrp(X, dims, init, mode, R, outm[mode], cd.PREC_BF16X3, stream=sptr)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        kern[mode] = {"ms": round(ms, 4), "gbs": round(mttkrp_bytes(dims, R, mode) / ms / 1e6, 1),
+                      "path": cd.mttkrp_path(dims, mode, R, cd.PREC_BF16X3)}
+    plan = cd.CpPlan(X, dims, R, [u.clone() for u in init], precision=cd.PREC_BF16X3, stream=sptr)
+    plan.run(3, stream=sptr)
+    e0, e1 = _events(torch)
+    e0.record(stream)
+    plan.run(10, stream=sptr)
+    e1.record(stream)
+    e1.synchronize()
+    sweep_ms = e0.elapsed_time(e1) / 10
+    fit = plan.true_fit(stream=sptr)
+    plan.close()
+    return {"dims": dims, "rank": R, "mttkrp": kern, "ms_per_sweep": round(sweep_ms, 4),
+            "sweep_gbs": round(sweep_bytes(dims, R) / sweep_ms / 1e6, 1), "fit_after_13_sweeps": round(fit, 8)}
+
+
+def leg_tucker(cd, torch, stream, sptr):
+    """Tucker HOSVD + 10 HOOI sweeps: 512^3 (32,32,32) and 128^4 (16^4),
+    Grams on the tensor cores (three-term BF16), TTM chains in BF16, FP64
+    eigensolves; reconstruction error relative to X."""
+    out = {}
+    for dims, ranks in (((512, 512, 512), (32, 32, 32)), ((128, 128, 128, 128), (16, 16, 16, 16))):
+        key = "x".join(map(str, dims)) + "_r" + str(ranks[0])
+        with torch.cuda.stream(stream):
+            X, _, _ = cd.make_tucker_tensor(dims, ranks, seed=20)
+        stream.synchronize()
+        core = torch.empty(int(np_prod(ranks)), device="cuda")
+        U = [torch.empty(d * r, device="cuda") for d, r in zip(dims, ranks)]
+        rec = torch.empty_like(X)
+        res = {}
+        for method in ("hosvd", "hooi10"):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if method == "hosvd":
+                cd.tucker_hosvd(X, dims, ranks, core, U, precision=cd.PREC_BF16X3, stream=sptr)
+            else:
+                cd.tucker_hooi(X, dims, ranks, core, U, sweeps=10, precision=cd.PREC_BF16X3, stream=sptr)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            cd.gentucker(rec, core, U, dims, ranks, stream=sptr)
+            torch.cuda.synchronize()
+            err = float(torch.linalg.norm((X - rec).double()) / torch.linalg.norm(X.double()))
+            res[method] = {"seconds": round(dt, 4), "rel_error": float(f"{err:.4e}")}
+        out[key] = res
+        del X, rec
+    return out
+
+
+def np_prod(xs):
+    p = 1
+    for x in xs:
+        p *= int(x)
+    return p
+
+
+def leg_batched(cd, torch, stream, sptr, n=4096):
+    """Batched CP-ALS: n tensors, dims uniform in [16, 96], ranks in [4, 16],
+    built like the 128^3 workload; one persistent kernel per sweep, graph
+    replay, autotuned launch shape; <= 50 sweeps or delta fit < 1e-6 per
+    tensor.  Parity sample: 16 tensors through the plain path."""
+    import numpy as np
+    rng = np.random.default_rng(30)
+    dims = [tuple(int(x) for x in rng.integers(16, 97, 3)) for _ in range(n)]
+    ranks = [int(x) for x in rng.integers(4, 17, n)]
+    b = cd.Batch(dims, ranks)
+    g = torch.Generator(device="cuda").manual_seed(31)
+    with torch.cuda.stream(stream):
+        for t, (d, r) in enumerate(zip(dims, ranks)):
+            facs = [torch.rand(x * r, generator=g, device="cuda") for x in d]
+            xv = b.x_view(t)
+            cd.gencp(xv, facs, d, r, stream=sptr)
+            nz = torch.randn(xv.numel(), generator=g, device="cuda")
+            xv.add_(nz * (1e-3 * torch.linalg.norm(xv) / (xv.numel() ** 0.5)))
+            for m in range(3):
+                b.u_view(t, m).copy_(torch.rand(d[m] * r, generator=g, device="cuda"))
+    stream.synchronize()
+    U0 = b.U.clone()
+    t0 = time.perf_counter()
+    th, cps = cd.cp_batched_tune(b, stream=sptr)
+    tune_s = time.perf_counter() - t0
+    b.U.copy_(U0)
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    e0.record(stream)
+    fits, sweeps, launches = cd.cp_als_batched(b, max_sweeps=50, tol=1e-6, stream=sptr)
+    e1.record(stream)
+    e1.synchronize()
+    secs = e0.elapsed_time(e1) * 1e-3
+    # parity sample through the plain single-tensor path (FP32, same start)
+    worst = 0.0
+    for t in rng.choice(n, 16, replace=False):
+        t = int(t)
+        U = [U0[b.u_offsets[3 * t + m]: b.u_offsets[3 * t + m] + dims[t][m] * ranks[t]].clone() for m in range(3)]
+        res = cd.cp_als(b.x_view(t).clone(), dims[t], ranks[t], U, max_sweeps=sweeps[t], tol=0.0,
+                        precision=cd.PREC_FP32, stream=sptr)
+        worst = max(worst, abs(res.fit_estimate - fits[t]))
+    elems = sum(np_prod(d) for d in dims)
+    return {"tensors": n, "elements": elems, "autotune": {"threads": th, "ctas_per_sm": cps, "seconds": round(tune_s, 3)},
+            "seconds": round(secs, 4), "sweep_kernels": launches, "sweeps_mean": round(float(np.mean(sweeps)), 2),
+            "fit_mean": round(float(np.mean(fits)), 6),
+            "gbs_mttkrp_traffic": round(3 * 4 * sum(np_prod(dims[t]) * sweeps[t] for t in range(n)) / secs / 1e9, 1),
+            "max_fit_diff_vs_plain_path_16_sampled": float(f"{worst:.3e}")}
+
+
+def leg_warmstart(cd, torch, n_train, n_eval):
+    """Learned warm start: 64^3 rank-8 smooth-factor tensors, network trained
+    on n_train ALS solutions the library generates (fresh tensors), then
+    sweeps and time to each tensor's reference fit - 1e-4 from HOSVD, learned
+    and judged (better of the two after one sweep) starts on n_eval held-out
+    tensors."""
+    import warmstart
+    w = warmstart.WarmStart(I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = w.train(n_train, batch=256, lr=1e-3, chunk=4096, label_sweeps=3, log_every=64)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    ev = w.evaluate(n_eval, id0=10 ** 9)
+    ev["train"] = {"samples": n_train, "seconds": round(train_s, 2),
+                   "loss_first": round(losses[0][1], 6) if losses else None,
+                   "loss_last": round(losses[-1][1], 6) if losses else None}
+    w.model.close()
+    return ev
+
+
 def config_dict(dims, R, precision, world=1):
     return {"workload": f"cp_als_sweep_{'x'.join(map(str, dims))}_r{R}", "dims": dims, "rank": R,
             "precision": precision, "global_batch": world, "seq_len": None,
@@ -329,6 +500,10 @@ def main():
                     help="time only the MTTKRP kernels (profiling runs) and exit")
     ap.add_argument("--kreps", type=int, default=10, help="timed MTTKRP launches per mode")
     ap.add_argument("--kwarm", type=int, default=3, help="untimed MTTKRP launches per mode")
+    ap.add_argument("--legs", default="cp128,order4,tucker,batched,warmstart",
+                    help="side workloads to add as extra keys (comma list, or 'none')")
+    ap.add_argument("--ws-train", type=int, default=204800, help="warm-start training samples")
+    ap.add_argument("--ws-eval", type=int, default=4096, help="warm-start held-out tensors")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -506,6 +681,25 @@ def main():
                      "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                      "step": f"cud_cp_als, {args.e2e_sweeps} sweeps, from pinned host buffers",
                      "seconds_per_step": round(e2e_s, 5)}
+
+    # ---- side workloads
+    legs = [x for x in args.legs.split(",") if x and x != "none"]
+    if rank == 0 and world == 1 and legs:
+        side = {}
+        fns = {"cp128": lambda: leg_cp_small(cd, torch, stream, sptr),
+               "order4": lambda: leg_order4(cd, torch, stream, sptr),
+               "tucker": lambda: leg_tucker(cd, torch, stream, sptr),
+               "batched": lambda: leg_batched(cd, torch, stream, sptr),
+               "warmstart": lambda: leg_warmstart(cd, torch, args.ws_train, args.ws_eval)}
+        for name in legs:
+            if name not in fns:
+                continue
+            try:
+                side[name] = fns[name]()
+            except Exception as exc:  # a side leg never stops the headline
+                side[name] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+            torch.cuda.synchronize()
+        result["workloads"] = side
 
     # ---- CPU baseline (rank 0, bounded sample)
     if rank == 0 and world == 1 and not args.no_cpu:

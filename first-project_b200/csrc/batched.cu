@@ -44,6 +44,7 @@ struct TensorMeta {
     int sweeps;
     double normx2;
     double fit, fit_prev;
+    double target;      // stop once fit >= target (<= 0: no target)
     double G[3][BMAXR * BMAXR];  // factor Grams (FP64)
 };
 
@@ -312,7 +313,8 @@ __global__ void __launch_bounds__(NT) k_batch_sweep(BatchArgs a) {
             t.fit_prev = t.fit;
             t.fit = fit;
             t.sweeps += 1;
-            if ((a.tol > 0 && t.sweeps >= 2 && fabs(t.fit - t.fit_prev) < a.tol) || t.sweeps >= a.max_sweeps) {
+            if ((a.tol > 0 && t.sweeps >= 2 && fabs(t.fit - t.fit_prev) < a.tol) || t.sweeps >= a.max_sweeps ||
+                (t.target > 0.0 && t.fit >= t.target)) {
                 t.done = 1;
                 atomicAdd(a.ndone, 1);
             }
@@ -410,10 +412,11 @@ long shape_class(int n, const int *dims, const int *ranks) {
 
 using namespace cud;
 
-extern "C" int cud_cp_als_batched(int ntensors, const long *dims, const long *ranks, const float *X,
-                                  const long *x_offsets, float *U, const long *u_offsets,
-                                  const cud_cp_options *opt_in, double *fits, int *sweeps,
-                                  int *kernel_launches, void *stream) {
+namespace {
+
+int batched_impl(int ntensors, const long *dims, const long *ranks, const float *X, const long *x_offsets, float *U,
+                 const long *u_offsets, const cud_cp_options *opt_in, const double *targets, double *fits,
+                 int *sweeps, int *kernel_launches, void *stream) {
     if (ntensors <= 0 || !dims || !ranks || !X || !x_offsets || !U || !u_offsets)
         return set_status(CUD_ERR_INVALID_ARGUMENT);
     cud_cp_options opt;
@@ -437,6 +440,7 @@ extern "C" int cud_cp_als_batched(int ntensors, const long *dims, const long *ra
         m.R = (int)ranks[t];
         hr[t] = m.R;
         m.xoff = x_offsets[t];
+        m.target = targets ? targets[t] : 0.0;
         work[t] = {-(double)m.dims[0] * m.dims[1] * m.dims[2] * m.R, t};
     }
     std::sort(work.begin(), work.end());
@@ -532,6 +536,24 @@ extern "C" int cud_cp_als_batched(int ntensors, const long *dims, const long *ra
         cudaStreamDestroy(cs);
     }
     return set_status(st);
+}
+
+}  // namespace
+
+extern "C" int cud_cp_als_batched(int ntensors, const long *dims, const long *ranks, const float *X,
+                                  const long *x_offsets, float *U, const long *u_offsets,
+                                  const cud_cp_options *opt_in, double *fits, int *sweeps,
+                                  int *kernel_launches, void *stream) {
+    return batched_impl(ntensors, dims, ranks, X, x_offsets, U, u_offsets, opt_in, nullptr, fits, sweeps,
+                        kernel_launches, stream);
+}
+
+extern "C" int cud_cp_als_batched_target(int ntensors, const long *dims, const long *ranks, const float *X,
+                                         const long *x_offsets, float *U, const long *u_offsets,
+                                         const cud_cp_options *opt_in, const double *target_fits, double *fits,
+                                         int *sweeps, int *kernel_launches, void *stream) {
+    return batched_impl(ntensors, dims, ranks, X, x_offsets, U, u_offsets, opt_in, target_fits, fits, sweeps,
+                        kernel_launches, stream);
 }
 
 extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *ranks, const float *X,

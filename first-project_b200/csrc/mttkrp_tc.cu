@@ -3,7 +3,7 @@
 // Around mode n the FP32 tensor is a (P, Q, S) array; the result is
 // M[q, r] = sum_kappa X(q, kappa) * KR(kappa, r), with kappa running over the
 // other modes.  Per CTA: one tile of 128 rows q (the MMA's M) and a
-// contiguous range of 32-deep contraction stages, pipelined NST deep between
+// contiguous range of 32-deep contraction stages, pipelined 3-4 deep between
 // four warp roles:
 //   * warp 0 (TMA): the 128 x 32 FP32 tile of X, in its native layout, into
 //     shared memory (mode 0: rows contiguous, a 2-D box over (q, s); other
@@ -15,11 +15,12 @@
 //     shared memory once;
 //   * warps 6-7 (KR producers): the stage's 32 Khatri-Rao rows.  The stage's
 //     kappa run over 32 consecutive rows of the fastest generating factor
-//     while the other factors contribute one constant row, so each thread
-//     loads two 128-bit vectors of one factor column (prefetched a stage
-//     ahead), scales, splits and stores 16 bytes per operand into the K-major
-//     canonical B layout.  They only wait for the slot to be free, so they
-//     run up to NST stages ahead of the MMA;
+//     while the other factors contribute one constant row, so the TMA warp
+//     brings those 32 rows x R of the factor into shared memory with the X
+//     tile, and each producer thread reads two 128-bit vectors of one column,
+//     scales them by the constant row (recomputed once per block of stages),
+//     splits and stores 16 bytes per operand into the K-major canonical B
+//     layout (general factor shapes: computed from global memory);
 //   * warp 1 (MMA): tcgen05.mma kind::f16, FP32 accumulation in TMEM:
 //     D += Xhi*KRhi + Xhi*KRlo + Xlo*KRhi  (BF16X3), or one product (BF16,
 //     FP16).
@@ -48,7 +49,8 @@ namespace {
 
 constexpr int BQ = 128;          // rows per CTA tile (MMA M)
 constexpr int BKS = 32;          // contraction depth per stage (two MMA K-steps of 16)
-constexpr int NST = 4;           // pipeline stages
+constexpr int NXMAX = 8;         // X tiles in flight (deep: hides DRAM latency)
+constexpr int NBMAX = 4;         // U / B / A stages (shallow: feeds the MMA)
 #ifndef CUD_TC_SEG
 #define CUD_TC_SEG 16
 #endif
@@ -70,14 +72,18 @@ struct TcArgs {
     long stages;       // total stages
     long chunk;        // stages per CTA
     long qtiles;
+    int nx, nb;        // X ring and U/B/A ring depths of this launch
+    int nkri;          // B items (row, 8-kappa chunk) made by the KR warps; the converters make the rest
+    long Rp;           // partial row width: R rounded up to a multiple of 4
     KrFactors gen;     // kind 0: factors after mode 0; kind 1: factors before the mode
     KrFactors outer;   // kind 1: factors after the mode (one constant row per stage)
-    float *part;       // [split][R][Q]
+    float *part;       // [split][Q][Rp]
     int *error;        // device flag
 };
 
 struct TcCtrl {
-    uint64_t full_x[NST], empty_x[NST], full_a[NST], empty_a[NST];
+    uint64_t full_x[NXMAX], empty_x[NXMAX];                       // X tiles
+    uint64_t full_u[NBMAX], empty_u[NBMAX], full_a[NBMAX], empty_a[NBMAX];  // U tiles, A + B operands
     uint64_t d_full[2], d_free[2], done;
     const float *gU[kMaxOrder];
     const float *oU[kMaxOrder];
@@ -90,8 +96,13 @@ constexpr size_t CTRL_BYTES = (sizeof(TcCtrl) + 1023) & ~size_t(1023);
 
 __host__ __device__ constexpr size_t b_tile_bytes(int Rpad) { return (size_t)Rpad * BKS * 2; }
 
-__host__ __device__ constexpr size_t tc_smem_bytes(int Rpad) {
-    return 1024 + CTRL_BYTES + (size_t)NST * X_STAGE_BYTES + (size_t)NST * 2 * b_tile_bytes(Rpad);
+// one U/B stage: (fast path) the U tile of Rpad x 32 FP32, B hi + lo
+__host__ __device__ constexpr size_t tc_ub_bytes(int Rpad, bool fast) {
+    return (fast ? (size_t)Rpad * 128 : 0) + 2 * b_tile_bytes(Rpad);
+}
+
+__host__ __device__ constexpr size_t tc_smem_bytes(int Rpad, bool fast, int nx, int nb) {
+    return 1024 + CTRL_BYTES + (size_t)nx * X_STAGE_BYTES + (size_t)nb * tc_ub_bytes(Rpad, fast);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
@@ -117,96 +128,117 @@ __device__ __forceinline__ void split_pair(float a, float b, uint32_t &hi, uint3
 // 8 values k = 8c..8c+7 of row n form one 16-byte chunk at n*16 + c*Rpad*16.
 // Descriptor: SBO (8-row groups) = 128 B, LBO (K chunks) = Rpad*16 B.
 
-// The Khatri-Rao values one producer thread makes per stage: KIPT items,
-// each (row r, chunk kc) = 8 consecutive kappa of one column r.
-template <int KIPT>
-struct KrRegs {
-    float f[KIPT][8];
-    float c[KIPT];
-};
-
-// Loads (fast path) or computes (general path) this thread's KR items for
-// stage g into registers.  `cache_key` / `cc` memoise the constant row,
-// which only changes when the stage crosses a row block of the fastest
-// generating factor or (kind 1) a slab.
-template <int KIPT>
-__device__ __forceinline__ void kr_load(const TcArgs &a, const TcCtrl &sm, long g, int kt,
-                                        KrRegs<KIPT> &o, long &cache_key, float (&cc)[KIPT]) {
-    long k0, kmax, s;
-    if (a.kind == 0) { k0 = g * BKS; kmax = a.S; s = 0; }
-    else { s = g / a.psteps; k0 = (g % a.psteps) * BKS; kmax = a.P; }
-    const int ng = a.gen.n, no = a.outer.n;
-    const long rows0 = sm.grows[0];
-    const long rest = k0 / rows0;
-    const long i0 = k0 - rest * rows0;
-    const long key = rest * 2147483647L + s;
-    const bool refresh = (key != cache_key);
-    cache_key = key;
+// Per-stage Khatri-Rao values of one producer item (row r, 8-kappa chunk kc)
+// on the general path (any factor shapes): computed from global memory.
+__device__ __forceinline__ void kr_general(const TcArgs &a, const TcCtrl &sm, long g, int r, int kc, float (&v)[8]) {
+    long k0, kmax;
+    if (a.kind == 0) { k0 = g * BKS; kmax = a.S; }
+    else { k0 = (g % a.psteps) * BKS; kmax = a.P; }
+    const long s = (a.kind == 0) ? 0 : g / a.psteps;
+    float c = 1.f;
+    long lin = s;
+    for (int f = 0; f < a.outer.n; f++) {
+        const long d = sm.orows[f];
+        c *= __ldg(sm.oU[f] + (lin % d) + r * d);
+        lin /= d;
+    }
 #pragma unroll
-    for (int it = 0; it < KIPT; it++) {
-        const int id = kt + NKR * it;
-        const int kc = id & 3;
-        const int r = id >> 2;
-#pragma unroll
-        for (int j = 0; j < 8; j++) o.f[it][j] = 0.f;
-        o.c[it] = 0.f;
-        if (r >= a.R) continue;
-        if (refresh) {
-            // the constant row: the digits of s over the outer factors and
-            // (fast path) of `rest` over the slower generating factors,
-            // recomputed per item so no index array lives in local memory
-            float c = 1.f;
-            long lin = s;
-            for (int f = 0; f < no; f++) {
-                const long d = sm.orows[f];
-                const long idx = lin % d;
-                lin /= d;
-                c *= __ldg(sm.oU[f] + idx + r * d);
-            }
-            if (a.fast) {
-                lin = rest;
-                for (int f = 1; f < ng; f++) {
-                    const long d = sm.grows[f];
-                    const long idx = lin % d;
-                    lin /= d;
-                    c *= __ldg(sm.gU[f] + idx + r * d);
-                }
-            }
-            cc[it] = c;
-        }
-        o.c[it] = cc[it];
-        if (a.fast) {
-            const float4 *src = reinterpret_cast<const float4 *>(sm.gU[0] + i0 + kc * 8 + r * rows0);
-            float4 v0 = __ldg(src), v1 = __ldg(src + 1);
-            o.f[it][0] = v0.x; o.f[it][1] = v0.y; o.f[it][2] = v0.z; o.f[it][3] = v0.w;
-            o.f[it][4] = v1.x; o.f[it][5] = v1.y; o.f[it][6] = v1.z; o.f[it][7] = v1.w;
-        } else {
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                long k = k0 + kc * 8 + j;
-                if (k >= kmax) continue;
-                float v = 1.f;
-                long lin = k;
-                for (int f = 0; f < ng; f++) {
-                    long d = sm.grows[f];
-                    v *= __ldg(sm.gU[f] + (lin % d) + r * d);
-                    lin /= d;
-                }
-                o.f[it][j] = v;
+    for (int j = 0; j < 8; j++) {
+        const long k = k0 + kc * 8 + j;
+        float x = 0.f;
+        if (k < kmax) {
+            x = c;
+            long l2 = k;
+            for (int f = 0; f < a.gen.n; f++) {
+                const long d = sm.grows[f];
+                x *= __ldg(sm.gU[f] + (l2 % d) + r * d);
+                l2 /= d;
             }
         }
+        v[j] = x;
     }
 }
 
-template <int KIPT, int MINB>
+// B item `id` -> (row r, 8-kappa chunk kc): 32 consecutive ids cover 8 rows x
+// 4 chunks, so a quarter-warp stores 128 contiguous bytes of the B tile.
+__device__ __forceinline__ void b_item(int id, int &r, int &kc) {
+    r = ((id >> 5) << 3) | (id & 7);
+    kc = (id >> 3) & 3;
+}
+
+// The 8 raw Khatri-Rao inputs of B item (r, kc) from the stage's U tile in
+// shared memory (128-byte swizzled: row r's 16-byte chunk c at c ^ (r & 7)).
+__device__ __forceinline__ void load_u_item(const float *us, int r, int kc, float4 &u0, float4 &u1) {
+    u0 = *reinterpret_cast<const float4 *>(us + r * BKS + (((2 * kc) ^ (r & 7)) << 2));
+    u1 = *reinterpret_cast<const float4 *>(us + r * BKS + (((2 * kc + 1) ^ (r & 7)) << 2));
+}
+
+// Makes B item (r, kc) of stage g: 8 Khatri-Rao values (fast path: the U
+// values u0, u1 times the constant row c; general path: from global
+// memory), rounded / split and stored into the canonical B layout.
+__device__ __forceinline__ void make_b_item(const TcArgs &a, const TcCtrl &sm, long g, int r, int kc, float c,
+                                            float4 u0, float4 u1, uint8_t *bh, uint8_t *bl, bool three, bool f16) {
+    float v[8];
+    if (a.fast) {
+        v[0] = u0.x * c; v[1] = u0.y * c; v[2] = u0.z * c; v[3] = u0.w * c;
+        v[4] = u1.x * c; v[5] = u1.y * c; v[6] = u1.z * c; v[7] = u1.w * c;
+    } else if (r < a.R) {
+        kr_general(a, sm, g, r, kc, v);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = 0.f;
+    }
+    const uint32_t off = (uint32_t)r * 16u + (uint32_t)kc * (uint32_t)a.Rpad * 16u;
+    uint4 h, l;
+    if (f16) {
+        h.x = pack_f16(v[0], v[1]); h.y = pack_f16(v[2], v[3]);
+        h.z = pack_f16(v[4], v[5]); h.w = pack_f16(v[6], v[7]);
+    } else if (three) {
+        split_pair(v[0], v[1], h.x, l.x); split_pair(v[2], v[3], h.y, l.y);
+        split_pair(v[4], v[5], h.z, l.z); split_pair(v[6], v[7], h.w, l.w);
+        *reinterpret_cast<uint4 *>(bl + off) = l;
+    } else {
+        h.x = pack_bf16(v[0], v[1]); h.y = pack_bf16(v[2], v[3]);
+        h.z = pack_bf16(v[4], v[5]); h.w = pack_bf16(v[6], v[7]);
+    }
+    *reinterpret_cast<uint4 *>(bh + off) = h;
+}
+
+// The constant row of the fast path for the block of stages starting at g:
+// the product over the slower generating factors (digits of kappa / rows0)
+// and the outer factors (digits of s) of their row for column r.
+__device__ __forceinline__ float kr_const_row(const TcArgs &a, const TcCtrl &sm, long g, int r) {
+    long k0, s;
+    if (a.kind == 0) { k0 = g * BKS; s = 0; }
+    else { k0 = (g % a.psteps) * BKS; s = g / a.psteps; }
+    float c = 1.f;
+    long lin = k0 / sm.grows[0];
+    for (int f = 1; f < a.gen.n; f++) {
+        const long d = sm.grows[f];
+        c *= __ldg(sm.gU[f] + (lin % d) + r * d);
+        lin /= d;
+    }
+    lin = s;
+    for (int f = 0; f < a.outer.n; f++) {
+        const long d = sm.orows[f];
+        c *= __ldg(sm.oU[f] + (lin % d) + r * d);
+        lin /= d;
+    }
+    return c;
+}
+
+template <int KIPT, int CIPT, int MINB>
 __global__ void __launch_bounds__(NTHREADS, MINB)
-    k_mttkrp_tc(const __grid_constant__ CUtensorMap tmap, TcArgs a) {
+    k_mttkrp_tc(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap umap, TcArgs a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     TcCtrl &sm = *reinterpret_cast<TcCtrl *>(base);
-    float *xst = reinterpret_cast<float *>(base + CTRL_BYTES);
-    uint8_t *bst = base + CTRL_BYTES + (size_t)NST * X_STAGE_BYTES;
-    const uint32_t bbytes = (uint32_t)b_tile_bytes(a.Rpad);
+    const int nx = a.nx, nb = a.nb;
+    uint8_t *xring = base + CTRL_BYTES;                        // nx X tiles
+    uint8_t *ubring = xring + (size_t)nx * X_STAGE_BYTES;      // nb (U tile, B hi, B lo)
+    const uint32_t ubytes = a.fast ? (uint32_t)a.Rpad * 128u : 0u;   // U tile: Rpad x 32 FP32
+    const uint32_t bbytes = (uint32_t)b_tile_bytes(a.Rpad);          // one B operand (hi or lo)
+    const uint32_t ubstage = ubytes + 2u * bbytes;
     const uint32_t a_col0 = 2u * (uint32_t)a.Rpad;  // two D buffers first, then the A stages
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long qtile = blockIdx.x % a.qtiles;
@@ -219,11 +251,15 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     volatile int *abort = &sm.abort;
 
     if (threadIdx.x == 0) {
-        for (int i = 0; i < NST; i++) {
+        // consumer / producer counts are warps: lane 0 arrives for its warp
+        // after __syncwarp
+        for (int i = 0; i < NXMAX; i++) {
             ptx::mbar_init(&sm.full_x[i], 1);
-            // producer barriers count warps: lane 0 arrives for its warp
-            // after __syncwarp, so each stage costs 6 arrivals, not 192
             ptx::mbar_init(&sm.empty_x[i], NCONV / 32);
+        }
+        for (int i = 0; i < NBMAX; i++) {
+            ptx::mbar_init(&sm.full_u[i], 1);
+            ptx::mbar_init(&sm.empty_u[i], NKR / 32 + (CIPT > 0 ? NCONV / 32 : 0));
             ptx::mbar_init(&sm.full_a[i], (NCONV + NKR) / 32);
             ptx::mbar_init(&sm.empty_a[i], 1);
         }
@@ -241,6 +277,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         }
         ptx::fence_mbar_init();
         ptx::prefetch_tmap(&tmap);
+        if (a.fast) ptx::prefetch_tmap(&umap);
     }
     if (warp == 0) {
         ptx::tmem_alloc(&sm.tmem_base, a.tmem_cols);
@@ -254,23 +291,36 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     const bool three = (a.prec == CUD_PREC_BF16X3 || a.prec == CUD_PREC_DEFAULT);
     const bool f16 = (a.prec == CUD_PREC_FP16);
 
-    long issued = 0;  // TMA loads issued (producer thread)
+    long issued_x = 0, issued_u = 0;  // TMA loads issued (producer thread)
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
         if (lane == 0) {
             for (long i = 0; i < nst && !*abort; i++) {
-                const int slot = (int)(i % NST);
-                const long use = i / NST;
-                if (use > 0 && !ptx::mbar_wait(&sm.empty_x[slot], (uint32_t)((use - 1) & 1), abort)) break;
                 const long g = st_beg + i;
-                issued = i + 1;
-                ptx::mbar_arrive_expect_tx(&sm.full_x[slot], X_STAGE_BYTES);
-                float *dst = xst + (size_t)slot * BQ * BKS;
-                if (a.kind == 0) {
-                    ptx::tma_load_2d(dst, &tmap, &sm.full_x[slot], (int)q0, (int)(g * BKS));
-                } else {
-                    const long s = g / a.psteps, p0 = (g % a.psteps) * BKS;
-                    ptx::tma_load_3d(dst, &tmap, &sm.full_x[slot], (int)p0, (int)q0, (int)s);
+                {
+                    const int slot = (int)(i % nx);
+                    const long use = i / nx;
+                    if (use > 0 && !ptx::mbar_wait(&sm.empty_x[slot], (uint32_t)((use - 1) & 1), abort)) break;
+                    uint8_t *dst = xring + (size_t)slot * X_STAGE_BYTES;
+                    ptx::mbar_arrive_expect_tx(&sm.full_x[slot], (uint32_t)X_STAGE_BYTES);
+                    if (a.kind == 0) {
+                        ptx::tma_load_2d(dst, &tmap, &sm.full_x[slot], (int)q0, (int)(g * BKS));
+                    } else {
+                        const long s = g / a.psteps, p0 = (g % a.psteps) * BKS;
+                        ptx::tma_load_3d(dst, &tmap, &sm.full_x[slot], (int)p0, (int)q0, (int)s);
+                    }
+                    issued_x = i + 1;
+                }
+                if (a.fast) {
+                    const int slot = (int)(i % nb);
+                    const long use = i / nb;
+                    if (use > 0 && !ptx::mbar_wait(&sm.empty_u[slot], (uint32_t)((use - 1) & 1), abort)) break;
+                    // first kappa of the stage along the fastest generating factor
+                    const long kf = (a.kind == 0) ? g * BKS : (g % a.psteps) * BKS;
+                    ptx::mbar_arrive_expect_tx(&sm.full_u[slot], ubytes);
+                    ptx::tma_load_2d(ubring + (size_t)slot * ubstage, &umap, &sm.full_u[slot],
+                                     (int)(kf % sm.grows[0]), 0);
+                    issued_u = i + 1;
                 }
             }
         }
@@ -280,8 +330,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             const uint32_t idesc = ptx::idesc_f16(f16 ? 0u : 1u, BQ, (uint32_t)a.Rpad);
             const uint32_t lbo = (uint32_t)a.Rpad * 16u;
             for (long i = 0; i < nst; i++) {
-                const int slot = (int)(i % NST);
-                const long use = i / NST;
+                const int slot = (int)(i % nb);
+                const long use = i / nb;
                 const long seg = i / SEG;
                 const int b = (int)(seg & 1);
                 const bool seg_first = (i % SEG) == 0;
@@ -293,7 +343,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
                 const uint32_t d = tbase + (uint32_t)b * (uint32_t)a.Rpad;
                 const uint32_t a_hi = tbase + a_col0 + (uint32_t)slot * 32u;
                 const uint32_t a_lo = a_hi + 16u;
-                const uint32_t b_hi = ptx::smem_addr(bst + (size_t)(2 * slot) * bbytes);
+                const uint32_t b_hi = ptx::smem_addr(ubring + (size_t)slot * ubstage + ubytes);
                 const uint32_t b_lo = b_hi + bbytes;
                 uint32_t acc = seg_first ? 0u : 1u;
 #pragma unroll
@@ -322,7 +372,13 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         const int row = sub * 32 + lane;          // row within the tile (= TMEM lane)
         const uint32_t lane_off = (uint32_t)(sub * 32) << 16;
         const long q = q0 + row;
-        float *P = a.part + z * a.R * a.Q;
+        const int ct = threadIdx.x - 64;  // converter thread 0..127
+        const long blk = a.fast ? (long)(sm.grows[0] / BKS) : 1;
+        long pos = a.fast ? st_beg % blk : 0;
+        float ccv[CIPT > 0 ? CIPT : 1];
+#pragma unroll
+        for (int j = 0; j < (CIPT > 0 ? CIPT : 1); j++) ccv[j] = 0.f;
+        float *P = a.part + (z * a.Q + q) * a.Rp;  // this row's partial (Rp floats)
         long flushed = 0;  // segments already added into the partial
         // Adds finished segment `seg` (TMEM buffer seg & 1) into the partial.
         auto flush = [&](long seg) {
@@ -339,13 +395,18 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
                     if (two) ptx::tmem_ld16(d + (uint32_t)c0 + 16u, v[1]);
                     ptx::tmem_wait_ld();
                     if (q < a.Q) {
-                        float *p = P + q + a.Q * c0;
 #pragma unroll
-                        for (int j = 0; j < 32; j++) {
-                            if (c0 + j < a.R) {
-                                const float val = __uint_as_float(v[j >> 4][j & 15]);
-                                if (seg == 0) p[a.Q * j] = val;
-                                else atomicAdd(p + a.Q * j, val);  // red.global.add.f32, RN
+                        for (int j4 = 0; j4 < 8; j4++) {
+                            const int c = c0 + 4 * j4;
+                            if (c < a.R) {  // columns R..Rp-1 of D are zero (zero B rows)
+                                const uint32_t *w = &v[j4 >> 2][(j4 & 3) * 4];
+                                float4 val = make_float4(__uint_as_float(w[0]), __uint_as_float(w[1]),
+                                                         __uint_as_float(w[2]), __uint_as_float(w[3]));
+                                float *pp = P + c;
+                                if (seg == 0) *reinterpret_cast<float4 *>(pp) = val;
+                                else asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(pp),
+                                                  "f"(val.x), "f"(val.y), "f"(val.z), "f"(val.w)
+                                                  : "memory");  // RN
                             }
                         }
                     }
@@ -356,15 +417,16 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             if (lane == 0) ptx::mbar_arrive(&sm.d_free[b]);
         };
         for (long i = 0; i < nst; i++) {
-            const int slot = (int)(i % NST);
-            const long use = i / NST;
+            const int xslot = (int)(i % nx), slot = (int)(i % nb);
+            const long xuse = i / nx, use = i / nb;
             // After an abort the loop keeps running (without waiting) so every
             // converter thread reaches the same warp-aligned tcgen05 instructions.
             if (use > 0 && !*abort) ptx::mbar_wait(&sm.empty_a[slot], (uint32_t)((use - 1) & 1), abort);
-            if (!*abort) ptx::mbar_wait(&sm.full_x[slot], (uint32_t)(use & 1), abort);
+            if (!*abort) ptx::mbar_wait(&sm.full_x[xslot], (uint32_t)(xuse & 1), abort);
+            if (CIPT > 0 && a.fast && !*abort) ptx::mbar_wait(&sm.full_u[slot], (uint32_t)(use & 1), abort);
             __syncwarp();
             float x[BKS];
-            const float *xs = xst + (size_t)slot * BQ * BKS;
+            const float *xs = reinterpret_cast<const float *>(xring + (size_t)xslot * X_STAGE_BYTES);
             if (a.kind == 0) {
 #pragma unroll
                 for (int k = 0; k < BKS; k++) x[k] = xs[k * BQ + row];
@@ -376,8 +438,23 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
                     x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
                 }
             }
+            // this thread's B items' U values, then the slot is free for the next load
+            float4 cu0[CIPT > 0 ? CIPT : 1], cu1[CIPT > 0 ? CIPT : 1];
+            if (CIPT > 0 && a.fast) {
+                const float *us = reinterpret_cast<const float *>(ubring + (size_t)slot * ubstage);
+#pragma unroll
+                for (int j = 0; j < CIPT; j++) {
+                    const int id = a.nkri + ct + NCONV * j;
+                    int r, kc;
+                    b_item(id < 4 * a.Rpad ? id : 0, r, kc);
+                    load_u_item(us, r, kc, cu0[j], cu1[j]);
+                }
+            }
             __syncwarp();
-            if (lane == 0) ptx::mbar_arrive(&sm.empty_x[slot]);
+            if (lane == 0) {
+                ptx::mbar_arrive(&sm.empty_x[xslot]);  // the X tile is consumed
+                if (CIPT > 0 && a.fast) ptx::mbar_arrive(&sm.empty_u[slot]);
+            }
             uint32_t hi[16], lo[16];
             if (f16) {
 #pragma unroll
@@ -392,6 +469,31 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             const uint32_t ta = tbase + lane_off + a_col0 + (uint32_t)slot * 32u;
             ptx::tmem_st16(ta, hi);
             if (three) ptx::tmem_st16(ta + 16, lo);
+            // this thread's share of the B tile
+            if (CIPT > 0) {
+                const long g = st_beg + i;
+                if (a.fast && (i == 0 || pos == 0)) {
+#pragma unroll
+                    for (int j = 0; j < CIPT; j++) {
+                        const int id = a.nkri + ct + NCONV * j;
+                        int r, kc;
+                        b_item(id, r, kc);
+                        ccv[j] = (id < 4 * a.Rpad && r < a.R) ? kr_const_row(a, sm, g, r) : 0.f;
+                    }
+                }
+                uint8_t *bh = ubring + (size_t)slot * ubstage + ubytes;
+#pragma unroll
+                for (int j = 0; j < CIPT; j++) {
+                    const int id = a.nkri + ct + NCONV * j;
+                    if (id < 4 * a.Rpad) {
+                        int r, kc;
+                        b_item(id, r, kc);
+                        make_b_item(a, sm, g, r, kc, ccv[j], cu0[j], cu1[j], bh, bh + bbytes, three, f16);
+                    }
+                }
+                ptx::fence_proxy_async_smem();  // generic-proxy B writes -> tensor core
+            }
+            if (a.fast) pos = (pos + 1 == blk) ? 0 : pos + 1;
             ptx::tmem_wait_st();
             ptx::tc_fence_before();
             __syncwarp();
@@ -403,42 +505,52 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     } else {
         // ------------------------------------------------------------ KR producers
         const int kt = threadIdx.x - 192;  // 0..63
-        long ckey = -1;
+        // fast path: the stage's 32 rows of the fastest generating factor
+        // arrive by TMA with X; the constant row changes every `blk` stages
+        const long blk = a.fast ? (long)(sm.grows[0] / BKS) : 1;
+        long pos = a.fast ? st_beg % blk : 0;  // stage index within its block
         float cc[KIPT];
 #pragma unroll
         for (int it = 0; it < KIPT; it++) cc[it] = 0.f;
-        KrRegs<KIPT> nxt;
-        if (nst > 0) kr_load<KIPT>(a, sm, st_beg, kt, nxt, ckey, cc);
-        for (long i = 0; i < nst; i++) {
-            const int slot = (int)(i % NST);
-            const long use = i / NST;
-            KrRegs<KIPT> cur = nxt;
-            if (i + 1 < nst) kr_load<KIPT>(a, sm, st_beg + i + 1, kt, nxt, ckey, cc);
+        for (long i = 0; i < nst; i++, pos = (pos + 1 == blk) ? 0 : pos + 1) {
+            const int slot = (int)(i % nb);
+            const long use = i / nb;
+            const long g = st_beg + i;
+            if (a.fast && (i == 0 || pos == 0)) {
+#pragma unroll
+                for (int it = 0; it < KIPT; it++) {
+                    const int id = kt + NKR * it;
+                    int r, kc;
+                    b_item(id, r, kc);
+                    cc[it] = (id < a.nkri && r < a.R) ? kr_const_row(a, sm, g, r) : 0.f;
+                }
+            }
+            uint8_t *st = ubring + (size_t)slot * ubstage;
+            float4 ku0[KIPT], ku1[KIPT];
+            if (a.fast) {
+                // the U tile: read this thread's values, then release the slot
+                if (!*abort) ptx::mbar_wait(&sm.full_u[slot], (uint32_t)(use & 1), abort);
+                const float *us = reinterpret_cast<const float *>(st);
+#pragma unroll
+                for (int it = 0; it < KIPT; it++) {
+                    const int id = kt + NKR * it;
+                    int r, kc;
+                    b_item(id < a.nkri ? id : 0, r, kc);
+                    load_u_item(us, r, kc, ku0[it], ku1[it]);
+                }
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(&sm.empty_u[slot]);
+            }
             if (use > 0 && !*abort) ptx::mbar_wait(&sm.empty_a[slot], (uint32_t)((use - 1) & 1), abort);
-            uint8_t *bh = bst + (size_t)(2 * slot) * bbytes;
-            uint8_t *bl = bh + bbytes;
+            uint8_t *bh = st + ubytes;
 #pragma unroll
             for (int it = 0; it < KIPT; it++) {
                 const int id = kt + NKR * it;
-                const int r = id >> 2, kc = id & 3;
-                if (r >= a.Rpad) continue;
-                const uint32_t off = (uint32_t)r * 16u + (uint32_t)kc * (uint32_t)a.Rpad * 16u;
-                float v[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) v[j] = cur.f[it][j] * cur.c[it];
-                uint4 h, l;
-                if (f16) {
-                    h.x = pack_f16(v[0], v[1]); h.y = pack_f16(v[2], v[3]);
-                    h.z = pack_f16(v[4], v[5]); h.w = pack_f16(v[6], v[7]);
-                } else if (three) {
-                    split_pair(v[0], v[1], h.x, l.x); split_pair(v[2], v[3], h.y, l.y);
-                    split_pair(v[4], v[5], h.z, l.z); split_pair(v[6], v[7], h.w, l.w);
-                    *reinterpret_cast<uint4 *>(bl + off) = l;
-                } else {
-                    h.x = pack_bf16(v[0], v[1]); h.y = pack_bf16(v[2], v[3]);
-                    h.z = pack_bf16(v[4], v[5]); h.w = pack_bf16(v[6], v[7]);
+                if (id < a.nkri) {
+                    int r, kc;
+                    b_item(id, r, kc);
+                    make_b_item(a, sm, g, r, kc, cc[it], ku0[it], ku1[it], bh, bh + bbytes, three, f16);
                 }
-                *reinterpret_cast<uint4 *>(bh + off) = h;
             }
             ptx::fence_proxy_async_smem();  // generic-proxy B writes -> tensor core
             __syncwarp();
@@ -450,9 +562,14 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     if (threadIdx.x == 0 && *abort) {
         // drain: the last load issued into each slot must land before the
         // CTA's shared memory goes away (bounded, abort flag ignored)
-        for (long i = (issued > NST ? issued - NST : 0); i < issued; i++) {
-            const uint32_t par = (uint32_t)((i / NST) & 1);
-            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.full_x[i % NST], par, 100000u); it++) {
+        for (long i = (issued_x > nx ? issued_x - nx : 0); i < issued_x; i++) {
+            const uint32_t par = (uint32_t)((i / nx) & 1);
+            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.full_x[i % nx], par, 100000u); it++) {
+            }
+        }
+        for (long i = (issued_u > nb ? issued_u - nb : 0); i < issued_u; i++) {
+            const uint32_t par = (uint32_t)((i / nb) & 1);
+            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.full_u[i % nb], par, 100000u); it++) {
             }
         }
         atomicExch(a.error, 1);
@@ -463,19 +580,29 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     if (warp == 0) ptx::tmem_dealloc(tbase, a.tmem_cols);
 }
 
-// out[e] = sum_z part[z][e] in FP64: 64 outputs per CTA, the splits spread
-// over 4 lanes per output (coalesced rows of 64), combined in fixed order.
-__global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict__ part, int splits,
-                                                         long n, float *__restrict__ out) {
-    __shared__ double red[4][64];
-    const int o = threadIdx.x & 63, lanez = threadIdx.x >> 6;
-    const long e = blockIdx.x * 64L + o;
-    double s = 0.0;
-    if (e < n)
-        for (int z = lanez; z < splits; z += 4) s += (double)__ldcs(part + (long)z * n + e);
-    red[lanez][o] = s;
+// out[q + Q r] = sum_z part[z][q][r] in FP64, fixed order.  A CTA owns 32
+// consecutive (q, r) slots of the padded partial rows (coalesced reads), each
+// summed by 8 lanes over the splits z = lane, lane + 8, ..., then combined
+// in lane order.
+__global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict__ part, int splits, long Q,
+                                                         long R, long Rp, float *__restrict__ out) {
+    __shared__ double red[8][32];
+    const int o = threadIdx.x & 31, zl = threadIdx.x >> 5;
+    const long e = blockIdx.x * 32L + o;  // q * Rp + r
+    const long n = Q * Rp;
+    double sum = 0.0;
+    if (e < n) {
+#pragma unroll 4
+        for (int z = zl; z < splits; z += 8) sum += (double)__ldcs(part + (long)z * n + e);
+    }
+    red[zl][o] = sum;
     __syncthreads();
-    if (lanez == 0 && e < n) out[e] = (float)(((red[0][o] + red[1][o]) + red[2][o]) + red[3][o]);
+    if (zl == 0 && e < n) {
+        double t = red[0][o];
+        for (int k = 1; k < 8; k++) t += red[k][o];
+        const long q = e / Rp, r = e - q * Rp;
+        if (r < R) out[q + Q * r] = (float)t;
+    }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -493,7 +620,31 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 struct TcPlan {
     int kind;
     long P, Q, S, Rpad, psteps, stages, qtiles, splits, chunk;
+    bool fast;
+    int nx, nb, ctas_per_sm;
 };
+
+// Launch shape: two CTAs per SM when their shared memory and TMEM (two D
+// buffers + 32 columns per A stage, at most 256 each) fit with 3 or 4
+// stages in both rings, else one CTA with 4; then enough contraction splits
+// to fill every SM.  (The X ring and the U/B/A ring are separate and could
+// differ in depth; a deeper X ring measured slower here.)
+void tc_shape(TcPlan &p) {
+    constexpr size_t kTwoCtaSmem = 115712;   // (228 KB - 2 x 1 KB reserved) / 2
+    p.ctas_per_sm = 1;
+    p.nx = p.nb = 4;
+    for (int n = 4; n >= 3; n--) {
+        if (tc_smem_bytes((int)p.Rpad, p.fast, n, n) <= kTwoCtaSmem && 2 * p.Rpad + 32 * n <= 256) {
+            p.ctas_per_sm = 2;
+            p.nx = p.nb = n;
+            break;
+        }
+    }
+    long want = std::max(1L, (p.ctas_per_sm * (long)kNumSMs) / p.qtiles);
+    p.splits = std::min(want, p.stages);
+    p.chunk = (p.stages + p.splits - 1) / p.splits;
+    p.splits = (p.stages + p.chunk - 1) / p.chunk;
+}
 
 bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPlan &p) {
     if (!(precision == CUD_PREC_BF16 || precision == CUD_PREC_FP16 || precision == CUD_PREC_BF16X3 ||
@@ -513,24 +664,26 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     p.stages = (p.kind == 0) ? (v.S + BKS - 1) / BKS : v.S * p.psteps;
     if (p.kind == 0 && p.stages * BKS > 0x7fffffffL) return false;
     p.qtiles = (v.Q + BQ - 1) / BQ;
-    long want = std::max(1L, (2L * kNumSMs) / p.qtiles);
-    p.splits = std::min(want, p.stages);
-    p.chunk = (p.stages + p.splits - 1) / p.splits;
-    p.splits = (p.stages + p.chunk - 1) / p.chunk;
+    // fast KR path: the fastest generating factor's row count is a multiple
+    // of 32, so each stage covers 32 of its rows (one TMA box)
+    const long rows0 = (mode == 0) ? dims[1] : dims[0];
+    p.fast = (rows0 % BKS == 0);
+    tc_shape(p);
     return true;
 }
 
-template <int KIPT, int MINB>
-int launch_tc(const CUtensorMap &tmap, const TcArgs &a, unsigned grid, cudaStream_t s) {
+template <int KIPT, int CIPT, int MINB>
+int launch_tc(const CUtensorMap &tmap, const CUtensorMap &umap, const TcArgs &a, size_t smem, unsigned grid,
+              cudaStream_t s) {
     static bool attr[64] = {false};
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && !attr[dev]) {
-        CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_tc<KIPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)tc_smem_bytes(RPAD_MAX)));
+        CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_tc<KIPT, CIPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       232448));
         attr[dev] = true;
     }
-    k_mttkrp_tc<KIPT, MINB><<<grid, NTHREADS, tc_smem_bytes(a.Rpad), s>>>(tmap, a);
+    k_mttkrp_tc<KIPT, CIPT, MINB><<<grid, NTHREADS, smem, s>>>(tmap, umap, a);
     CUD_CHECK_LAUNCH("mttkrp_tc");
     return CUD_OK;
 }
@@ -541,7 +694,7 @@ int mttkrp_tc_query(int order, const long *dims, int mode, long R, int precision
     TcPlan p;
     if (!tc_plan(order, dims, mode, R, precision, p)) return CUD_ERR_UNSUPPORTED;
     if (!encode_fn()) return CUD_ERR_UNSUPPORTED;
-    if (ws_bytes) *ws_bytes = sizeof(float) * (size_t)p.splits * R * p.Q + 256;
+    if (ws_bytes) *ws_bytes = sizeof(float) * (size_t)p.splits * ((R + 3) / 4 * 4) * p.Q + 256;
     return CUD_OK;
 }
 
@@ -572,6 +725,26 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     }
     if (cr != CUDA_SUCCESS) return CUD_ERR_UNSUPPORTED;
+    const float *U0 = U[(mode == 0) ? 1 : 0];
+    // A misaligned fastest factor takes the general KR path; the launch shape
+    // (stages, splits, shared memory) stays the planned one, so the workspace
+    // sized by mttkrp_tc_query still holds.
+    const bool fast = p.fast && ((reinterpret_cast<uintptr_t>(U0) & 15) == 0);
+    CUtensorMap umap;
+    memset(&umap, 0, sizeof(umap));
+    if (fast) {
+        // the fastest generating factor (rows0 x R, column-major): a box of
+        // 32 rows x Rpad columns per stage; columns >= R read as zero
+        const long rows0 = (mode == 0) ? dims[1] : dims[0];
+        cuuint64_t gdim[2] = {(cuuint64_t)rows0, (cuuint64_t)R};
+        cuuint64_t gstride[1] = {(cuuint64_t)rows0 * 4};
+        cuuint32_t box[2] = {BKS, (cuuint32_t)p.Rpad};
+        cuuint32_t estr[2] = {1, 1};
+        cr = encode(&umap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(U0), gdim, gstride, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (cr != CUDA_SUCCESS) return CUD_ERR_UNSUPPORTED;
+    }
 
     TcArgs a;
     a.P = p.P; a.Q = p.Q; a.S = p.S; a.R = R;
@@ -582,6 +755,15 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     a.stages = p.stages;
     a.chunk = p.chunk;
     a.qtiles = p.qtiles;
+    a.nx = p.nx;
+    a.nb = p.nb;
+    a.Rp = (R + 3) / 4 * 4;
+    // B items: 4 per padded row; the KR warps take about half (whole warps of
+    // work, at least 64), the converters the rest
+    const int ni = 4 * (int)p.Rpad;
+    a.nkri = std::max(64, (ni / 2) / 64 * 64);
+    const int kipt_need = a.nkri / NKR;
+    const int cipt_need = (ni - a.nkri + NCONV - 1) / NCONV;
     a.gen.n = 0;
     a.outer.n = 0;
     for (int m = 0; m < order; m++) {
@@ -591,27 +773,27 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
         f.rows[f.n] = dims[m];
         f.n++;
     }
-    // Fast KR path: every stage covers 32 consecutive rows of the fastest
-    // generating factor (its row count is a multiple of 32) and that
-    // factor's columns can be read as aligned 128-bit vectors.
-    a.fast = (a.gen.rows[0] % BKS == 0) && ((reinterpret_cast<uintptr_t>(a.gen.U[0]) & 15) == 0);
+    a.fast = fast ? 1 : 0;
     char *w = static_cast<char *>(ws);
     a.error = reinterpret_cast<int *>(w);
     a.part = reinterpret_cast<float *>(w + 256);
     CUD_CHECK(cudaMemsetAsync(a.error, 0, sizeof(int), s));
-    // two D buffers + NST A stages of 32 columns, rounded to a power of two
-    a.tmem_cols = (2 * p.Rpad + NST * 32 <= 256) ? 256u : 512u;
+    // two D buffers + nst A stages of 32 columns, rounded to a power of two
+    a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;
     unsigned grid = (unsigned)(p.qtiles * p.splits);
-    // KR items (row, 8-kappa chunk) per producer thread: 4 Rpad / 64
-    int kipt = (int)((4 * p.Rpad + NKR - 1) / NKR);
+    const size_t smem = tc_smem_bytes((int)p.Rpad, p.fast, p.nx, p.nb);
     int st;
-    if (kipt <= 1) st = launch_tc<1, 2>(tmap, a, grid, s);
-    else if (kipt <= 2) st = launch_tc<2, 2>(tmap, a, grid, s);
-    else if (kipt <= 4) st = launch_tc<4, 2>(tmap, a, grid, s);
-    else st = launch_tc<8, 1>(tmap, a, grid, s);
+    if (p.ctas_per_sm == 2) {
+        if (kipt_need <= 1 && cipt_need <= 0) st = launch_tc<1, 0, 2>(tmap, umap, a, smem, grid, s);
+        else if (kipt_need <= 1 && cipt_need <= 1) st = launch_tc<1, 1, 2>(tmap, umap, a, smem, grid, s);
+        else if (kipt_need <= 2 && cipt_need <= 1) st = launch_tc<2, 1, 2>(tmap, umap, a, smem, grid, s);
+        else st = launch_tc<4, 2, 2>(tmap, umap, a, smem, grid, s);
+    } else {
+        if (kipt_need <= 2 && cipt_need <= 2) st = launch_tc<2, 2, 1>(tmap, umap, a, smem, grid, s);
+        else st = launch_tc<4, 2, 1>(tmap, umap, a, smem, grid, s);
+    }
     if (st) return st;
-    long n = R * p.Q;
-    k_sum_tc_partials<<<(unsigned)((n + 63) / 64), 256, 0, s>>>(a.part, (int)p.splits, n, out);
+    k_sum_tc_partials<<<(unsigned)((p.Q * a.Rp + 31) / 32), 256, 0, s>>>(a.part, (int)p.splits, p.Q, R, a.Rp, out);
     CUD_CHECK_LAUNCH("mttkrp_tc reduce");
     return CUD_OK;
 }

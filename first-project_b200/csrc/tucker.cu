@@ -96,15 +96,42 @@ bool valid(int order, const long *dims, const long *ranks, float *const *U, cons
 
 }  // namespace
 
+// tucker_tc.cu
+bool tucker_tc_supported(int order, const long *dims, const long *ranks);
+int tucker_tc_factors(const float *X, int order, const long *dims, const long *ranks, float *const *U, int n0,
+                      bool three, cudaStream_t s, int *worst);
+int tucker_tc_core(const float *X, int order, const long *dims, const long *ranks, float *const *U, float *core,
+                   bool three, cudaStream_t s);
+int tucker_tc_hooi_sweep(const float *X, int order, const long *dims, const long *ranks, float *const *U,
+                         bool three, cudaStream_t s, int *worst);
+
 }  // namespace cud
 
 using namespace cud;
 
+namespace {
+
+// Tensor cores for every precision but FP32 (CUD_PREC_BF16: one-term Grams;
+// BF16X3 / DEFAULT: three-term Grams; TTMs BF16), when the extents allow.
+bool use_tc(int precision, int order, const long *dims, const long *ranks) {
+    return precision != CUD_PREC_FP32 && precision != CUD_PREC_FP16 && tucker_tc_supported(order, dims, ranks);
+}
+
+}  // namespace
+
 extern "C" int cud_tucker_hosvd(const float *X, int order, const long *dims, const long *ranks,
                                 float *core, float *const *U, int precision, void *stream) {
-    (void)precision;
     if (!valid(order, dims, ranks, U, X, core)) return set_status(CUD_ERR_INVALID_ARGUMENT);
     cudaStream_t s = as_stream(stream);
+    if (use_tc(precision, order, dims, ranks)) {
+        const bool three = precision != CUD_PREC_BF16;
+        int worst = CUD_OK;
+        int st = tucker_tc_factors(X, order, dims, ranks, U, 0, three, s, &worst);
+        if (st == CUD_OK) st = tucker_tc_core(X, order, dims, ranks, U, core, three, s);
+        if (st) return set_status(st);
+        CUD_CHECK(cudaStreamSynchronize(s));
+        return set_status(worst);
+    }
     TuckerWork w;
     int st = alloc_work(order, dims, ranks, w);
     if (st) return set_status(st);
@@ -124,9 +151,20 @@ extern "C" int cud_tucker_hosvd(const float *X, int order, const long *dims, con
 
 extern "C" int cud_tucker_hooi(const float *X, int order, const long *dims, const long *ranks,
                                float *core, float *const *U, int sweeps, int precision, void *stream) {
-    (void)precision;
     if (!valid(order, dims, ranks, U, X, core) || sweeps < 0) return set_status(CUD_ERR_INVALID_ARGUMENT);
     cudaStream_t s = as_stream(stream);
+    if (use_tc(precision, order, dims, ranks)) {
+        const bool three = precision != CUD_PREC_BF16;
+        int worst = CUD_OK;
+        // initial U_2..U_N from the Grams (tucker_hooi.cu:45-75), U_1 too when no sweep runs
+        int st = tucker_tc_factors(X, order, dims, ranks, U, sweeps > 0 ? 1 : 0, three, s, &worst);
+        for (int it = 0; it < sweeps && st == CUD_OK; it++)
+            st = tucker_tc_hooi_sweep(X, order, dims, ranks, U, three, s, &worst);
+        if (st == CUD_OK) st = tucker_tc_core(X, order, dims, ranks, U, core, three, s);
+        if (st) return set_status(st);
+        CUD_CHECK(cudaStreamSynchronize(s));
+        return set_status(worst);
+    }
     TuckerWork w;
     int st = alloc_work(order, dims, ranks, w);
     if (st) return set_status(st);

@@ -1,0 +1,349 @@
+// Tucker HOSVD / HOOI on the tensor cores: the unfolding Grams and the TTM
+// chains are BF16 GEMMs with FP32 accumulation (gemm_tc.cu); the Gram
+// eigenproblems stay in FP64 (eig.cu).  Same algorithm and factor convention
+// as tucker.cu (src/tucker_hosvd.cu:3-103, src/tucker4_hosvd.cu:3-141,
+// decomposition/GPU/normal/tucker/tucker_hooi.cu:3-218); the reference runs
+// its Grams as FP32 SGEMMs and its TTMs as FP16 GemmEx (src/ttm.cu:4-47).
+//
+// Layout trick: the GEMM wants its contraction index contiguous.  A TTM over
+// the fastest mode of a column-major tensor is such a GEMM as it stands, and
+// writing its output with the new rank index slowest -- (d_1, ..., d_N-1, r_0)
+// -- makes the next mode the fastest one.  So the HOSVD core is N GEMMs over a
+// BF16 copy of X with no transposes, and each HOOI projection is one rotating
+// copy of X followed by N-1 such GEMMs.  Gram operands X_(n) (rows = mode n,
+// the other modes contiguous) come from one convert-and-unfold kernel.
+//
+// Precision: BF16 -> Grams from one BF16 GEMM; BF16X3 / DEFAULT -> Grams
+// from the three-term split (hi hi + hi lo + lo hi).  TTMs are BF16 in both.
+#include <cuda_bf16.h>
+
+#include "kernels.cuh"
+
+namespace cud {
+
+namespace {
+
+__device__ __forceinline__ void put_split(__nv_bfloat16 *hi, __nv_bfloat16 *lo, long o, float x) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    hi[o] = h;
+    if (lo) lo[o] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
+// View X as (Q, S) with q fastest (a (P = 1, Q, S) mode view): out[q*S + s],
+// 32 x 32 tiles through shared memory (coalesced on both sides).
+__global__ void __launch_bounds__(256) k_unfold_t(const float *__restrict__ X, long Q, long S,
+                                                  __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
+    __shared__ float tile[32][33];
+    const long tq = (Q + 31) / 32, ts = (S + 31) / 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (long t = blockIdx.x; t < tq * ts; t += gridDim.x) {
+        const long q0 = (t % tq) * 32, s0 = (t / tq) * 32;
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            const long q = q0 + tx, s = s0 + k;
+            tile[k][tx] = (q < Q && s < S) ? X[q + Q * s] : 0.f;
+        }
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            const long q = q0 + k, s = s0 + tx;
+            if (q < Q && s < S) put_split(hi, lo, q * S + s, tile[tx][k]);
+        }
+    }
+}
+
+// View X as (P, Q, S), P > 1: out[q*(P*S) + p + P*s] = X[p + P*q + P*Q*s];
+// each (q, s) pair is a run of P contiguous values on both sides.
+__global__ void __launch_bounds__(256) k_unfold_runs(const float *__restrict__ X, long P, long Q, long S,
+                                                     __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
+    const long rows = Q * S;
+    for (long qs = blockIdx.y; qs < rows; qs += gridDim.y) {
+        const long q = qs / S, s = qs - q * S;
+        const float *src = X + P * q + P * Q * s;
+        const long o = q * (P * S) + P * s;
+        for (long p = blockIdx.x * 256L + threadIdx.x; p < P; p += (long)gridDim.x * 256L)
+            put_split(hi, lo, o + p, src[p]);
+    }
+}
+
+// A BF16 (Q, S) matrix with q fastest -> rows of q with s contiguous, row
+// stride Sp >= S, the pad columns S..Sp-1 zero.
+__global__ void __launch_bounds__(256) k_transpose_bf16(const __nv_bfloat16 *__restrict__ X, long Q, long S,
+                                                        long Sp, __nv_bfloat16 *__restrict__ out) {
+    __shared__ __nv_bfloat16 tile[32][34];
+    const long tq = (Q + 31) / 32, ts = (Sp + 31) / 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (long t = blockIdx.x; t < tq * ts; t += gridDim.x) {
+        const long q0 = (t % tq) * 32, s0 = (t / tq) * 32;
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            const long q = q0 + tx, s = s0 + k;
+            tile[k][tx] = (q < Q && s < S) ? X[q + Q * s] : __float2bfloat16_rn(0.f);
+        }
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            const long q = q0 + k, s = s0 + tx;
+            if (q < Q && s < Sp) out[q * Sp + s] = tile[tx][k];
+        }
+    }
+}
+
+__global__ void k_f32_to_f64(const float *__restrict__ a, double *__restrict__ b, long n) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        b[e] = (double)a[e];
+}
+
+__global__ void k_take_top_f32(const double *__restrict__ V, long n, long r, float *__restrict__ U) {
+    const long total = n * r;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long i = e % n, j = e / n;
+        U[e] = (float)V[i + n * (n - r + j)];
+    }
+}
+
+__global__ void k_to_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict__ b, long n) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        b[e] = __float2bfloat16_rn(a[e]);
+}
+
+unsigned gfor(long n) { return (unsigned)std::min<long>((n + 255) / 256, 16L * kNumSMs); }
+
+// X viewed as (P, Q, S) -> X_(view) rows of Q, the rest contiguous (BF16).
+int unfold_bf16(const float *X, long P, long Q, long S, __nv_bfloat16 *hi, __nv_bfloat16 *lo, cudaStream_t s) {
+    if (P == 1) {
+        const long tiles = ((Q + 31) / 32) * ((S + 31) / 32);
+        k_unfold_t<<<(unsigned)std::min<long>(tiles, 16L * kNumSMs), 256, 0, s>>>(X, Q, S, hi, lo);
+    } else {
+        const unsigned gx = (unsigned)std::min<long>((P + 255) / 256, 64);
+        const unsigned gy = (unsigned)std::min<long>(Q * S, 65535);
+        k_unfold_runs<<<dim3(gx, gy), 256, 0, s>>>(X, P, Q, S, hi, lo);
+    }
+    CUD_CHECK_LAUNCH("unfold_bf16");
+    return CUD_OK;
+}
+
+struct TcWork {
+    __nv_bfloat16 *xb = nullptr;       // X in BF16 (rotated as needed), total
+    __nv_bfloat16 *uh = nullptr, *ul = nullptr;  // Gram operands, total each
+    __nv_bfloat16 *z0 = nullptr, *z1 = nullptr;  // chain intermediates
+    __nv_bfloat16 *ub = nullptr;       // a factor in BF16
+    float *g32 = nullptr;              // Gram FP32
+    double *g64 = nullptr, *W = nullptr, *V = nullptr;
+    void *gws = nullptr;               // GEMM workspace
+    size_t gws_bytes = 0;
+};
+
+int tc_alloc(int order, const long *dims, const long *ranks, bool three, TcWork &w) {
+    long total = 1, maxd = 0, maxr = 0;
+    for (int m = 0; m < order; m++) {
+        total *= dims[m];
+        maxd = std::max(maxd, dims[m]);
+        maxr = std::max(maxr, ranks[m]);
+    }
+    // largest chain intermediate: X with one mode reduced to its rank
+    long zmax = 0;
+    for (int m = 0; m < order; m++) zmax = std::max(zmax, total / dims[m] * ranks[m]);
+    // GEMM workspace: the largest of the Gram and TTM shapes used
+    size_t gw = 0;
+    for (int m = 0; m < order; m++) {
+        gw = std::max(gw, gemm_tc_ws_bytes(dims[m], dims[m], total / dims[m]));
+        gw = std::max(gw, gemm_tc_ws_bytes(total / dims[m], ranks[m], dims[m]));
+        long rest = 1;
+        for (int q = 0; q < order; q++)
+            if (q != m) rest *= ranks[q];
+        gw = std::max(gw, gemm_tc_ws_bytes(dims[m], dims[m], (rest + 7) / 8 * 8));
+    }
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t off = 0;
+    const size_t o_xb = off; off += up(2 * (size_t)total);
+    const size_t o_uh = off; off += up(2 * (size_t)total);
+    const size_t o_ul = off; off += three ? up(2 * (size_t)total) : 0;
+    const size_t o_z0 = off; off += up(2 * (size_t)zmax);
+    const size_t o_z1 = off; off += up(2 * (size_t)zmax);
+    const size_t o_ub = off; off += up(2 * (size_t)maxd * maxr);
+    const size_t o_g32 = off; off += up(4 * (size_t)maxd * maxd);
+    const size_t o_g64 = off; off += up(8 * (size_t)maxd * maxd);
+    const size_t o_W = off; off += up(8 * (size_t)maxd);
+    const size_t o_V = off; off += up(8 * (size_t)maxd * maxd);
+    const size_t o_gws = off; off += up(gw);
+    int st;
+    char *p = static_cast<char *>(scratch(kSlotTmp1, off, &st));
+    if (!p) return st;
+    w.xb = (__nv_bfloat16 *)(p + o_xb);
+    w.uh = (__nv_bfloat16 *)(p + o_uh);
+    w.ul = three ? (__nv_bfloat16 *)(p + o_ul) : nullptr;
+    w.z0 = (__nv_bfloat16 *)(p + o_z0);
+    w.z1 = (__nv_bfloat16 *)(p + o_z1);
+    w.ub = (__nv_bfloat16 *)(p + o_ub);
+    w.g32 = (float *)(p + o_g32);
+    w.g64 = (double *)(p + o_g64);
+    w.W = (double *)(p + o_W);
+    w.V = (double *)(p + o_V);
+    w.gws = p + o_gws;
+    w.gws_bytes = gw;
+    return CUD_OK;
+}
+
+GemmEpi epi_f32(float *out, long ldm, long ldn, int accumulate) {
+    GemmEpi e;
+    memset(&e, 0, sizeof(e));
+    e.alpha = 1.f;
+    e.out_f32 = out; e.f32_ldm = ldm; e.f32_ldn = ldn; e.f32_accumulate = accumulate;
+    return e;
+}
+
+// Gram (I x I, FP64 into w.g64) of the rows of the I x K BF16 operands:
+// hi hi^T, plus hi lo^T + lo hi^T when use_lo.
+int gram_tc(const TcWork &w, long I, long K, bool use_lo, cudaStream_t s) {
+    if (gemm_tc_ws_bytes(I, I, K) > w.gws_bytes) return CUD_ERR_INVALID_ARGUMENT;
+    int st = gemm_tc_bf16(w.uh, K, w.uh, K, I, I, K, epi_f32(w.g32, I, 1, 0), w.gws, s);
+    if (st) return st;
+    if (use_lo && w.ul) {
+        if ((st = gemm_tc_bf16(w.uh, K, w.ul, K, I, I, K, epi_f32(w.g32, I, 1, 1), w.gws, s))) return st;
+        if ((st = gemm_tc_bf16(w.ul, K, w.uh, K, I, I, K, epi_f32(w.g32, I, 1, 1), w.gws, s))) return st;
+    }
+    k_f32_to_f64<<<gfor(I * I), 256, 0, s>>>(w.g32, w.g64, I * I);
+    CUD_CHECK_LAUNCH("gram_tc");
+    return CUD_OK;
+}
+
+// U (I x r, FP32) = eigenvectors of the r largest eigenvalues of w.g64.
+int top_vectors(const TcWork &w, long I, long r, float *U, cudaStream_t s) {
+    int st = syev_jacobi(w.g64, I, w.W, w.V, 60, s);
+    if (st != CUD_OK && st != CUD_ERR_NOT_CONVERGED) return st;
+    k_take_top_f32<<<gfor(I * r), 256, 0, s>>>(w.V, I, r, U);
+    CUD_CHECK_LAUNCH("top_vectors");
+    return st;
+}
+
+// One TTM over the fastest mode: T (K x rest, K fastest, BF16) times U
+// (K x r, FP32) -> (rest x r) with r slowest: BF16 into zout, or FP32 into
+// fout.  Returns the GEMM status.
+int ttm_fast(const TcWork &w, const __nv_bfloat16 *T, long K, long rest, const float *U, long r,
+             __nv_bfloat16 *zout, float *fout, cudaStream_t s) {
+    if (gemm_tc_ws_bytes(rest, r, K) > w.gws_bytes) return CUD_ERR_INVALID_ARGUMENT;
+    k_to_bf16<<<gfor(K * r), 256, 0, s>>>(U, w.ub, K * r);
+    CUD_CHECK_LAUNCH("ttm factor bf16");
+    GemmEpi e;
+    memset(&e, 0, sizeof(e));
+    e.alpha = 1.f;
+    if (fout) { e.out_f32 = fout; e.f32_ldm = 1; e.f32_ldn = rest; }
+    else { e.out_bf16 = zout; e.bf16_ldm = 1; e.bf16_ldn = rest; }
+    return gemm_tc_bf16(T, K, w.ub, K, rest, r, K, e, w.gws, s);
+}
+
+// Contracts modes `first`, first+1, ... (cyclically) of T -- laid out with
+// mode `first` fastest, cyclic order -- except mode `skip` (or none when
+// skip < 0, all `order` modes).  Returns the BF16 buffer holding the result
+// (or writes FP32 `final_out` at the last step) and its element count.
+int chain(const TcWork &w, const __nv_bfloat16 *T, int order, const long *dims, const long *ranks,
+          float *const *U, int first, int skip, float *final_out, const __nv_bfloat16 **res, cudaStream_t s) {
+    long cur[2 * kMaxOrder];  // sizes in layout order
+    for (int k = 0; k < order; k++) cur[k] = dims[(first + k) % order];
+    long total = 1;
+    for (int k = 0; k < order; k++) total *= cur[k];
+    const int nsteps = (skip < 0) ? order : order - 1;
+    const __nv_bfloat16 *src = T;
+    for (int step = 0; step < nsteps; step++) {
+        const int m = (first + step) % order;  // the fastest mode now
+        const long K = cur[step];
+        const long rest = total / K;
+        const bool last = (step == nsteps - 1);
+        __nv_bfloat16 *dst = (step & 1) ? w.z1 : w.z0;
+        int st = ttm_fast(w, src, K, rest, U[m], ranks[m], dst, (last && final_out) ? final_out : nullptr, s);
+        if (st) return st;
+        cur[order + step] = ranks[m];
+        total = rest * ranks[m];
+        src = dst;
+    }
+    *res = src;
+    return CUD_OK;
+}
+
+bool tc_ok(int order, const long *dims, const long *ranks) {
+    if (order < 2 || order > kMaxOrder) return false;
+    for (int m = 0; m < order; m++)
+        if (dims[m] % 8 != 0) return false;  // GEMM leading dimensions
+    long total = 1;
+    for (int m = 0; m < order; m++) total *= dims[m];
+    return total / dims[order - 1] % 8 == 0;
+}
+
+}  // namespace
+
+bool tucker_tc_supported(int order, const long *dims, const long *ranks) { return tc_ok(order, dims, ranks); }
+
+// The HOSVD factors of the given modes (U[n] for n in [n0, order)) from BF16
+// Gram GEMMs.
+int tucker_tc_factors(const float *X, int order, const long *dims, const long *ranks, float *const *U, int n0,
+                      bool three, cudaStream_t s, int *worst) {
+    TcWork w;
+    int st = tc_alloc(order, dims, ranks, three, w);
+    if (st) return st;
+    long total = 1;
+    for (int m = 0; m < order; m++) total *= dims[m];
+    for (int n = n0; n < order; n++) {
+        long P = 1, S = 1;
+        for (int m = 0; m < n; m++) P *= dims[m];
+        for (int m = n + 1; m < order; m++) S *= dims[m];
+        if ((st = unfold_bf16(X, P, dims[n], S, w.uh, w.ul, s))) return st;
+        if ((st = gram_tc(w, dims[n], total / dims[n], three, s))) return st;
+        st = top_vectors(w, dims[n], ranks[n], U[n], s);
+        if (st == CUD_ERR_NOT_CONVERGED) *worst = st;
+        else if (st) return st;
+    }
+    return CUD_OK;
+}
+
+// core = X x_0 U_0^T x_1 ... (ranks in mode order), BF16 TTM chain.
+int tucker_tc_core(const float *X, int order, const long *dims, const long *ranks, float *const *U, float *core,
+                   bool three, cudaStream_t s) {
+    TcWork w;
+    int st = tc_alloc(order, dims, ranks, three, w);
+    if (st) return st;
+    long total = 1;
+    for (int m = 0; m < order; m++) total *= dims[m];
+    if ((st = unfold_bf16(X, total, 1, 1, w.xb, nullptr, s))) return st;  // plain BF16 copy
+    const __nv_bfloat16 *res;
+    return chain(w, w.xb, order, dims, ranks, U, 0, -1, core, &res, s);
+}
+
+// One HOOI sweep: for each mode n, U_n = top eigenvectors of the Gram of
+// Y = X x_{m != n} U_m^T.
+int tucker_tc_hooi_sweep(const float *X, int order, const long *dims, const long *ranks, float *const *U,
+                         bool three, cudaStream_t s, int *worst) {
+    TcWork w;
+    int st = tc_alloc(order, dims, ranks, three, w);
+    if (st) return st;
+    long total = 1;
+    for (int m = 0; m < order; m++) total *= dims[m];
+    for (int n = 0; n < order; n++) {
+        // rotate X so mode n+1 is fastest: (P = prod_{m<=n} d_m) x rest transposed
+        long Pn = 1;
+        for (int m = 0; m <= n; m++) Pn *= dims[m];
+        const long rest = total / Pn;
+        const int first = (n + 1) % order;
+        if (rest == 1) st = unfold_bf16(X, total, 1, 1, w.xb, nullptr, s);
+        else st = unfold_bf16(X, 1, Pn, rest, w.xb, nullptr, s);
+        if (st) return st;
+        const __nv_bfloat16 *Y;
+        if ((st = chain(w, w.xb, order, dims, ranks, U, first, n, nullptr, &Y, s))) return st;
+        // Y: mode n fastest, then the other modes' ranks -> rows of mode n
+        long R = 1;
+        for (int m = 0; m < order; m++)
+            if (m != n) R *= ranks[m];
+        // Y (BF16) has mode n fastest: a tiled transpose gives the Gram
+        // operand's rows; Y is already rounded, so there is no low part
+        // rows padded to a multiple of 8 (the GEMM's leading-dimension rule)
+        const long Rp = (R + 7) / 8 * 8;
+        const long tiles = ((dims[n] + 31) / 32) * ((Rp + 31) / 32);
+        k_transpose_bf16<<<(unsigned)std::min<long>(tiles, 16L * kNumSMs), 256, 0, s>>>(Y, dims[n], R, Rp, w.uh);
+        CUD_CHECK_LAUNCH("hooi transpose");
+        if ((st = gram_tc(w, dims[n], Rp, false, s))) return st;
+        st = top_vectors(w, dims[n], ranks[n], U[n], s);
+        if (st == CUD_ERR_NOT_CONVERGED) *worst = st;
+        else if (st) return st;
+    }
+    return CUD_OK;
+}
+
+}  // namespace cud

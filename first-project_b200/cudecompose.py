@@ -124,6 +124,22 @@ _sig("cud_cp_plan_destroy", [_vp])
 _sig("cud_cp_als_batched", [_i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ctypes.POINTER(_l), _vp,
                             ctypes.POINTER(_l), ctypes.POINTER(CpOptions), ctypes.POINTER(_d),
                             ctypes.POINTER(_i), ctypes.POINTER(_i), _vp])
+_sig("cud_cp_als_batched_target", [_i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ctypes.POINTER(_l), _vp,
+                                   ctypes.POINTER(_l), ctypes.POINTER(CpOptions), ctypes.POINTER(_d),
+                                   ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_i), _vp])
+_sig("cud_ws_model_create", [_i, _i, _i, _i, ctypes.c_ulonglong, ctypes.POINTER(_vp)])
+_sig("cud_ws_model_destroy", [_vp])
+_sig("cud_ws_model_params", [_vp, ctypes.POINTER(_vp), _i])
+_sig("cud_ws_model_grads", [_vp, ctypes.POINTER(_vp)])
+_sig("cud_ws_backward", [_vp, _vp, _vp, _vp, _i, ctypes.POINTER(_d), _vp])
+_sig("cud_ws_train_step", [_vp, _vp, _vp, _vp, _i, ctypes.c_float, ctypes.POINTER(_d), _vp])
+_sig("cud_ws_predict", [_vp, _vp, _i, _vp, _vp])
+_sig("cud_ws_generate", [_l, _l, ctypes.c_ulonglong, _i, _i, _d, _vp, _vp, _vp, _vp])
+_sig("cud_ws_omega", [_i, _i, ctypes.c_ulonglong, _vp, _vp])
+_sig("cud_ws_features", [_vp, _l, _i, _vp, _i, _vp, _vp, _vp, _vp])
+_sig("cud_ws_canonical", [_vp, _vp, _l, _i, _i, _vp])
+_sig("cud_ws_uncanonical", [_vp, _vp, _vp, _l, _i, _i, _vp])
+_sig("cud_ws_hosvd_init", [_vp, _l, _i, _i, _vp, _vp])
 _sig("cud_cp_batched_tune", [_i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ctypes.POINTER(_l), _vp,
                              ctypes.POINTER(_l), ctypes.POINTER(_i), ctypes.POINTER(_i), _vp])
 _sig("cud_factor_gram", [_vp, _l, _l, _vp, _vp])
@@ -480,6 +496,21 @@ def cp_als_batched(batch, max_sweeps=50, tol=1e-6, use_graph=True, sweeps_per_gr
     _check(_lib.cud_cp_als_batched(batch.n, d, r, _ptr(batch.X), xo, _ptr(batch.U), uo,
                                    ctypes.byref(opt), fits, sw, ctypes.byref(launches),
                                    _stream(stream)), "cp_als_batched")
+    return list(fits), list(sw), launches.value
+
+
+def cp_als_batched_target(batch, targets, max_sweeps=50, use_graph=True, sweeps_per_graph=1, stream=None):
+    """Batched CP-ALS where tensor t stops once its fit >= targets[t].
+    Returns (fits, sweeps, kernel_launches)."""
+    d, r, xo, uo = batch._args()
+    opt = CpOptions(max_sweeps, 0.0, PREC_FP32, 1 if use_graph else 0, sweeps_per_graph, 0.0)
+    tg = (_d * batch.n)(*[float(x) for x in targets])
+    fits = (_d * batch.n)()
+    sw = (_i * batch.n)()
+    launches = _i(0)
+    _check(_lib.cud_cp_als_batched_target(batch.n, d, r, _ptr(batch.X), xo, _ptr(batch.U), uo,
+                                          ctypes.byref(opt), tg, fits, sw, ctypes.byref(launches),
+                                          _stream(stream)), "cp_als_batched_target")
     return list(fits), list(sw), launches.value
 
 

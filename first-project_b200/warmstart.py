@@ -1,0 +1,231 @@
+"""Learned warm start for CP-ALS: host pipeline over the library's C ABI.
+
+A multilayer perceptron (3*I*S -> hidden -> hidden -> 3*I*R, ReLU) maps
+Gaussian sketches of a tensor's three mode unfoldings, X_(m) Omega_m scaled
+by 1/||X||, to the canonical form of its CP factors (unit, sign-fixed columns
+of U_0 and U_1; weights in U_2 / ||X||; columns by weight).  Everything that
+touches the data runs in the library's kernels: the seeded workload generator
+(cud_ws_generate), the sketches (a BF16 tensor-core GEMM per mode,
+cud_ws_features), the training targets (ALS solutions from the library's own
+batched CP-ALS, cud_cp_als_batched, then cud_ws_canonical), the network's
+forward / backward / Adam (cud_ws_train_step on tcgen05 GEMMs), the HOSVD
+initialisation the network is judged against (cud_ws_hosvd_init: per-tensor
+mode Grams and Jacobi eigenvectors, the reference's src/tucker_hosvd.cu
+method), and the ALS that both initialisations feed
+(cud_cp_als_batched_target, src/cp_als.cu's update).  PyTorch only holds the
+device buffers.
+
+The reference has no learned component; plain HOSVD-initialised ALS stays the
+fallback and the judge: both runs stop at the same per-tensor fit.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+import cudecompose as cd
+
+_lib = cd.library()
+_F = ctypes.c_void_p
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class WarmStartMLP:
+    """The network: FP32 master weights and Adam state on the device
+    (cud_ws_model_*).  Parameters in the order W1, b1, W2, b2, W3, b3 with
+    W row-major (out x in)."""
+
+    def __init__(self, in_dim, hidden, out_dim, max_batch, seed=0):
+        self.in_dim, self.hidden, self.out_dim, self.max_batch = in_dim, hidden, out_dim, max_batch
+        h = ctypes.c_void_p()
+        cd._check(_lib.cud_ws_model_create(in_dim, hidden, out_dim, max_batch, seed, ctypes.byref(h)),
+                  "ws_model_create")
+        self._h = h
+
+    def shapes(self):
+        H, D, O = self.hidden, self.in_dim, self.out_dim
+        return [(H, D), (H,), (H, H), (H,), (O, H), (O,)]
+
+    def _host_arrays(self, arrays=None):
+        if arrays is None:
+            arrays = [np.zeros(s, np.float32) for s in self.shapes()]
+        arrays = [np.ascontiguousarray(a, dtype=np.float32) for a in arrays]
+        ptrs = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in arrays])
+        return arrays, ptrs
+
+    def get_params(self):
+        arrays, ptrs = self._host_arrays()
+        cd._check(_lib.cud_ws_model_params(self._h, ptrs, 0), "ws_model_params")
+        return arrays
+
+    def set_params(self, arrays):
+        arrays, ptrs = self._host_arrays(arrays)
+        cd._check(_lib.cud_ws_model_params(self._h, ptrs, 1), "ws_model_params")
+
+    def grads(self):
+        arrays, ptrs = self._host_arrays()
+        cd._check(_lib.cud_ws_model_grads(self._h, ptrs), "ws_model_grads")
+        return arrays
+
+    def backward(self, inp, inp_t, target, stream=None):
+        loss = ctypes.c_double(0.0)
+        cd._check(_lib.cud_ws_backward(self._h, _p(inp), _p(inp_t), _p(target), inp.shape[0],
+                                       ctypes.byref(loss), cd._stream(stream)), "ws_backward")
+        return loss.value
+
+    def train_step(self, inp, inp_t, target, lr, stream=None, want_loss=True):
+        loss = ctypes.c_double(0.0)
+        cd._check(_lib.cud_ws_train_step(self._h, _p(inp), _p(inp_t), _p(target), inp.shape[0], lr,
+                                         ctypes.byref(loss) if want_loss else None, cd._stream(stream)),
+                  "ws_train_step")
+        return loss.value if want_loss else None
+
+    def predict(self, inp, out, stream=None):
+        cd._check(_lib.cud_ws_predict(self._h, _p(inp), inp.shape[0], _p(out), cd._stream(stream)),
+                  "ws_predict")
+
+    def close(self):
+        if self._h:
+            _lib.cud_ws_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class WarmStart:
+    """The smooth-factor workload (I^3 tensors, rank R, noise relative to
+    ||X_clean||), its sketches (width S) and the network that maps them to
+    initial factors."""
+
+    def __init__(self, I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256):
+        self.I, self.R, self.S, self.noise, self.seed = I, R, S, noise, seed
+        self.in_dim, self.out_dim = 3 * I * S, 3 * I * R
+        self.max_batch = max_batch
+        self.omega = torch.empty(3 * S * I * I, dtype=torch.bfloat16, device="cuda")
+        cd._check(_lib.cud_ws_omega(I, S, seed + 7919, _p(self.omega), None), "ws_omega")
+        self.model = WarmStartMLP(self.in_dim, hidden, self.out_dim, max_batch, seed)
+
+    # ---------------------------------------------------------------- data
+    def batch(self, n, id0):
+        """n tensors with ids id0.. : a cd.Batch holding X and the generating
+        factors (as its U), and ||X_clean||^2."""
+        b = cd.Batch([(self.I,) * 3] * n, [self.R] * n)
+        clean = torch.empty(n, dtype=torch.float64, device="cuda")
+        cd._check(_lib.cud_ws_generate(n, id0, self.seed, self.I, self.R, self.noise, _p(b.X), _p(b.U),
+                                       _p(clean), None), "ws_generate")
+        return b, clean
+
+    def features(self, X, t0, n):
+        """Features of tensors t0..t0+n-1 of a packed X: (in, in_t, ||X||^2)."""
+        inp = torch.empty((n, self.in_dim), dtype=torch.bfloat16, device="cuda")
+        inp_t = torch.empty((self.in_dim, n), dtype=torch.bfloat16, device="cuda")
+        xn = torch.empty(n, dtype=torch.float64, device="cuda")
+        Xp = ctypes.c_void_p(X.data_ptr() + 4 * t0 * self.I ** 3)
+        cd._check(_lib.cud_ws_features(Xp, n, self.I, _p(self.omega), self.S, _p(inp), _p(inp_t), _p(xn), None),
+                  "ws_features")
+        return inp, inp_t, xn
+
+    def targets(self, b, xnorm2, label_sweeps):
+        """ALS solutions (label_sweeps sweeps of the library's batched ALS
+        from the generating factors) in canonical form, n x 3IR."""
+        cd.cp_als_batched(b, max_sweeps=label_sweeps, tol=0.0)
+        T = b.U[: b.n * self.out_dim].clone()
+        cd._check(_lib.cud_ws_canonical(_p(T), _p(xnorm2), b.n, self.I, self.R, None), "ws_canonical")
+        return T.view(b.n, self.out_dim)
+
+    # ---------------------------------------------------------------- training
+    def train(self, n_train, batch=256, lr=1e-3, chunk=2048, label_sweeps=3, id0=0, log_every=0):
+        """One pass over n_train freshly generated tensors (ids id0..): per
+        chunk, generate, label by ALS, then one Adam step per minibatch."""
+        losses = []
+        step = 0
+        for c0 in range(0, n_train, chunk):
+            n = min(chunk, n_train - c0)
+            n -= n % batch
+            if n == 0:
+                break
+            b, _ = self.batch(n, id0 + c0)
+            xn_all = torch.empty(n, dtype=torch.float64, device="cuda")
+            feats = []
+            for t0 in range(0, n, batch):
+                inp, inp_t, xn = self.features(b.X, t0, batch)
+                xn_all[t0:t0 + batch] = xn
+                feats.append((inp, inp_t))
+            T = self.targets(b, xn_all, label_sweeps)
+            for k, t0 in enumerate(range(0, n, batch)):
+                inp, inp_t = feats[k]
+                want = log_every and step % log_every == 0
+                loss = self.model.train_step(inp, inp_t, T[t0:t0 + batch].contiguous(), lr, want_loss=bool(want))
+                if want:
+                    losses.append((step, loss))
+                step += 1
+        return losses
+
+    # ---------------------------------------------------------------- evaluation
+    def learned_init(self, b):
+        """Initial factors from the network for every tensor of batch b (into b.U)."""
+        n = b.n
+        Y = torch.empty((n, self.out_dim), dtype=torch.float32, device="cuda")
+        xn_all = torch.empty(n, dtype=torch.float64, device="cuda")
+        for t0 in range(0, n, self.max_batch):
+            m = min(self.max_batch, n - t0)
+            inp, _, xn = self.features(b.X, t0, m)
+            xn_all[t0:t0 + m] = xn
+            self.model.predict(inp, Y[t0:t0 + m])
+        cd._check(_lib.cud_ws_uncanonical(_p(Y), _p(xn_all), _p(b.U), n, self.I, self.R, None), "ws_uncanonical")
+
+    def hosvd_init(self, b):
+        cd._check(_lib.cud_ws_hosvd_init(_p(b.X), b.n, self.I, self.R, _p(b.U), None), "ws_hosvd_init")
+
+    def judged_init(self, b):
+        """Learned factors, judged against HOSVD: one ALS sweep from each, and
+        each tensor keeps the start with the better fit (its factors after
+        that sweep).  Never worse than the HOSVD start; costs the extra sweep
+        and the HOSVD initialisation."""
+        self.hosvd_init(b)
+        f_h, _, _ = cd.cp_als_batched(b, max_sweeps=1, tol=0.0)
+        U_h = b.U.clone()
+        self.learned_init(b)
+        f_l, _, _ = cd.cp_als_batched(b, max_sweeps=1, tol=0.0)
+        keep_h = torch.tensor([fh > fl for fh, fl in zip(f_h, f_l)], device="cuda")
+        per = 3 * self.I * self.R
+        Ub = b.U[: b.n * per].view(b.n, per)
+        Ub[keep_h] = U_h[: b.n * per].view(b.n, per)[keep_h]
+        return float(keep_h.float().mean().item())
+
+    def evaluate(self, n_eval, id0, margin=1e-4, max_sweeps=200, ref_sweeps=200):
+        """Sweeps and time for HOSVD-init and learned-init ALS to reach, per
+        tensor, the fit of a long ALS run from the generating factors minus
+        `margin`.  Times include the initialisation (Grams + eigensolves, or
+        sketches + network) and the ALS; the device work is timed with CUDA
+        events."""
+        b, _ = self.batch(n_eval, id0)
+        ref_fits, _, _ = cd.cp_als_batched(b, max_sweeps=ref_sweeps, tol=1e-9)
+        targets = [f - margin for f in ref_fits]
+        out = {"n": n_eval, "margin": margin, "reference_fit_mean": float(np.mean(ref_fits))}
+        for name, init in (("hosvd", self.hosvd_init), ("learned", self.learned_init),
+                           ("judged", self.judged_init)):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record()
+            init(b)
+            fits, sweeps, launches = cd.cp_als_batched_target(b, targets, max_sweeps=max_sweeps)
+            e1.record()
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            reached = [f >= t for f, t in zip(fits, targets)]
+            out[name] = {"sweeps_mean": float(np.mean(sweeps)), "sweeps_median": float(np.median(sweeps)),
+                         "reached": float(np.mean(reached)), "seconds": round(max(e0.elapsed_time(e1) * 1e-3, 0.0), 4),
+                         "wall_seconds": round(wall, 4), "sweep_kernels": launches}
+        return out

@@ -247,6 +247,13 @@ int cud_cp_als_batched(int ntensors, const long *dims, const long *ranks, const 
                        const cud_cp_options *opt, double *fits, int *sweeps, int *kernel_launches,
                        void *stream);
 
+/* cud_cp_als_batched with a per-tensor stopping fit: tensor t is done once
+ * its fit >= target_fits[t] (host array; <= 0 disables for that tensor). */
+int cud_cp_als_batched_target(int ntensors, const long *dims, const long *ranks, const float *X,
+                              const long *x_offsets, float *U, const long *u_offsets,
+                              const cud_cp_options *opt, const double *target_fits, double *fits, int *sweeps,
+                              int *kernel_launches, void *stream);
+
 /* Extension: autotunes the batched sweep's launch shape (threads per CTA,
  * CTAs per SM) for this batch's shape class by timing two sweeps per
  * candidate; U_scratch is a copy of the factors (overwritten).  The choice
@@ -292,6 +299,58 @@ int cud_cp_residual(const float *X, int order, const long *dims, const float *co
 /* Extension: the exact fit (cud_cp_residual) of the plan's current factors,
  * independent of the fit estimate the sweep derives from its last MTTKRP. */
 int cud_cp_plan_true_fit(cud_cp_plan plan, double *fit, void *stream);
+
+/* ---------------------------------------------------------------- learned warm start
+ * Extension (no counterpart in the reference): a multilayer perceptron
+ * in -> hidden -> hidden -> out (ReLU) that maps random sketches of a
+ * tensor's mode unfoldings to initial CP factors for src/cp_als.cu's ALS.
+ * FP32 master weights, BF16 tensor-core GEMMs (cud_gemm_bf16) for the
+ * forward and backward passes, Adam.  All sizes multiples of 8. */
+typedef struct cud_ws_model_s *cud_ws_model;
+
+int cud_ws_model_create(int in_dim, int hidden, int out_dim, int max_batch, unsigned long long seed,
+                        cud_ws_model *model);
+int cud_ws_model_destroy(cud_ws_model model);
+/* host[k] (k = W1, b1, W2, b2, W3, b3; W row-major out x in; NULL skips):
+ * set = 1 copies host -> model (and refreshes the BF16 copies), 0 the reverse */
+int cud_ws_model_params(cud_ws_model model, float *const *host, int set);
+/* the gradients of the last cud_ws_backward / cud_ws_train_step, same order */
+int cud_ws_model_grads(cud_ws_model model, float *const *host);
+/* in: batch x in_dim BF16 (row-major), in_t: its transpose, target: batch x
+ * out_dim FP32.  Forward + backward of the MSE loss (loss may be NULL). */
+int cud_ws_backward(cud_ws_model model, const void *in, const void *in_t, const float *target, int batch,
+                    double *loss, void *stream);
+/* cud_ws_backward followed by one Adam step (betas 0.9, 0.999) */
+int cud_ws_train_step(cud_ws_model model, const void *in, const void *in_t, const float *target, int batch,
+                      float lr, double *loss, void *stream);
+/* forward pass: out = batch x out_dim FP32 */
+int cud_ws_predict(cud_ws_model model, const void *in, int batch, float *out, void *stream);
+
+/* Workload: ntensors I^3 tensors (column-major, X[t] at X + t I^3) whose
+ * CP factors (F[t][m], I x R column-major, at F + (3t + m) I R) have
+ * columns sum_{q<3} a_q sin(2 pi w_q i / I + p_q), w ~ U[0.5, 4],
+ * p ~ U[0, 2 pi), a ~ N(0, 1), plus i.i.d. Gaussian noise of relative
+ * Frobenius size `noise`; tensor ids id0.. with `seed` (counter-based: the
+ * same (seed, id) always gives the same tensor).  clean_norm2[t] =
+ * ||X_clean||^2.  I <= 128, R <= 16, ntensors <= 65535. */
+int cud_ws_generate(long ntensors, long id0, unsigned long long seed, int I, int R, double noise, float *X,
+                    float *F, double *clean_norm2, void *stream);
+/* the three Gaussian projections Omega_m^T (S x I^2 each, BF16, N(0, 1)) */
+int cud_ws_omega(int I, int S, unsigned long long seed, void *omega, void *stream);
+/* features of each tensor: [X_(m) Omega_m for m = 0, 1, 2] / ||X|| (BF16,
+ * ntensors x 3 I S, and its transpose in_t if not NULL); xnorm2 = ||X||^2 */
+int cud_ws_features(const float *X, long ntensors, int I, const void *omega, int S, void *in, void *in_t,
+                    double *xnorm2, void *stream);
+/* canonical form of CP factors in place: unit columns of U_0, U_1 with
+ * non-negative sums, weights and signs in U_2 / ||X||, columns by weight */
+int cud_ws_canonical(float *F, const double *xnorm2, long ntensors, int I, int R, void *stream);
+/* network output (canonical, ntensors x 3 I R) -> ALS initial factors */
+int cud_ws_uncanonical(const float *Y, const double *xnorm2, float *F, long ntensors, int I, int R,
+                       void *stream);
+/* HOSVD initialisation (src/tucker_hosvd.cu:3-103 applied per tensor): the
+ * R leading eigenvectors of each mode Gram X_(m) X_(m)^T (I <= 64, Jacobi
+ * in FP32) as the initial factors F */
+int cud_ws_hosvd_init(const float *X, long ntensors, int I, int R, float *F, void *stream);
 
 /* src/cp_als.cu:20-24: the reference's initialisation -- cuRAND default
  * pseudo-random generator, seed 1234, uniform [0,1) into U[1], then U[2], ...

@@ -352,3 +352,105 @@ def unfolding_dot_khatri_rao(X3, factors, n):
         K = (factors[m][:, None, :] * K[None, :, :]).reshape(-1, K.shape[1])
     Xn = np.moveaxis(X3, n, 0).reshape(X3.shape[n], -1, order="F")
     return Xn @ K
+
+
+# ---------------------------------------------------------------- learned warm start
+# NumPy restatements of the workload generator and of the network's forward /
+# backward pass (the library's csrc/warmstart.cu and gemm_tc.cu), for the
+# warm-start parity tests.  The reference has no learned component; these pin
+# the library's own generator and training kernels.
+
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _mix64(z):
+    """SplitMix64 finaliser (Steele, Lea and Flood, OOPSLA 2014), uint64
+    arrays, wrapping arithmetic."""
+    z = np.asarray(z, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def _hash3(seed, a, b):
+    with np.errstate(over="ignore"):
+        inner = _mix64(np.asarray(b, dtype=np.uint64) + np.uint64(0x632BE59BD9B4E019))
+        mid = _mix64((np.asarray(a, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)) ^ inner)
+    return _mix64(np.uint64(seed) ^ mid)
+
+
+def _u01(h):
+    return (np.asarray(h, dtype=np.uint64) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def _normal2(h1, h2):
+    u1 = 1.0 - _u01(h1)
+    u2 = _u01(h2)
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(np.pi * 2.0 * u2)
+
+
+def ws_factors(gid, seed, I, R):
+    """Generating factors of tensor `gid`: 3 column-major I x R matrices,
+    columns sum_q a_q sin(2 pi w_q i / I + p_q)."""
+    out = []
+    i = np.arange(I, dtype=np.float64)
+    for m in range(3):
+        F = np.zeros((I, R))
+        for r in range(R):
+            col = m * R + r
+            v = np.zeros(I)
+            for q in range(3):
+                b = col * 8 + q * 2
+                w = 0.5 + 3.5 * _u01(_hash3(seed, gid, b * 4 + 0))
+                p = 2.0 * np.pi * _u01(_hash3(seed, gid, b * 4 + 1))
+                amp = _normal2(_hash3(seed, gid, b * 4 + 2), _hash3(seed, gid, b * 4 + 3))
+                v += amp * np.sin(2.0 * np.pi * w * i / I + p)
+            F[:, r] = v
+        out.append(F.astype(np.float32).astype(np.float64))
+    return out
+
+
+def ws_tensor(gid, seed, I, R, noise):
+    """The workload tensor (column-major, flattened) and its factors."""
+    F = ws_factors(gid, seed, I, R)
+    clean = np.einsum("ir,jr,kr->kji", *F).reshape(-1)  # element (i, j, k) at i + I j + I^2 k
+    n = I ** 3
+    norm2 = float(np.sum((F[0].T @ F[0]) * (F[1].T @ F[1]) * (F[2].T @ F[2])))
+    sigma = noise * np.sqrt(norm2 / n)
+    c = np.arange(n, dtype=np.uint64)
+    s2 = np.uint64(seed) ^ np.uint64(0x5BD1E995)
+    z = _normal2(_hash3(s2, gid, np.uint64(2) * c), _hash3(s2, gid, np.uint64(2) * c + np.uint64(1)))
+    return (clean + sigma * z).astype(np.float32), F, norm2
+
+
+def round_bf16_np(a):
+    """Round-to-nearest-even to BF16, returned as float64 values."""
+    x = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+    lsb = (x >> np.uint32(16)) & np.uint32(1)
+    r = (x + np.uint32(0x7FFF) + lsb) & np.uint32(0xFFFF0000)
+    return r.view(np.float32).astype(np.float64)
+
+
+def ws_mlp_grads(params, X, T):
+    """Forward + backward of the warm-start MLP with the GPU path's rounding
+    points: BF16 weights and activations, FP32 accumulation (here FP64), the
+    MSE loss 1/(B D) sum (Y - T)^2.  Returns (loss, [gW1, gb1, gW2, gb2, gW3,
+    gb3])."""
+    W1, b1, W2, b2, W3, b3 = [np.asarray(p, np.float64) for p in params]
+    W1h, W2h, W3h = round_bf16_np(W1), round_bf16_np(W2), round_bf16_np(W3)
+    X = round_bf16_np(X)
+    B, D = X.shape
+    H1 = round_bf16_np(np.maximum(X @ W1h.T + b1, 0.0))
+    H2 = round_bf16_np(np.maximum(H1 @ W2h.T + b2, 0.0))
+    Y = (H2 @ W3h.T + b3).astype(np.float32).astype(np.float64)
+    O = Y.shape[1]
+    diff = (Y - T).astype(np.float32).astype(np.float64)
+    loss = float(np.mean(diff ** 2))
+    dY = round_bf16_np(diff * (2.0 / (B * O)))
+    gW3, gb3 = dY.T @ H2, dY.sum(0)
+    dH2 = round_bf16_np((dY @ W3h) * (H2 > 0))
+    gW2, gb2 = dH2.T @ H1, dH2.sum(0)
+    dH1 = round_bf16_np((dH2 @ W2h) * (H1 > 0))
+    gW1, gb1 = dH1.T @ X, dH1.sum(0)
+    return loss, [gW1, gb1, gW2, gb2, gW3, gb3]

@@ -142,3 +142,36 @@ def test_tucker_vs_oracle(cd, dims, ranks, method):
     err = rel(host(rec).astype(np.float64), X.astype(np.float64))
     err_or = rel(oracle.gentucker(core_or, ranks, facs_or, dims), X.astype(np.float64))
     assert abs(err - err_or) <= 1e-5
+
+
+@pytest.mark.parametrize("dims,ranks", [((64, 48, 40), (8, 6, 5)), ((32, 24, 16, 40), (4, 3, 2, 5))])
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
+@pytest.mark.parametrize("method", ["hosvd", "hooi"])
+def test_tucker_tensor_cores_vs_oracle(cd, dims, ranks, precision, method):
+    """Tensor-core Grams (BF16 / three-term split) and BF16 TTM chains against
+    the FP64 oracle: the factor subspaces, and the core through the
+    reconstruction error."""
+    X = tucker_data(dims, ranks, seed=sum(dims) + len(precision))
+    dX = dev_t(X)
+    U = [torch.zeros(d * r, device="cuda") for d, r in zip(dims, ranks)]
+    core = torch.zeros(int(np.prod(ranks)), device="cuda")
+    prec = cd.PRECISIONS[precision]
+    if method == "hosvd":
+        cd.tucker_hosvd(dX, dims, ranks, core, U, precision=prec)
+        core_or, facs_or = oracle.tucker_hosvd(X, dims, ranks)
+    else:
+        cd.tucker_hooi(dX, dims, ranks, core, U, sweeps=3, precision=prec)
+        core_or, facs_or = oracle.tucker_hooi(X, dims, ranks, sweeps=3)
+    # three-term Grams are FP32-accurate; a BF16 operand (the one-term Gram,
+    # and HOOI's projections of the BF16 copy of X) perturbs X by about
+    # 2^-9 relative -- as much again as the data's own 1e-3 noise
+    gap_tol = 2e-4 if (precision == "bf16x3" and method == "hosvd") else 2e-2
+    for u, w, d, r in zip(U, facs_or, dims, ranks):
+        assert subspace_gap(host(u), w, d, r) <= gap_tol
+    rec = torch.empty(int(np.prod(dims)), device="cuda")
+    cd.gentucker(rec, core, U, dims, ranks)
+    err = float(torch.linalg.norm((dX - rec).double()) / torch.linalg.norm(dX.double()))
+    rec_or = oracle.gentucker(core_or, ranks, facs_or, dims)
+    err_or = float(np.linalg.norm(X.astype(np.float64) - rec_or) / np.linalg.norm(X.astype(np.float64)))
+    # BF16 TTM inputs: the core carries relative errors of about 2^-9
+    assert err <= err_or + 5e-3

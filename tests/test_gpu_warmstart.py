@@ -1,0 +1,137 @@
+"""Learned warm start: the generator, sketches, canonical targets, HOSVD
+initialisation and the network's gradients against the CPU oracle, and the
+end-to-end claim -- ALS from the trained network's factors reaches the same
+per-tensor fit in fewer sweeps than ALS from HOSVD factors."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ws(cd):
+    import warmstart
+    return warmstart
+
+
+def test_generator_matches_oracle(cd, ws):
+    w = ws.WarmStart(I=16, R=4, S=8, hidden=64, noise=1e-3, seed=11, max_batch=16)
+    b, clean = w.batch(3, id0=40)
+    torch.cuda.synchronize()
+    for t in range(3):
+        X, F, norm2 = oracle.ws_tensor(40 + t, 11, 16, 4, 1e-3)
+        for m in range(3):
+            got = b.u_view(t, m).cpu().numpy().reshape(4, 16).T
+            assert np.allclose(got, F[m], rtol=1e-5, atol=1e-5)
+        assert abs(clean[t].item() - norm2) <= 1e-9 * norm2
+        gx = b.x_view(t).cpu().numpy()
+        assert np.max(np.abs(gx - X)) <= 1e-5 * np.max(np.abs(X))
+        # the noise has the requested relative size
+        rec = oracle.gencp((16, 16, 16), [f.reshape(-1, order="F") for f in F], 4)
+        rel = np.linalg.norm(gx - rec) / np.sqrt(norm2)
+        assert 0.7e-3 < rel < 1.3e-3
+
+
+def test_features_match_numpy(cd, ws):
+    I, S = 16, 8
+    w = ws.WarmStart(I=I, R=4, S=S, hidden=64, seed=3, max_batch=16)
+    b, _ = w.batch(8, id0=0)
+    inp, inp_t, xn = w.features(b.X, 0, 8)
+    torch.cuda.synchronize()
+    om = w.omega.float().cpu().numpy().reshape(3, S, I * I)
+    for t in range(8):
+        X = b.x_view(t).cpu().numpy().astype(np.float64).reshape(I, I, I)  # [k][j][i]
+        assert abs(xn[t].item() - np.sum(X ** 2)) <= 1e-9 * np.sum(X ** 2)
+        unf = [X.transpose(2, 0, 1).reshape(I, I * I),   # mode 0: row i, kappa = j + I k
+               X.transpose(1, 0, 2).reshape(I, I * I),   # mode 1: row j, kappa = i + I k
+               X.reshape(I, I * I)]                      # mode 2: row k, kappa = i + I j
+        want = np.concatenate([(oracle.round_bf16_np(unf[m]) @ om[m].T).reshape(-1) for m in range(3)])
+        want /= np.sqrt(np.sum(X ** 2))
+        got = inp[t].float().cpu().numpy()
+        assert np.linalg.norm(got - want) <= 8e-3 * np.linalg.norm(want)
+        assert torch.equal(inp_t[:, t], inp[t])
+
+
+def test_canonical_form(cd, ws):
+    I, R = 16, 4
+    w = ws.WarmStart(I=I, R=R, S=8, hidden=64, seed=5, max_batch=16)
+    b, _ = w.batch(6, id0=100)
+    xn = torch.tensor([float(np.sum(b.x_view(t).cpu().numpy().astype(np.float64) ** 2)) for t in range(6)],
+                      dtype=torch.float64, device="cuda")
+    T = w.targets(b, xn, label_sweeps=1).cpu().numpy()
+    for t in range(6):
+        A = T[t, :I * R].reshape(R, I).T
+        B = T[t, I * R:2 * I * R].reshape(R, I).T
+        C = T[t, 2 * I * R:].reshape(R, I).T
+        assert np.allclose(np.linalg.norm(A, axis=0), 1.0, atol=1e-5)
+        assert np.allclose(np.linalg.norm(B, axis=0), 1.0, atol=1e-5)
+        assert (A.sum(0) >= 0).all() and (B.sum(0) >= 0).all()
+        wgt = np.linalg.norm(C, axis=0)
+        assert (np.diff(wgt) <= 1e-6).all()
+        # same CP tensor as the ALS factors it came from (C scaled back)
+        facs = [b.u_view(t, m).cpu().numpy().reshape(R, I).T for m in range(3)]
+        rec0 = np.einsum("ir,jr,kr->ijk", *facs)
+        rec1 = np.einsum("ir,jr,kr->ijk", A, B, C * np.sqrt(xn[t].item()))
+        assert np.linalg.norm(rec1 - rec0) <= 1e-4 * np.linalg.norm(rec0)
+
+
+def test_hosvd_init_matches_eigh(cd, ws):
+    I, R = 32, 4
+    w = ws.WarmStart(I=I, R=R, S=8, hidden=64, seed=9, max_batch=16)
+    b, _ = w.batch(4, id0=7)
+    w.hosvd_init(b)
+    torch.cuda.synchronize()
+    for t in range(4):
+        X = b.x_view(t).cpu().numpy().astype(np.float64)
+        for m in range(3):
+            G = oracle.unfold_gram(X.astype(np.float32), (I, I, I), m)
+            evals, evecs = np.linalg.eigh(G)
+            want = evecs[:, ::-1][:, :R]
+            got = b.u_view(t, m).cpu().numpy().reshape(R, I).T.astype(np.float64)
+            # same leading subspace (singular values of want^T got all ~1)
+            sv = np.linalg.svd(want.T @ got, compute_uv=False)
+            assert sv.min() > 1 - 1e-4
+
+
+def _small_params(rng, D, H, O):
+    return [rng.standard_normal((H, D)) * np.sqrt(2.0 / D), 0.1 * rng.standard_normal(H),
+            rng.standard_normal((H, H)) * np.sqrt(2.0 / H), 0.1 * rng.standard_normal(H),
+            rng.standard_normal((O, H)) * np.sqrt(2.0 / H), 0.1 * rng.standard_normal(O)]
+
+
+def test_mlp_gradients_match_oracle(cd, ws):
+    D, H, O, B = 48, 32, 24, 16
+    rng = np.random.default_rng(0)
+    m = ws.WarmStartMLP(D, H, O, B, seed=1)
+    params = _small_params(rng, D, H, O)
+    m.set_params(params)
+    got_p = m.get_params()
+    for a, b in zip(got_p, params):
+        assert np.allclose(a, b.astype(np.float32))
+    X = rng.standard_normal((B, D))
+    T = rng.standard_normal((B, O))
+    inp = torch.from_numpy(oracle.round_bf16_np(X).astype(np.float32)).to(torch.bfloat16).cuda()
+    inp_t = inp.t().contiguous()
+    tgt = torch.from_numpy(T.astype(np.float32)).cuda()
+    loss = m.backward(inp, inp_t, tgt)
+    want_loss, want = oracle.ws_mlp_grads([p.astype(np.float32) for p in params], X, T)
+    assert abs(loss - want_loss) <= 1e-4 * want_loss
+    got = m.grads()
+    for g, wv in zip(got, want):
+        # BF16 rounding of activations and of dY can land one ulp apart
+        # where the FP32 and FP64 sums straddle a rounding boundary
+        assert np.linalg.norm(g - wv) <= 2e-2 * np.linalg.norm(wv), (np.linalg.norm(g - wv), np.linalg.norm(wv))
+    m.close()
+
+
+def test_training_reduces_loss(cd, ws):
+    w = ws.WarmStart(I=16, R=4, S=8, hidden=128, seed=21, max_batch=64)
+    losses = w.train(4096, batch=64, lr=1e-3, chunk=1024, label_sweeps=2, log_every=8)
+    first = np.mean([l for _, l in losses[:4]])
+    last = np.mean([l for _, l in losses[-4:]])
+    assert np.isfinite(last) and last < 0.8 * first
