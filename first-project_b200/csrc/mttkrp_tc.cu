@@ -55,8 +55,9 @@ constexpr int NBMAX = 4;         // U / B / A stages (shallow: feeds the MMA)
 #define CUD_TC_SEG 16
 #endif
 constexpr int SEG = CUD_TC_SEG;  // stages per TMEM accumulation segment
-constexpr int NTHREADS = 256;    // w0 TMA, w1 MMA, w2-5 A converters, w6-7 KR producers
-constexpr int NCONV = 128;       // A converter threads
+constexpr int NTHREADS = 384;    // w0 TMA, w1 MMA, w2-9 A converters, w10-11 KR producers
+constexpr int NCONV = 256;       // A converter threads: two warps per TMEM lane quarter
+constexpr int KHALF = BKS / 2;   // contraction values per converter thread and stage
 constexpr int NKR = 64;          // KR producer threads
 constexpr int X_STAGE_BYTES = BQ * BKS * 4;  // 16 KB
 constexpr int RPAD_MAX = 128;
@@ -130,29 +131,33 @@ __device__ __forceinline__ void split_pair(float a, float b, uint32_t &hi, uint3
 
 // Per-stage Khatri-Rao values of one producer item (row r, 8-kappa chunk kc)
 // on the general path (any factor shapes): computed from global memory.
+// Indices fit 32 bits (tc_plan checks every extent), so the digit
+// arithmetic uses 32-bit unsigned division.
 __device__ __forceinline__ void kr_general(const TcArgs &a, const TcCtrl &sm, long g, int r, int kc, float (&v)[8]) {
-    long k0, kmax;
-    if (a.kind == 0) { k0 = g * BKS; kmax = a.S; }
-    else { k0 = (g % a.psteps) * BKS; kmax = a.P; }
-    const long s = (a.kind == 0) ? 0 : g / a.psteps;
+    const uint32_t gs = (uint32_t)g, ps = (uint32_t)a.psteps;
+    uint32_t k0, kmax, s;
+    if (a.kind == 0) { k0 = gs * BKS; kmax = (uint32_t)a.S; s = 0; }
+    else { s = gs / ps; k0 = (gs - s * ps) * BKS; kmax = (uint32_t)a.P; }
     float c = 1.f;
-    long lin = s;
+    uint32_t lin = s;
     for (int f = 0; f < a.outer.n; f++) {
-        const long d = sm.orows[f];
-        c *= __ldg(sm.oU[f] + (lin % d) + r * d);
-        lin /= d;
+        const uint32_t d = (uint32_t)sm.orows[f];
+        const uint32_t qd = lin / d;
+        c *= __ldg(sm.oU[f] + (lin - qd * d) + (long)r * d);
+        lin = qd;
     }
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-        const long k = k0 + kc * 8 + j;
+        const uint32_t k = k0 + kc * 8 + j;
         float x = 0.f;
         if (k < kmax) {
             x = c;
-            long l2 = k;
+            uint32_t l2 = k;
             for (int f = 0; f < a.gen.n; f++) {
-                const long d = sm.grows[f];
-                x *= __ldg(sm.gU[f] + (l2 % d) + r * d);
-                l2 /= d;
+                const uint32_t d = (uint32_t)sm.grows[f];
+                const uint32_t qd = l2 / d;
+                x *= __ldg(sm.gU[f] + (l2 - qd * d) + (long)r * d);
+                l2 = qd;
             }
         }
         v[j] = x;
@@ -206,23 +211,27 @@ __device__ __forceinline__ void make_b_item(const TcArgs &a, const TcCtrl &sm, l
 
 // The constant row of the fast path for the block of stages starting at g:
 // the product over the slower generating factors (digits of kappa / rows0)
-// and the outer factors (digits of s) of their row for column r.
+// and the outer factors (digits of s) of their row for column r (32-bit
+// digit arithmetic, as above).
 __device__ __forceinline__ float kr_const_row(const TcArgs &a, const TcCtrl &sm, long g, int r) {
-    long k0, s;
-    if (a.kind == 0) { k0 = g * BKS; s = 0; }
-    else { k0 = (g % a.psteps) * BKS; s = g / a.psteps; }
+    const uint32_t gs = (uint32_t)g, ps = (uint32_t)a.psteps;
+    uint32_t k0, s;
+    if (a.kind == 0) { k0 = gs * BKS; s = 0; }
+    else { s = gs / ps; k0 = (gs - s * ps) * BKS; }
     float c = 1.f;
-    long lin = k0 / sm.grows[0];
+    uint32_t lin = k0 / (uint32_t)sm.grows[0];
     for (int f = 1; f < a.gen.n; f++) {
-        const long d = sm.grows[f];
-        c *= __ldg(sm.gU[f] + (lin % d) + r * d);
-        lin /= d;
+        const uint32_t d = (uint32_t)sm.grows[f];
+        const uint32_t qd = lin / d;
+        c *= __ldg(sm.gU[f] + (lin - qd * d) + (long)r * d);
+        lin = qd;
     }
     lin = s;
     for (int f = 0; f < a.outer.n; f++) {
-        const long d = sm.orows[f];
-        c *= __ldg(sm.oU[f] + (lin % d) + r * d);
-        lin /= d;
+        const uint32_t d = (uint32_t)sm.orows[f];
+        const uint32_t qd = lin / d;
+        c *= __ldg(sm.oU[f] + (lin - qd * d) + (long)r * d);
+        lin = qd;
     }
     return c;
 }
@@ -265,7 +274,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         }
         for (int b = 0; b < 2; b++) {
             ptx::mbar_init(&sm.d_full[b], 1);
-            ptx::mbar_init(&sm.d_free[b], NCONV / 32);
+            ptx::mbar_init(&sm.d_free[b], 4);  // the first converter warp of each lane quarter
         }
         ptx::mbar_init(&sm.done, 1);
         sm.abort = 0;
@@ -366,13 +375,14 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             for (long it = 0; it < 40000 && !ptx::mbar_try_wait_hint(&sm.done, 0, 100000u); it++) {
             }
         }
-    } else if (warp < 6) {
+    } else if (warp < 10) {
         // ------------------------------------------------------------ A converters
         const int sub = warp & 3;                 // TMEM sub-partition of this warp
+        const int half = (warp - 2) >> 2;         // which 16 of the stage's 32 contraction values
         const int row = sub * 32 + lane;          // row within the tile (= TMEM lane)
         const uint32_t lane_off = (uint32_t)(sub * 32) << 16;
         const long q = q0 + row;
-        const int ct = threadIdx.x - 64;  // converter thread 0..127
+        const int ct = threadIdx.x - 64;  // converter thread 0..255
         const long blk = a.fast ? (long)(sm.grows[0] / BKS) : 1;
         long pos = a.fast ? st_beg % blk : 0;
         float ccv[CIPT > 0 ? CIPT : 1];
@@ -388,18 +398,16 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             if (ok) {
                 ptx::tc_fence_after();
                 const uint32_t d = tbase + lane_off + (uint32_t)b * (uint32_t)a.Rpad;
-                for (int c0 = 0; c0 < a.Rpad; c0 += 32) {
-                    uint32_t v[2][16];
-                    const bool two = c0 + 16 < a.Rpad;  // warp-uniform
-                    ptx::tmem_ld16(d + (uint32_t)c0, v[0]);
-                    if (two) ptx::tmem_ld16(d + (uint32_t)c0 + 16u, v[1]);
+                for (int c0 = 0; c0 < a.Rpad; c0 += 16) {
+                    uint32_t v[16];
+                    ptx::tmem_ld16(d + (uint32_t)c0, v);
                     ptx::tmem_wait_ld();
                     if (q < a.Q) {
 #pragma unroll
-                        for (int j4 = 0; j4 < 8; j4++) {
+                        for (int j4 = 0; j4 < 4; j4++) {
                             const int c = c0 + 4 * j4;
                             if (c < a.R) {  // columns R..Rp-1 of D are zero (zero B rows)
-                                const uint32_t *w = &v[j4 >> 2][(j4 & 3) * 4];
+                                const uint32_t *w = &v[j4 * 4];
                                 float4 val = make_float4(__uint_as_float(w[0]), __uint_as_float(w[1]),
                                                          __uint_as_float(w[2]), __uint_as_float(w[3]));
                                 float *pp = P + c;
@@ -425,16 +433,16 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             if (!*abort) ptx::mbar_wait(&sm.full_x[xslot], (uint32_t)(xuse & 1), abort);
             if (CIPT > 0 && a.fast && !*abort) ptx::mbar_wait(&sm.full_u[slot], (uint32_t)(use & 1), abort);
             __syncwarp();
-            float x[BKS];
+            float x[KHALF];
             const float *xs = reinterpret_cast<const float *>(xring + (size_t)xslot * X_STAGE_BYTES);
             if (a.kind == 0) {
 #pragma unroll
-                for (int k = 0; k < BKS; k++) x[k] = xs[k * BQ + row];
+                for (int k = 0; k < KHALF; k++) x[k] = xs[(KHALF * half + k) * BQ + row];
             } else {
                 const float4 *r4 = reinterpret_cast<const float4 *>(xs + row * BKS);
 #pragma unroll
-                for (int c = 0; c < 8; c++) {
-                    float4 v = r4[c ^ (row & 7)];
+                for (int c = 0; c < 4; c++) {
+                    float4 v = r4[(4 * half + c) ^ (row & 7)];
                     x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
                 }
             }
@@ -455,20 +463,22 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
                 ptx::mbar_arrive(&sm.empty_x[xslot]);  // the X tile is consumed
                 if (CIPT > 0 && a.fast) ptx::mbar_arrive(&sm.empty_u[slot]);
             }
-            uint32_t hi[16], lo[16];
+            uint32_t hi[KHALF / 2], lo[KHALF / 2];
             if (f16) {
 #pragma unroll
-                for (int c = 0; c < 16; c++) hi[c] = pack_f16(x[2 * c], x[2 * c + 1]);
+                for (int c = 0; c < KHALF / 2; c++) hi[c] = pack_f16(x[2 * c], x[2 * c + 1]);
             } else if (three) {
 #pragma unroll
-                for (int c = 0; c < 16; c++) split_pair(x[2 * c], x[2 * c + 1], hi[c], lo[c]);
+                for (int c = 0; c < KHALF / 2; c++) split_pair(x[2 * c], x[2 * c + 1], hi[c], lo[c]);
             } else {
 #pragma unroll
-                for (int c = 0; c < 16; c++) hi[c] = pack_bf16(x[2 * c], x[2 * c + 1]);
+                for (int c = 0; c < KHALF / 2; c++) hi[c] = pack_bf16(x[2 * c], x[2 * c + 1]);
             }
-            const uint32_t ta = tbase + lane_off + a_col0 + (uint32_t)slot * 32u;
-            ptx::tmem_st16(ta, hi);
-            if (three) ptx::tmem_st16(ta + 16, lo);
+            // A stage: hi in columns 0-15, lo in 16-31 (2 values per column);
+            // this warp's half is 8 columns of each
+            const uint32_t ta = tbase + lane_off + a_col0 + (uint32_t)slot * 32u + 8u * (uint32_t)half;
+            ptx::tmem_st8(ta, hi);
+            if (three) ptx::tmem_st8(ta + 16, lo);
             // this thread's share of the B tile
             if (CIPT > 0) {
                 const long g = st_beg + i;
@@ -498,13 +508,15 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             ptx::tc_fence_before();
             __syncwarp();
             if (lane == 0) ptx::mbar_arrive(&sm.full_a[slot]);
-            // a segment just ended: drain the one before it (long finished)
-            if ((i % SEG) == SEG - 1 && i / SEG >= 1) flush(flushed++);
+            // a segment just ended: drain the one before it (long finished);
+            // the first converter warp of each lane quarter does the flushes
+            if (half == 0 && (i % SEG) == SEG - 1 && i / SEG >= 1) flush(flushed++);
         }
-        while (flushed < nseg) flush(flushed++);
+        if (half == 0)
+            while (flushed < nseg) flush(flushed++);
     } else {
         // ------------------------------------------------------------ KR producers
-        const int kt = threadIdx.x - 192;  // 0..63
+        const int kt = threadIdx.x - (64 + NCONV);  // 0..63
         // fast path: the stage's 32 rows of the fastest generating factor
         // arrive by TMA with X; the constant row changes every `blk` stages
         const long blk = a.fast ? (long)(sm.grows[0] / BKS) : 1;
@@ -640,7 +652,10 @@ void tc_shape(TcPlan &p) {
             break;
         }
     }
-    long want = std::max(1L, (p.ctas_per_sm * (long)kNumSMs) / p.qtiles);
+    // one wave of CTAs, minus two slots: a sweep runs the R x R solve on a
+    // second stream beside the MTTKRP, and a grid that needs every slot
+    // would push one CTA into a second wave behind it
+    long want = std::max(1L, (p.ctas_per_sm * (long)kNumSMs - 2) / p.qtiles);
     p.splits = std::min(want, p.stages);
     p.chunk = (p.stages + p.splits - 1) / p.splits;
     p.splits = (p.stages + p.chunk - 1) / p.chunk;
@@ -663,6 +678,7 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     p.psteps = (p.kind == 0) ? 1 : (v.P + BKS - 1) / BKS;
     p.stages = (p.kind == 0) ? (v.S + BKS - 1) / BKS : v.S * p.psteps;
     if (p.kind == 0 && p.stages * BKS > 0x7fffffffL) return false;
+    if (p.stages > 0x7fffffffL) return false;  // 32-bit stage / digit arithmetic in the kernel
     p.qtiles = (v.Q + BQ - 1) / BQ;
     // fast KR path: the fastest generating factor's row count is a multiple
     // of 32, so each stage covers 32 of its rows (one TMA box)
@@ -758,10 +774,10 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     a.nx = p.nx;
     a.nb = p.nb;
     a.Rp = (R + 3) / 4 * 4;
-    // B items: 4 per padded row; the KR warps take about half (whole warps of
-    // work, at least 64), the converters the rest
+    // B items: 4 per padded row; the KR warps take about a quarter (whole
+    // warps of work, at least 64), the eight converter warps the rest
     const int ni = 4 * (int)p.Rpad;
-    a.nkri = std::max(64, (ni / 2) / 64 * 64);
+    a.nkri = std::max(64, (ni / 4) / 64 * 64);
     const int kipt_need = a.nkri / NKR;
     const int cipt_need = (ni - a.nkri + NCONV - 1) / NCONV;
     a.gen.n = 0;
@@ -786,8 +802,7 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     if (p.ctas_per_sm == 2) {
         if (kipt_need <= 1 && cipt_need <= 0) st = launch_tc<1, 0, 2>(tmap, umap, a, smem, grid, s);
         else if (kipt_need <= 1 && cipt_need <= 1) st = launch_tc<1, 1, 2>(tmap, umap, a, smem, grid, s);
-        else if (kipt_need <= 2 && cipt_need <= 1) st = launch_tc<2, 1, 2>(tmap, umap, a, smem, grid, s);
-        else st = launch_tc<4, 2, 2>(tmap, umap, a, smem, grid, s);
+        else st = launch_tc<2, 2, 2>(tmap, umap, a, smem, grid, s);
     } else {
         if (kipt_need <= 2 && cipt_need <= 2) st = launch_tc<2, 2, 1>(tmap, umap, a, smem, grid, s);
         else st = launch_tc<4, 2, 1>(tmap, umap, a, smem, grid, s);

@@ -39,15 +39,16 @@ __global__ void __launch_bounds__(256) k_factor_gram(const float *__restrict__ U
 // eigenvectors accumulated in Q (global).  One CTA; rotations of disjoint
 // (p, q) pairs run in parallel in round-robin order.  Returns sweeps used.
 __device__ int block_jacobi_smem(double *A, double *Q, int n, int max_sweeps, double tol) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nthr = blockDim.x * blockDim.y;
     __shared__ double s_cos[128], s_sin[128];
     __shared__ int s_p[128], s_q[128];
     __shared__ double s_off;
     int m = (n + 1) & ~1;  // even number of players (a dummy when n is odd)
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) Q[e] = (e % n == e / n) ? 1.0 : 0.0;
+    for (int e = tid; e < n * n; e += nthr) Q[e] = (e % n == e / n) ? 1.0 : 0.0;
     __syncthreads();
     int sweep;
     for (sweep = 0; sweep < max_sweeps; sweep++) {
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             double off = 0.0, dia = 0.0;
             for (int j = 0; j < n; j++)
                 for (int i = 0; i < n; i++) {
@@ -60,7 +61,7 @@ __device__ int block_jacobi_smem(double *A, double *Q, int n, int max_sweeps, do
         if (s_off < 0) break;
         for (int round = 0; round < m - 1; round++) {
             // round-robin pairing: player 0 fixed, others rotate
-            for (int k = threadIdx.x; k < m / 2; k += blockDim.x) {
+            for (int k = tid; k < m / 2; k += nthr) {
                 int a = (k == 0) ? 0 : 1 + (k - 1 + round) % (m - 1);
                 int b = 1 + (m - 2 - k + round) % (m - 1);
                 int p = min(a, b), q = max(a, b);
@@ -80,7 +81,7 @@ __device__ int block_jacobi_smem(double *A, double *Q, int n, int max_sweeps, do
             }
             __syncthreads();
             // rows: A <- J^T A
-            for (int e = threadIdx.x; e < (m / 2) * n; e += blockDim.x) {
+            for (int e = tid; e < (m / 2) * n; e += nthr) {
                 int k = e / n, col = e % n;
                 int p = s_p[k], q = s_q[k];
                 if (q >= n) continue;
@@ -91,7 +92,7 @@ __device__ int block_jacobi_smem(double *A, double *Q, int n, int max_sweeps, do
             }
             __syncthreads();
             // columns: A <- A J, Q <- Q J
-            for (int e = threadIdx.x; e < (m / 2) * n; e += blockDim.x) {
+            for (int e = tid; e < (m / 2) * n; e += nthr) {
                 int k = e / n, row = e % n;
                 int p = s_p[k], q = s_q[k];
                 if (q >= n) continue;
@@ -117,70 +118,81 @@ __device__ int block_jacobi_smem(double *A, double *Q, int n, int max_sweeps, do
 // V in dynamic shared memory, two barriers per pivot.  `work` is global
 // scratch of 2 R^2 doubles.
 __global__ void __launch_bounds__(512) k_normal_inverse(NormalArgs a) {
+    // 32 x 16 threads: element (i, j) of an R x R matrix visited as
+    // i = tx, tx + 32, ...; j = ty, ty + 16, ... (no per-element division)
     extern __shared__ double V[];  // R x R
     __shared__ int s_fail;
     __shared__ double rowk[160], colk[160];
+    __shared__ const double *sG[kMaxOrder];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
     const int R = a.R;
-    for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-        double v = 1.0;
-        for (int m = 0; m < a.nG; m++)
-            if (m != a.mode) v *= a.G[m][e];
-        V[e] = v;
+    if (tid == 0) {
+#pragma unroll
+        for (int m = 0; m < kMaxOrder; m++) sG[m] = (m < a.nG) ? a.G[m] : nullptr;
+        s_fail = 0;
     }
-    if (threadIdx.x == 0) s_fail = 0;
+    __syncthreads();
+    for (int j = ty; j < R; j += 16)
+        for (int i = tx; i < R; i += 32) {
+            double v = 1.0;
+            for (int m = 0; m < a.nG; m++)
+                if (m != a.mode) v *= sG[m][i + R * j];
+            V[i + R * j] = v;
+        }
     __syncthreads();
     double maxdiag = 0.0;
     for (int j = 0; j < R; j++) maxdiag = fmax(maxdiag, fabs(V[j + R * j]));
     for (int k = 0; k < R; k++) {
         const double piv = V[k + R * k];
         if (!(piv > 1e-13 * maxdiag) || !isfinite(piv)) {  // same decision in every thread
-            if (threadIdx.x == 0) s_fail = 1;
+            if (tid == 0) s_fail = 1;
             break;
         }
         const double inv = 1.0 / piv;
-        for (int j = threadIdx.x; j < R; j += blockDim.x) {
+        for (int j = tid; j < R; j += 512) {
             rowk[j] = (j == k ? 1.0 : V[k + R * j]) * inv;
             colk[j] = V[j + R * k];
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-            const int i = e % R, j = e / R;
-            const double old = (j == k) ? 0.0 : V[e];
-            V[e] = (i == k) ? rowk[j] : old - colk[i] * rowk[j];
+        for (int j = ty; j < R; j += 16) {
+            const double rj = rowk[j];
+            for (int i = tx; i < R; i += 32) {
+                const double old = (j == k) ? 0.0 : V[i + R * j];
+                V[i + R * j] = (i == k) ? rj : old - colk[i] * rj;
+            }
         }
         __syncthreads();
     }
     __syncthreads();
     double *Q = a.work + R * R;   // R x R (pinv path)
     if (!s_fail) {
-        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-            const int i = e % R, j = e / R;
-            a.Vinv[e] = 0.5 * (V[e] + V[j + R * i]);  // symmetrise the rounding
-        }
+        for (int j = ty; j < R; j += 16)
+            for (int i = tx; i < R; i += 32) a.Vinv[i + R * j] = 0.5 * (V[i + R * j] + V[j + R * i]);  // symmetrise
     } else {
         // pseudo-inverse: rebuild V, eigendecompose, invert eigenvalues above tol
-        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-            double v = 1.0;
-            for (int m = 0; m < a.nG; m++)
-                if (m != a.mode) v *= a.G[m][e];
-            V[e] = v;
-        }
+        for (int j = ty; j < R; j += 16)
+            for (int i = tx; i < R; i += 32) {
+                double v = 1.0;
+                for (int m = 0; m < a.nG; m++)
+                    if (m != a.mode) v *= sG[m][i + R * j];
+                V[i + R * j] = v;
+            }
         __syncthreads();
         block_jacobi_smem(V, Q, R, 60, 1e-15);
         __syncthreads();
         double lmax = 0.0;
         for (int j = 0; j < R; j++) lmax = fmax(lmax, fabs(V[j + R * j]));
         double cut = lmax * (double)R * 2.2e-16;
-        for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-            int i = e % R, j = e / R;
-            double s = 0.0;
-            for (int k = 0; k < R; k++) {
-                double l = V[k + R * k];
-                if (l > cut) s += Q[i + R * k] * Q[j + R * k] / l;
+        for (int j = ty; j < R; j += 16)
+            for (int i = tx; i < R; i += 32) {
+                double sacc = 0.0;
+                for (int k = 0; k < R; k++) {
+                    double l = V[k + R * k];
+                    if (l > cut) sacc += Q[i + R * k] * Q[j + R * k] / l;
+                }
+                a.Vinv[i + R * j] = sacc;
             }
-            a.Vinv[e] = s;
-        }
-        if (threadIdx.x == 0 && a.fallbacks) atomicAdd(a.fallbacks, 1);
+        if (tid == 0 && a.fallbacks) atomicAdd(a.fallbacks, 1);
     }
 }
 
@@ -243,22 +255,40 @@ __global__ void __launch_bounds__(256) k_fit(FitArgs a) {
 // CTA to finish (atomic ticket) sums the partials in CTA order --
 // deterministic -- writes G, resets the ticket and, if asked, the fit.
 constexpr int UPD_RB = 16;
+constexpr int UPD_STAGE_V = 64;  // V^-1 staged in shared memory up to this R
+constexpr int SU_LD = UPD_RB + 1;  // sU column stride (odd: conflict-free Gram reads)
 
 template <int NT, int NACC>
 __global__ void __launch_bounds__(NT) k_update(UpdateArgs a) {
-    extern __shared__ double sU[];  // UPD_RB x R
+    // shared: sU (UPD_RB x R FP64), sM (UPD_RB x R FP32, this chunk of M),
+    // sV (R x R FP64, V^-1 staged when R <= UPD_STAGE_V)
+    extern __shared__ double smem_d[];
     __shared__ int s_last;
     __shared__ double s_red[NT / 32];
     const int R = a.R;
     const long I = a.I;
+    double *sU = smem_d;  // SU_LD x R
+    float *sM = reinterpret_cast<float *>(sU + SU_LD * R);
+    double *sV = sU + SU_LD * R + (UPD_RB * R + 1) / 2;
+    const bool stage_v = a.Vinv && R <= UPD_STAGE_V;
+    if (stage_v)
+        for (int e = threadIdx.x; e < R * R; e += NT) sV[e] = a.Vinv[e];
+    const double *V = stage_v ? sV : a.Vinv;
     const long rpb = (I + gridDim.x - 1) / gridDim.x;
     const long r0 = blockIdx.x * rpb, r1 = min(I, r0 + rpb);
     double acc[NACC];
 #pragma unroll
     for (int k = 0; k < NACC; k++) acc[k] = 0.0;
+    const int p0 = threadIdx.x % R, q0 = threadIdx.x / R, dp = NT % R, dq = NT / R;
     double inner = 0.0;
     for (long c0 = r0; c0 < r1; c0 += UPD_RB) {
         const int nr = (int)min((long)UPD_RB, r1 - c0);
+        // this chunk's rows of M, coalesced, then everything from shared memory
+        for (int e = threadIdx.x; e < UPD_RB * R; e += NT) {
+            const int i = e % UPD_RB, c = e / UPD_RB;
+            sM[e] = (i < nr) ? a.M[c0 + i + I * c] : 0.f;
+        }
+        __syncthreads();
         for (int e = threadIdx.x; e < UPD_RB * R; e += NT) {
             const int i = e % UPD_RB, c = e / UPD_RB;
             double u = 0.0;
@@ -266,27 +296,33 @@ __global__ void __launch_bounds__(NT) k_update(UpdateArgs a) {
                 const long gi = c0 + i;
                 if (a.Vinv) {
                     double s = 0.0;
-                    for (int r = 0; r < R; r++) s = fma((double)a.M[gi + I * r], a.Vinv[r + R * c], s);
+                    for (int r = 0; r < R; r++) s = fma((double)sM[i + UPD_RB * r], V[r + R * c], s);
                     float uf = (float)s;
                     a.U[gi + I * c] = uf;
                     u = (double)uf;
                 } else {
-                    u = (double)a.M[gi + I * c];
+                    u = (double)sM[e];
                 }
-                if (a.fit_out) inner += (double)a.M[gi + I * c] * u;
+                if (a.fit_out) inner += (double)sM[e] * u;
             }
-            sU[i + UPD_RB * c] = u;
+            sU[i + SU_LD * c] = u;
         }
         __syncthreads();
+        // Gram entries e = tid + NT k, (p, q) = (e mod R, e / R) stepped
+        // incrementally (no division per entry)
+        {
+            int p = p0, q = q0;
 #pragma unroll
-        for (int k = 0; k < NACC; k++) {
-            const int e = threadIdx.x + NT * k;
-            if (e < R * R) {
-                const int p = e % R, q = e / R;
-                double s = acc[k];
+            for (int k = 0; k < NACC; k++) {
+                if (q < R) {
+                    double s = acc[k];
 #pragma unroll
-                for (int i = 0; i < UPD_RB; i++) s = fma(sU[i + UPD_RB * p], sU[i + UPD_RB * q], s);
-                acc[k] = s;
+                    for (int i = 0; i < UPD_RB; i++) s = fma(sU[i + SU_LD * p], sU[i + SU_LD * q], s);
+                    acc[k] = s;
+                }
+                p += dp;
+                q += dq;
+                if (p >= R) { p -= R; q++; }
             }
         }
         __syncthreads();
@@ -313,10 +349,19 @@ __global__ void __launch_bounds__(NT) k_update(UpdateArgs a) {
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    // last CTA: fixed-order sum of the partials
+    // last CTA: fixed-order sum of the partials, 8 independent loads in
+    // flight per element (lanes b = j mod 8, combined in a fixed tree)
     for (long e = threadIdx.x; e < stride; e += NT) {
-        double s = 0.0;
-        for (unsigned b = 0; b < gridDim.x; b++) s += __ldcg(a.gpart + b * stride + e);
+        double p8[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        unsigned b = 0;
+        for (; b + 8 <= gridDim.x; b += 8) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) p8[j] += __ldcg(a.gpart + (b + j) * stride + e);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; j++)  // tail: constant indices keep p8 in registers
+            if (b + j < gridDim.x) p8[j] += __ldcg(a.gpart + (b + j) * stride + e);
+        const double s = ((p8[0] + p8[1]) + (p8[2] + p8[3])) + ((p8[4] + p8[5]) + (p8[6] + p8[7]));
         if (e < (long)R * R) a.G_out[e] = s;
         else s_red[0] = s;  // inner product (written by exactly one thread)
     }
@@ -348,13 +393,16 @@ __global__ void __launch_bounds__(NT) k_update(UpdateArgs a) {
 
 }  // namespace
 
-int update_blocks(long I) { return (int)std::max(1L, std::min((long)kNumSMs, (I + UPD_RB - 1) / UPD_RB)); }
+// At least 64 rows per CTA: the last CTA sums one partial Gram per CTA
+// serially, so fewer, fuller CTAs finish sooner for the I_n of CP factors.
+int update_blocks(long I) { return (int)std::max(1L, std::min((long)kNumSMs, (I + 63) / 64)); }
 
 size_t update_ws_doubles(long I, long R) { return (size_t)update_blocks(I) * (size_t)(R * R + 1); }
 
 int factor_update(const UpdateArgs &a, cudaStream_t s) {
     const int nb = update_blocks(a.I);
-    const size_t smem = sizeof(double) * UPD_RB * a.R;
+    const size_t smem = sizeof(double) * SU_LD * a.R + sizeof(float) * (UPD_RB * a.R + 2) +
+                        (a.R <= UPD_STAGE_V ? sizeof(double) * a.R * a.R : 0);
     if (a.R <= 32) k_update<256, 4><<<nb, 256, smem, s>>>(a);
     else if (a.R <= 64) k_update<256, 16><<<nb, 256, smem, s>>>(a);
     else if (a.R <= 160) k_update<512, 50><<<nb, 512, smem, s>>>(a);
@@ -402,7 +450,7 @@ int normal_inverse(const NormalArgs &a, cudaStream_t s) {
     if (a.R > 160) return CUD_ERR_UNSUPPORTED;
     int st = normal_inverse_prepare();
     if (st) return st;
-    k_normal_inverse<<<1, 512, smem, s>>>(a);
+    k_normal_inverse<<<1, dim3(32, 16), smem, s>>>(a);
     CUD_CHECK_LAUNCH("normal_inverse");
     return CUD_OK;
 }

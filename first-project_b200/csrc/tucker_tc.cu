@@ -206,8 +206,15 @@ int gram_tc(const TcWork &w, long I, long K, bool use_lo, cudaStream_t s) {
     return CUD_OK;
 }
 
-// U (I x r, FP32) = eigenvectors of the r largest eigenvalues of w.g64.
+// U (I x r, FP32) = eigenvectors of the r largest eigenvalues of w.g64:
+// subspace iteration (fast when the Gram has a gap after its r-th
+// eigenvalue), else the full FP64 Jacobi eigensolver.
 int top_vectors(const TcWork &w, long I, long r, float *U, cudaStream_t s) {
+    if (subspace_ws_doubles(I, r) <= (size_t)I * I) {
+        const int sst = top_eigvecs_subspace(w.g64, I, r, U, w.V, 300, s);
+        if (sst == CUD_OK) return CUD_OK;
+        if (sst != CUD_ERR_NOT_CONVERGED && sst != CUD_ERR_UNSUPPORTED) return sst;
+    }
     int st = syev_jacobi(w.g64, I, w.W, w.V, 60, s);
     if (st != CUD_OK && st != CUD_ERR_NOT_CONVERGED) return st;
     k_take_top_f32<<<gfor(I * r), 256, 0, s>>>(w.V, I, r, U);

@@ -243,6 +243,61 @@ __global__ void __launch_bounds__(256) k_ws_uncanon(const float *Y, const double
     }
 }
 
+// Aligns each sample's target factors to the prediction (in place): the
+// target's rank-1 terms are matched to the predicted ones greedily by
+// |<a, a'> <b, b'> <c, c'>| (columns normalised), reordered into the
+// prediction's order, and sign-aligned -- the target's U_0 and U_1 columns
+// flipped to agree with the prediction, U_2 compensating so each rank-1
+// term is unchanged.  Removes the loss's dependence on the arbitrary order
+// and signs of CP components.  One CTA (R*R <= 256 threads) per sample.
+__global__ void __launch_bounds__(256) k_ws_align(const float *Y, float *T, int I, int R) {
+    __shared__ float sim[16][16], sga[16][16], sgb[16][16];
+    __shared__ int match[16];
+    __shared__ float tmp[3 * 128 * 16];
+    const long t = blockIdx.x;
+    const int per = I * R;
+    const float *y = Y + t * 3 * per;
+    float *tt = T + t * 3 * per;
+    const int p = threadIdx.x / R, q = threadIdx.x % R;  // predicted p, target q
+    if (threadIdx.x < R * R) {
+        float prod = 1.f, sa = 1.f, sb = 1.f;
+        for (int m = 0; m < 3; m++) {
+            const float *yp = y + m * per + p * I, *tq = tt + m * per + q * I;
+            float d = 0.f, ny = 0.f, nt = 0.f;
+            for (int i = 0; i < I; i++) { d += yp[i] * tq[i]; ny += yp[i] * yp[i]; nt += tq[i] * tq[i]; }
+            const float c = d / sqrtf(fmaxf(ny * nt, 1e-30f));
+            prod *= c;
+            if (m == 0) sa = (d < 0.f) ? -1.f : 1.f;
+            if (m == 1) sb = (d < 0.f) ? -1.f : 1.f;
+        }
+        sim[p][q] = fabsf(prod);
+        sga[p][q] = sa;
+        sgb[p][q] = sb;
+    }
+    for (int e = threadIdx.x; e < 3 * per; e += blockDim.x) tmp[e] = tt[e];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bool used_p[16] = {}, used_q[16] = {};
+        for (int k = 0; k < R; k++) {  // greedy: the best remaining pair, fixed tie order
+            float best = -1.f;
+            int bp = 0, bq = 0;
+            for (int a = 0; a < R; a++)
+                for (int b = 0; b < R; b++)
+                    if (!used_p[a] && !used_q[b] && sim[a][b] > best) { best = sim[a][b]; bp = a; bq = b; }
+            used_p[bp] = used_q[bq] = true;
+            match[bp] = bq;
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 3 * per; e += blockDim.x) {
+        const int m = e / per, rem = e % per, r = rem / I, i = rem % I;
+        const int qq = match[r];
+        const float sa = sga[r][qq], sb = sgb[r][qq];
+        const float sg = (m == 0) ? sa : (m == 1 ? sb : sa * sb);
+        tt[e] = sg * tmp[m * per + qq * I + i];
+    }
+}
+
 // MSE loss 1/(B*D) sum (Y - T)^2 and its gradient dY = 2 (Y - T) / (B*D) as
 // BF16 (B x D) and its transpose (D x B).  loss2[0] += partial sums.
 __global__ void __launch_bounds__(256) k_ws_mse(const float *Y, const float *T, long B, long D,
@@ -495,6 +550,8 @@ struct cud_ws_model_s {
     void *ws = nullptr;
     size_t ws_bytes = 0;
     long step = 0;
+    int align_I = 0, align_R = 0;  // when set, targets are aligned to the prediction (k_ws_align)
+    float *Ta = nullptr;           // the aligned copy of the targets
 };
 
 using namespace cud;
@@ -549,6 +606,12 @@ int ws_backward(cud_ws_model m, const __nv_bfloat16 *in, const __nv_bfloat16 *in
     int st = ws_forward(m, in, B, m->Y, s);
     if (st) return st;
     CUD_CHECK(cudaMemsetAsync(m->loss, 0, sizeof(double), s));
+    if (m->align_I > 0) {
+        CUD_CHECK(cudaMemcpyAsync(m->Ta, target, sizeof(float) * B * O, cudaMemcpyDeviceToDevice, s));
+        k_ws_align<<<(unsigned)B, 256, 0, s>>>(m->Y, m->Ta, m->align_I, m->align_R);
+        CUD_CHECK_LAUNCH("ws align");
+        target = m->Ta;
+    }
     k_ws_mse<<<grid_for(B * O), 256, 0, s>>>(m->Y, target, B, O, m->dY, m->dYt, m->loss);
     CUD_CHECK_LAUNCH("ws mse");
     // layer 3
@@ -599,7 +662,7 @@ extern "C" int cud_ws_model_create(int in_dim, int hidden, int out_dim, int max_
                                  gemm_tc_ws_bytes(O, H, B), gemm_tc_ws_bytes(B, H, O), gemm_tc_ws_bytes(H, H, B),
                                  gemm_tc_ws_bytes(H, D, B)});
     // + 256-byte rounding of each of the 41 buffers carved below
-    m->bytes = 4 * f32 + bf + 4 * (size_t)B * O + 256 + wsb + 48 * 256;
+    m->bytes = 4 * f32 + bf + 8 * (size_t)B * O + 256 + wsb + 48 * 256;
     if (cudaMalloc(&m->mem, m->bytes) != cudaSuccess) {
         cudaGetLastError();
         delete m;
@@ -621,6 +684,7 @@ extern "C" int cud_ws_model_create(int in_dim, int hidden, int out_dim, int max_
     m->dH2 = (__nv_bfloat16 *)take(2 * B * H); m->dH2t = (__nv_bfloat16 *)take(2 * B * H);
     m->dH1 = (__nv_bfloat16 *)take(2 * B * H); m->dH1t = (__nv_bfloat16 *)take(2 * B * H);
     m->Y = (float *)take(4 * (size_t)B * O);
+    m->Ta = (float *)take(4 * (size_t)B * O);
     m->loss = (double *)take(64);
     m->ws_bytes = wsb;
     m->ws = take(wsb);
@@ -642,6 +706,14 @@ extern "C" int cud_ws_model_create(int in_dim, int hidden, int out_dim, int max_
         return set_status(st);
     }
     *out = m;
+    return set_status(CUD_OK);
+}
+
+extern "C" int cud_ws_model_align(cud_ws_model m, int I, int R) {
+    if (!m || I < 0 || R < 0 || R > 16 || I > 128 || (I > 0 && 3 * I * R != m->out))
+        return set_status(CUD_ERR_INVALID_ARGUMENT);
+    m->align_I = I;
+    m->align_R = R;
     return set_status(CUD_OK);
 }
 

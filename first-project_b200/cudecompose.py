@@ -129,6 +129,7 @@ _sig("cud_cp_als_batched_target", [_i, ctypes.POINTER(_l), ctypes.POINTER(_l), _
                                    ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_i), _vp])
 _sig("cud_ws_model_create", [_i, _i, _i, _i, ctypes.c_ulonglong, ctypes.POINTER(_vp)])
 _sig("cud_ws_model_destroy", [_vp])
+_sig("cud_ws_model_align", [_vp, _i, _i])
 _sig("cud_ws_model_params", [_vp, ctypes.POINTER(_vp), _i])
 _sig("cud_ws_model_grads", [_vp, ctypes.POINTER(_vp)])
 _sig("cud_ws_backward", [_vp, _vp, _vp, _vp, _i, ctypes.POINTER(_d), _vp])

@@ -107,13 +107,16 @@ class WarmStart:
     ||X_clean||), its sketches (width S) and the network that maps them to
     initial factors."""
 
-    def __init__(self, I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256):
+    def __init__(self, I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256, align=True):
         self.I, self.R, self.S, self.noise, self.seed = I, R, S, noise, seed
         self.in_dim, self.out_dim = 3 * I * S, 3 * I * R
         self.max_batch = max_batch
         self.omega = torch.empty(3 * S * I * I, dtype=torch.bfloat16, device="cuda")
         cd._check(_lib.cud_ws_omega(I, S, seed + 7919, _p(self.omega), None), "ws_omega")
         self.model = WarmStartMLP(self.in_dim, hidden, self.out_dim, max_batch, seed)
+        if align:
+            # the loss matches components and signs to the prediction
+            cd._check(_lib.cud_ws_model_align(self.model._h, I, R), "ws_model_align")
 
     # ---------------------------------------------------------------- data
     def batch(self, n, id0):

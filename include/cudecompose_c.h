@@ -311,6 +311,11 @@ typedef struct cud_ws_model_s *cud_ws_model;
 int cud_ws_model_create(int in_dim, int hidden, int out_dim, int max_batch, unsigned long long seed,
                         cud_ws_model *model);
 int cud_ws_model_destroy(cud_ws_model model);
+/* When I, R > 0 (out_dim = 3 I R): the loss compares the prediction with
+ * the targets' CP factors matched to it -- components reordered and signs
+ * aligned (U_0, U_1 flipped, U_2 compensating) -- instead of their given
+ * order.  I = R = 0 restores the plain loss. */
+int cud_ws_model_align(cud_ws_model model, int I, int R);
 /* host[k] (k = W1, b1, W2, b2, W3, b3; W row-major out x in; NULL skips):
  * set = 1 copies host -> model (and refreshes the BF16 copies), 0 the reverse */
 int cud_ws_model_params(cud_ws_model model, float *const *host, int set);
