@@ -55,10 +55,17 @@ constexpr int NBMAX = 4;         // U / B / A stages (shallow: feeds the MMA)
 #define CUD_TC_SEG 16
 #endif
 constexpr int SEG = CUD_TC_SEG;  // stages per TMEM accumulation segment
+#ifndef CUD_TC_KR_ITEMS
+#define CUD_TC_KR_ITEMS 64  // B items per stage made by the KR warp (two CTAs per SM; twice that with one)
+#endif
 constexpr int NTHREADS = 384;    // w0 TMA, w1 MMA, w2-9 A converters, w10-11 KR producers
-constexpr int NCONV = 256;       // A converter threads: two warps per TMEM lane quarter
-constexpr int KHALF = BKS / 2;   // contraction values per converter thread and stage
-constexpr int NKR = 64;          // KR producer threads
+constexpr int NCONV = 256;       // A converter threads: two groups of one warp per TMEM lane quarter
+constexpr int GROUPS = 2;        // converter groups (stages i with i % GROUPS == group)
+constexpr int GCONV = NCONV / GROUPS;  // converter threads per stage
+constexpr int FLUSH_GRP = (CUD_TC_SEG - 1) % GROUPS;  // converts each segment's last stage
+static_assert(CUD_TC_SEG % GROUPS == 0, "segments hold whole converter rounds");
+constexpr int NKR = 64;          // KR producer threads: one warp per stage parity
+constexpr int KRW = NKR / GROUPS;  // KR producer threads per stage
 constexpr int X_STAGE_BYTES = BQ * BKS * 4;  // 16 KB
 constexpr int RPAD_MAX = 128;
 
@@ -166,6 +173,39 @@ __device__ __forceinline__ void kr_general(const TcArgs &a, const TcCtrl &sm, lo
 
 // B item `id` -> (row r, 8-kappa chunk kc): 32 consecutive ids cover 8 rows x
 // 4 chunks, so a quarter-warp stores 128 contiguous bytes of the B tile.
+// Position in a ring of n slots: stage i sits in slot i % n for the
+// (i / n)-th time, advanced by one per stage without dividing.
+struct Ring {
+    int slot, n;
+    long use;
+    __device__ explicit Ring(int n_) : slot(0), n(n_), use(0) {}
+    __device__ __forceinline__ void next() {
+        if (++slot == n) {
+            slot = 0;
+            ++use;
+        }
+    }
+    // advance by `step` stages (step <= n)
+    __device__ __forceinline__ void next(int step) {
+        slot += step;
+        if (slot >= n) {
+            slot -= n;
+            ++use;
+        }
+    }
+    // parity of the slot's previous phase (the one a producer waits out)
+    __device__ __forceinline__ uint32_t prev_parity() const { return (uint32_t)((use - 1) & 1); }
+};
+
+// Parity waits and ring depths.  A consumer that visits every GROUPS-th
+// stage waits on a slot whose phases, with an odd ring depth, alternate
+// between it and the other group; a parity wait is only exact when the
+// barrier has already completed the phase before the awaited one.  Every
+// consumer therefore first waits for the MMA of stage i - nb (empty_a): that
+// MMA ran after the other group's full_a arrival for stage i - nb, which came
+// after its own full_x / full_u waits for that stage, so the X and U slots'
+// previous phases are complete (the X ring is as deep as the A/B ring).
+
 __device__ __forceinline__ void b_item(int id, int &r, int &kc) {
     r = ((id >> 5) << 3) | (id & 7);
     kc = (id >> 3) & 3;
@@ -178,35 +218,65 @@ __device__ __forceinline__ void load_u_item(const float *us, int r, int kc, floa
     u1 = *reinterpret_cast<const float4 *>(us + r * BKS + (((2 * kc + 1) ^ (r & 7)) << 2));
 }
 
-// Makes B item (r, kc) of stage g: 8 Khatri-Rao values (fast path: the U
-// values u0, u1 times the constant row c; general path: from global
-// memory), rounded / split and stored into the canonical B layout.
-__device__ __forceinline__ void make_b_item(const TcArgs &a, const TcCtrl &sm, long g, int r, int kc, float c,
-                                            float4 u0, float4 u1, uint8_t *bh, uint8_t *bl, bool three, bool f16) {
-    float v[8];
-    if (a.fast) {
-        v[0] = u0.x * c; v[1] = u0.y * c; v[2] = u0.z * c; v[3] = u0.w * c;
-        v[4] = u1.x * c; v[5] = u1.y * c; v[6] = u1.z * c; v[7] = u1.w * c;
-    } else if (r < a.R) {
-        kr_general(a, sm, g, r, kc, v);
-    } else {
+// Packs 16 consecutive contraction values x[k0..k0+15] of an A row into 8
+// hi words (and, for BF16x3, 8 lo words), two values per word.
+__device__ __forceinline__ void split_half(const float (&x)[BKS], int k0, uint32_t (&hi)[8], uint32_t (&lo)[8],
+                                           bool three, bool f16) {
 #pragma unroll
-        for (int j = 0; j < 8; j++) v[j] = 0.f;
+    for (int c = 0; c < 8; c++) {
+        const float a0 = x[k0 + 2 * c], a1 = x[k0 + 2 * c + 1];
+        lo[c] = 0u;
+        if (f16) hi[c] = pack_f16(a0, a1);
+        else if (three) split_pair(a0, a1, hi[c], lo[c]);
+        else hi[c] = pack_bf16(a0, a1);
     }
-    const uint32_t off = (uint32_t)r * 16u + (uint32_t)kc * (uint32_t)a.Rpad * 16u;
-    uint4 h, l;
+}
+
+// Rounds / splits the 8 Khatri-Rao values of a B item into its hi (and, for
+// BF16x3, lo) words.
+__device__ __forceinline__ void pack_b_item(const float (&v)[8], uint4 &h, uint4 &l, bool three, bool f16) {
+    l = make_uint4(0u, 0u, 0u, 0u);
     if (f16) {
         h.x = pack_f16(v[0], v[1]); h.y = pack_f16(v[2], v[3]);
         h.z = pack_f16(v[4], v[5]); h.w = pack_f16(v[6], v[7]);
     } else if (three) {
         split_pair(v[0], v[1], h.x, l.x); split_pair(v[2], v[3], h.y, l.y);
         split_pair(v[4], v[5], h.z, l.z); split_pair(v[6], v[7], h.w, l.w);
-        *reinterpret_cast<uint4 *>(bl + off) = l;
     } else {
         h.x = pack_bf16(v[0], v[1]); h.y = pack_bf16(v[2], v[3]);
         h.z = pack_bf16(v[4], v[5]); h.w = pack_bf16(v[6], v[7]);
     }
+}
+
+// Fast path: the words of B item (r, kc) from the U values u0, u1 times the
+// constant row c.
+__device__ __forceinline__ void fast_b_item(float c, float4 u0, float4 u1, uint4 &h, uint4 &l, bool three,
+                                            bool f16) {
+    const float v[8] = {u0.x * c, u0.y * c, u0.z * c, u0.w * c, u1.x * c, u1.y * c, u1.z * c, u1.w * c};
+    pack_b_item(v, h, l, three, f16);
+}
+
+// Stores B item (r, kc) into the canonical (K-major, no swizzle) B layout.
+__device__ __forceinline__ void store_b_item(const TcArgs &a, int r, int kc, uint4 h, uint4 l, uint8_t *bh,
+                                             uint8_t *bl, bool three) {
+    const uint32_t off = (uint32_t)r * 16u + (uint32_t)kc * (uint32_t)a.Rpad * 16u;
     *reinterpret_cast<uint4 *>(bh + off) = h;
+    if (three) *reinterpret_cast<uint4 *>(bl + off) = l;
+}
+
+// General path: B item (r, kc) of stage g from the factors in global memory.
+__device__ __forceinline__ void general_b_item(const TcArgs &a, const TcCtrl &sm, long g, int r, int kc,
+                                               uint8_t *bh, uint8_t *bl, bool three, bool f16) {
+    float v[8];
+    if (r < a.R) {
+        kr_general(a, sm, g, r, kc, v);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = 0.f;
+    }
+    uint4 h, l;
+    pack_b_item(v, h, l, three, f16);
+    store_b_item(a, r, kc, h, l, bh, bl, three);
 }
 
 // The constant row of the fast path for the block of stages starting at g:
@@ -264,17 +334,17 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         // after __syncwarp
         for (int i = 0; i < NXMAX; i++) {
             ptx::mbar_init(&sm.full_x[i], 1);
-            ptx::mbar_init(&sm.empty_x[i], NCONV / 32);
+            ptx::mbar_init(&sm.empty_x[i], GCONV / 32);
         }
         for (int i = 0; i < NBMAX; i++) {
             ptx::mbar_init(&sm.full_u[i], 1);
-            ptx::mbar_init(&sm.empty_u[i], NKR / 32 + (CIPT > 0 ? NCONV / 32 : 0));
-            ptx::mbar_init(&sm.full_a[i], (NCONV + NKR) / 32);
+            ptx::mbar_init(&sm.empty_u[i], KRW / 32 + (CIPT > 0 ? GCONV / 32 : 0));
+            ptx::mbar_init(&sm.full_a[i], (GCONV + KRW) / 32);
             ptx::mbar_init(&sm.empty_a[i], 1);
         }
         for (int b = 0; b < 2; b++) {
             ptx::mbar_init(&sm.d_full[b], 1);
-            ptx::mbar_init(&sm.d_free[b], 4);  // the first converter warp of each lane quarter
+            ptx::mbar_init(&sm.d_free[b], 4);  // the flushing group's four warps
         }
         ptx::mbar_init(&sm.done, 1);
         sm.abort = 0;
@@ -304,32 +374,41 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
         if (lane == 0) {
+            // stage coordinates advance by counters (no division in the loop):
+            // kind 1 stage g = s * psteps + p; uk = first kappa of the stage
+            // modulo the fastest generating factor's rows
+            Ring xr(nx), ur(nb);
+            long ks = (a.kind == 0) ? 0 : st_beg / a.psteps;
+            long kp = (a.kind == 0) ? st_beg : st_beg % a.psteps;
+            const long rows0 = sm.grows[0];
+            long uk = a.fast ? (kp * BKS) % rows0 : 0;
             for (long i = 0; i < nst && !*abort; i++) {
-                const long g = st_beg + i;
                 {
-                    const int slot = (int)(i % nx);
-                    const long use = i / nx;
-                    if (use > 0 && !ptx::mbar_wait(&sm.empty_x[slot], (uint32_t)((use - 1) & 1), abort)) break;
-                    uint8_t *dst = xring + (size_t)slot * X_STAGE_BYTES;
-                    ptx::mbar_arrive_expect_tx(&sm.full_x[slot], (uint32_t)X_STAGE_BYTES);
+                    if (xr.use > 0 && !ptx::mbar_wait(&sm.empty_x[xr.slot], xr.prev_parity(), abort)) break;
+                    uint8_t *dst = xring + (size_t)xr.slot * X_STAGE_BYTES;
+                    ptx::mbar_arrive_expect_tx(&sm.full_x[xr.slot], (uint32_t)X_STAGE_BYTES);
                     if (a.kind == 0) {
-                        ptx::tma_load_2d(dst, &tmap, &sm.full_x[slot], (int)q0, (int)(g * BKS));
+                        ptx::tma_load_2d(dst, &tmap, &sm.full_x[xr.slot], (int)q0, (int)(kp * BKS));
                     } else {
-                        const long s = g / a.psteps, p0 = (g % a.psteps) * BKS;
-                        ptx::tma_load_3d(dst, &tmap, &sm.full_x[slot], (int)p0, (int)q0, (int)s);
+                        ptx::tma_load_3d(dst, &tmap, &sm.full_x[xr.slot], (int)(kp * BKS), (int)q0, (int)ks);
                     }
                     issued_x = i + 1;
                 }
                 if (a.fast) {
-                    const int slot = (int)(i % nb);
-                    const long use = i / nb;
-                    if (use > 0 && !ptx::mbar_wait(&sm.empty_u[slot], (uint32_t)((use - 1) & 1), abort)) break;
-                    // first kappa of the stage along the fastest generating factor
-                    const long kf = (a.kind == 0) ? g * BKS : (g % a.psteps) * BKS;
-                    ptx::mbar_arrive_expect_tx(&sm.full_u[slot], ubytes);
-                    ptx::tma_load_2d(ubring + (size_t)slot * ubstage, &umap, &sm.full_u[slot],
-                                     (int)(kf % sm.grows[0]), 0);
+                    if (ur.use > 0 && !ptx::mbar_wait(&sm.empty_u[ur.slot], ur.prev_parity(), abort)) break;
+                    ptx::mbar_arrive_expect_tx(&sm.full_u[ur.slot], ubytes);
+                    ptx::tma_load_2d(ubring + (size_t)ur.slot * ubstage, &umap, &sm.full_u[ur.slot], (int)uk, 0);
                     issued_u = i + 1;
+                }
+                xr.next();
+                ur.next();
+                kp++;
+                uk += BKS;
+                if (uk == rows0) uk = 0;
+                if (a.kind != 0 && kp == a.psteps) {
+                    kp = 0;
+                    ks++;
+                    uk = 0;  // rows0 divides P = psteps * BKS on the fast path
                 }
             }
         }
@@ -338,9 +417,10 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         if (lane == 0) {
             const uint32_t idesc = ptx::idesc_f16(f16 ? 0u : 1u, BQ, (uint32_t)a.Rpad);
             const uint32_t lbo = (uint32_t)a.Rpad * 16u;
-            for (long i = 0; i < nst; i++) {
-                const int slot = (int)(i % nb);
-                const long use = i / nb;
+            Ring ar(nb);
+            for (long i = 0; i < nst; i++, ar.next()) {
+                const int slot = ar.slot;
+                const long use = ar.use;
                 const long seg = i / SEG;
                 const int b = (int)(seg & 1);
                 const bool seg_first = (i % SEG) == 0;
@@ -377,14 +457,17 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         }
     } else if (warp < 10) {
         // ------------------------------------------------------------ A converters
+        // Two groups of four warps (one warp per TMEM lane quarter); group
+        // grp converts the stages i with i % 2 == grp, all 32 contraction
+        // values of its row, so two stages are converted at a time.
         const int sub = warp & 3;                 // TMEM sub-partition of this warp
-        const int half = (warp - 2) >> 2;         // which 16 of the stage's 32 contraction values
+        const int grp = (warp - 2) >> 2;          // stage parity of this warp's group
         const int row = sub * 32 + lane;          // row within the tile (= TMEM lane)
         const uint32_t lane_off = (uint32_t)(sub * 32) << 16;
         const long q = q0 + row;
-        const int ct = threadIdx.x - 64;  // converter thread 0..255
+        const int ct = row;  // converter thread within its group, 0..127
         const long blk = a.fast ? (long)(sm.grows[0] / BKS) : 1;
-        long pos = a.fast ? st_beg % blk : 0;
+        long pos = a.fast ? (st_beg + grp) % blk : 0;  // stage index within its row block
         float ccv[CIPT > 0 ? CIPT : 1];
 #pragma unroll
         for (int j = 0; j < (CIPT > 0 ? CIPT : 1); j++) ccv[j] = 0.f;
@@ -424,149 +507,184 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             __syncwarp();
             if (lane == 0) ptx::mbar_arrive(&sm.d_free[b]);
         };
-        for (long i = 0; i < nst; i++) {
-            const int xslot = (int)(i % nx), slot = (int)(i % nb);
-            const long xuse = i / nx, use = i / nb;
+        Ring xr(nx), ar(nb);
+        if (grp) {
+            xr.next();
+            ar.next();
+        }
+        for (long i = grp; i < nst; i += GROUPS, xr.next(GROUPS), ar.next(GROUPS)) {
+            const int xslot = xr.slot, slot = ar.slot;
+            const long xuse = xr.use, use = ar.use;
             // After an abort the loop keeps running (without waiting) so every
             // converter thread reaches the same warp-aligned tcgen05 instructions.
             if (use > 0 && !*abort) ptx::mbar_wait(&sm.empty_a[slot], (uint32_t)((use - 1) & 1), abort);
             if (!*abort) ptx::mbar_wait(&sm.full_x[xslot], (uint32_t)(xuse & 1), abort);
             if (CIPT > 0 && a.fast && !*abort) ptx::mbar_wait(&sm.full_u[slot], (uint32_t)(use & 1), abort);
             __syncwarp();
-            float x[KHALF];
+            float x[BKS];
             const float *xs = reinterpret_cast<const float *>(xring + (size_t)xslot * X_STAGE_BYTES);
             if (a.kind == 0) {
 #pragma unroll
-                for (int k = 0; k < KHALF; k++) x[k] = xs[(KHALF * half + k) * BQ + row];
+                for (int k = 0; k < BKS; k++) x[k] = xs[k * BQ + row];
             } else {
                 const float4 *r4 = reinterpret_cast<const float4 *>(xs + row * BKS);
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    float4 v = r4[(4 * half + c) ^ (row & 7)];
+                for (int c = 0; c < BKS / 4; c++) {
+                    float4 v = r4[c ^ (row & 7)];
                     x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
                 }
             }
-            // this thread's B items' U values, then the slot is free for the next load
-            float4 cu0[CIPT > 0 ? CIPT : 1], cu1[CIPT > 0 ? CIPT : 1];
-            if (CIPT > 0 && a.fast) {
-                const float *us = reinterpret_cast<const float *>(ubring + (size_t)slot * ubstage);
-#pragma unroll
-                for (int j = 0; j < CIPT; j++) {
-                    const int id = a.nkri + ct + NCONV * j;
-                    int r, kc;
-                    b_item(id < 4 * a.Rpad ? id : 0, r, kc);
-                    load_u_item(us, r, kc, cu0[j], cu1[j]);
-                }
-            }
+            // A stage: hi in columns 0-15, lo in 16-31 (2 values per column),
+            // as two halves of 16 contraction values
+            uint32_t hi0[8], lo0[8], hi1[8], lo1[8];
+            split_half(x, 0, hi0, lo0, three, f16);
+            split_half(x, 16, hi1, lo1, three, f16);
+            // A release must follow the instructions that consume the loaded
+            // values: an arrive issued while a shared-memory load is still in
+            // flight lets the next TMA overwrite the data under it.  The split
+            // above reads every X value.
             __syncwarp();
-            if (lane == 0) {
-                ptx::mbar_arrive(&sm.empty_x[xslot]);  // the X tile is consumed
-                if (CIPT > 0 && a.fast) ptx::mbar_arrive(&sm.empty_u[slot]);
+            if (lane == 0) ptx::mbar_arrive(&sm.empty_x[xslot]);  // the X tile is consumed
+            const uint32_t ta = tbase + lane_off + a_col0 + (uint32_t)slot * 32u;
+            ptx::tmem_st8(ta, hi0);
+            ptx::tmem_st8(ta + 8u, hi1);
+            if (three) {
+                ptx::tmem_st8(ta + 16u, lo0);
+                ptx::tmem_st8(ta + 24u, lo1);
             }
-            uint32_t hi[KHALF / 2], lo[KHALF / 2];
-            if (f16) {
-#pragma unroll
-                for (int c = 0; c < KHALF / 2; c++) hi[c] = pack_f16(x[2 * c], x[2 * c + 1]);
-            } else if (three) {
-#pragma unroll
-                for (int c = 0; c < KHALF / 2; c++) split_pair(x[2 * c], x[2 * c + 1], hi[c], lo[c]);
-            } else {
-#pragma unroll
-                for (int c = 0; c < KHALF / 2; c++) hi[c] = pack_bf16(x[2 * c], x[2 * c + 1]);
-            }
-            // A stage: hi in columns 0-15, lo in 16-31 (2 values per column);
-            // this warp's half is 8 columns of each
-            const uint32_t ta = tbase + lane_off + a_col0 + (uint32_t)slot * 32u + 8u * (uint32_t)half;
-            ptx::tmem_st8(ta, hi);
-            if (three) ptx::tmem_st8(ta + 16, lo);
             // this thread's share of the B tile
             if (CIPT > 0) {
                 const long g = st_beg + i;
-                if (a.fast && (i == 0 || pos == 0)) {
+                // the constant row changed since this group's previous stage
+                if (a.fast && (i == grp || pos < GROUPS)) {
 #pragma unroll
                     for (int j = 0; j < CIPT; j++) {
-                        const int id = a.nkri + ct + NCONV * j;
+                        const int id = a.nkri + ct + GCONV * j;
                         int r, kc;
                         b_item(id, r, kc);
                         ccv[j] = (id < 4 * a.Rpad && r < a.R) ? kr_const_row(a, sm, g, r) : 0.f;
                     }
                 }
                 uint8_t *bh = ubring + (size_t)slot * ubstage + ubytes;
+                if (a.fast) {
+                    // the items' words from the U tile; they consume every U
+                    // value read, so the tile can be released after them
+                    const float *us = reinterpret_cast<const float *>(ubring + (size_t)slot * ubstage);
+                    uint4 ch[CIPT > 0 ? CIPT : 1], cl[CIPT > 0 ? CIPT : 1];
 #pragma unroll
-                for (int j = 0; j < CIPT; j++) {
-                    const int id = a.nkri + ct + NCONV * j;
-                    if (id < 4 * a.Rpad) {
+                    for (int j = 0; j < CIPT; j++) {
+                        const int id = a.nkri + ct + GCONV * j;
                         int r, kc;
-                        b_item(id, r, kc);
-                        make_b_item(a, sm, g, r, kc, ccv[j], cu0[j], cu1[j], bh, bh + bbytes, three, f16);
+                        b_item(id < 4 * a.Rpad ? id : 0, r, kc);
+                        float4 u0, u1;
+                        load_u_item(us, r, kc, u0, u1);
+                        fast_b_item(ccv[j], u0, u1, ch[j], cl[j], three, f16);
+                    }
+                    __syncwarp();
+                    if (lane == 0) ptx::mbar_arrive(&sm.empty_u[slot]);
+#pragma unroll
+                    for (int j = 0; j < CIPT; j++) {
+                        const int id = a.nkri + ct + GCONV * j;
+                        if (id < 4 * a.Rpad) {
+                            int r, kc;
+                            b_item(id, r, kc);
+                            store_b_item(a, r, kc, ch[j], cl[j], bh, bh + bbytes, three);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < CIPT; j++) {
+                        const int id = a.nkri + ct + GCONV * j;
+                        if (id < 4 * a.Rpad) {
+                            int r, kc;
+                            b_item(id, r, kc);
+                            general_b_item(a, sm, g, r, kc, bh, bh + bbytes, three, f16);
+                        }
                     }
                 }
                 ptx::fence_proxy_async_smem();  // generic-proxy B writes -> tensor core
             }
-            if (a.fast) pos = (pos + 1 == blk) ? 0 : pos + 1;
+            if (a.fast) {
+                pos += GROUPS;
+                while (pos >= blk) pos -= blk;
+            }
             ptx::tmem_wait_st();
             ptx::tc_fence_before();
             __syncwarp();
             if (lane == 0) ptx::mbar_arrive(&sm.full_a[slot]);
             // a segment just ended: drain the one before it (long finished);
-            // the first converter warp of each lane quarter does the flushes
-            if (half == 0 && (i % SEG) == SEG - 1 && i / SEG >= 1) flush(flushed++);
+            // the group converting each segment's last stage does the flushes
+            if (grp == FLUSH_GRP && (i % SEG) == SEG - 1 && i / SEG >= 1) flush(flushed++);
         }
-        if (half == 0)
+        if (grp == FLUSH_GRP)
             while (flushed < nseg) flush(flushed++);
     } else {
         // ------------------------------------------------------------ KR producers
-        const int kt = threadIdx.x - (64 + NCONV);  // 0..63
+        // one warp per stage parity, like the converter groups
+        const int kgrp = warp - 10;
+        const int kt = lane;
         // fast path: the stage's 32 rows of the fastest generating factor
         // arrive by TMA with X; the constant row changes every `blk` stages
         const long blk = a.fast ? (long)(sm.grows[0] / BKS) : 1;
-        long pos = a.fast ? st_beg % blk : 0;  // stage index within its block
+        long pos = a.fast ? (st_beg + kgrp) % blk : 0;  // stage index within its block
         float cc[KIPT];
 #pragma unroll
         for (int it = 0; it < KIPT; it++) cc[it] = 0.f;
-        for (long i = 0; i < nst; i++, pos = (pos + 1 == blk) ? 0 : pos + 1) {
-            const int slot = (int)(i % nb);
-            const long use = i / nb;
+        Ring ar(nb);
+        if (kgrp) ar.next();
+        for (long i = kgrp; i < nst; i += GROUPS, ar.next(GROUPS)) {
+            const int slot = ar.slot;
+            const long use = ar.use;
             const long g = st_beg + i;
-            if (a.fast && (i == 0 || pos == 0)) {
+            // the constant row changed since this warp's previous stage
+            if (a.fast && (i == kgrp || pos < GROUPS)) {
 #pragma unroll
                 for (int it = 0; it < KIPT; it++) {
-                    const int id = kt + NKR * it;
+                    const int id = kt + KRW * it;
                     int r, kc;
                     b_item(id, r, kc);
                     cc[it] = (id < a.nkri && r < a.R) ? kr_const_row(a, sm, g, r) : 0.f;
                 }
             }
             uint8_t *st = ubring + (size_t)slot * ubstage;
-            float4 ku0[KIPT], ku1[KIPT];
+            // the slot's B tile is free once the MMA of stage i - nb is done
+            if (use > 0 && !*abort) ptx::mbar_wait(&sm.empty_a[slot], (uint32_t)((use - 1) & 1), abort);
+            uint4 kh[KIPT], kl[KIPT];
             if (a.fast) {
-                // the U tile: read this thread's values, then release the slot
+                // the U tile: make this thread's items' words (they consume
+                // every U value read), then release the tile
                 if (!*abort) ptx::mbar_wait(&sm.full_u[slot], (uint32_t)(use & 1), abort);
                 const float *us = reinterpret_cast<const float *>(st);
 #pragma unroll
                 for (int it = 0; it < KIPT; it++) {
-                    const int id = kt + NKR * it;
+                    const int id = kt + KRW * it;
                     int r, kc;
                     b_item(id < a.nkri ? id : 0, r, kc);
-                    load_u_item(us, r, kc, ku0[it], ku1[it]);
+                    float4 u0, u1;
+                    load_u_item(us, r, kc, u0, u1);
+                    fast_b_item(cc[it], u0, u1, kh[it], kl[it], three, f16);
                 }
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(&sm.empty_u[slot]);
             }
-            if (use > 0 && !*abort) ptx::mbar_wait(&sm.empty_a[slot], (uint32_t)((use - 1) & 1), abort);
             uint8_t *bh = st + ubytes;
 #pragma unroll
             for (int it = 0; it < KIPT; it++) {
-                const int id = kt + NKR * it;
+                const int id = kt + KRW * it;
                 if (id < a.nkri) {
                     int r, kc;
                     b_item(id, r, kc);
-                    make_b_item(a, sm, g, r, kc, cc[it], ku0[it], ku1[it], bh, bh + bbytes, three, f16);
+                    if (a.fast) store_b_item(a, r, kc, kh[it], kl[it], bh, bh + bbytes, three);
+                    else general_b_item(a, sm, g, r, kc, bh, bh + bbytes, three, f16);
                 }
             }
             ptx::fence_proxy_async_smem();  // generic-proxy B writes -> tensor core
             __syncwarp();
             if (lane == 0) ptx::mbar_arrive(&sm.full_a[slot]);
+            if (a.fast) {
+                pos += GROUPS;
+                while (pos >= blk) pos -= blk;
+            }
         }
     }
 
@@ -597,7 +715,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 // summed by 8 lanes over the splits z = lane, lane + 8, ..., then combined
 // in lane order.
 __global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict__ part, int splits, long Q,
-                                                         long R, long Rp, float *__restrict__ out) {
+                                                         long R, long Rp, const int *__restrict__ error,
+                                                         float *__restrict__ out) {
     __shared__ double red[8][32];
     const int o = threadIdx.x & 31, zl = threadIdx.x >> 5;
     const long e = blockIdx.x * 32L + o;  // q * Rp + r
@@ -613,6 +732,9 @@ __global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict
         double t = red[0][o];
         for (int k = 1; k < 8; k++) t += red[k][o];
         const long q = e / Rp, r = e - q * Rp;
+        // a CTA whose bounded wait expired left its partial incomplete: the
+        // output becomes NaN so the failure cannot pass for a result
+        if (*error) t = __longlong_as_double(0x7ff8000000000000LL);
         if (r < R) out[q + Q * r] = (float)t;
     }
 }
@@ -774,12 +896,13 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     a.nx = p.nx;
     a.nb = p.nb;
     a.Rp = (R + 3) / 4 * 4;
-    // B items: 4 per padded row; the KR warps take about a quarter (whole
-    // warps of work, at least 64), the eight converter warps the rest
+    // B items: 4 per padded row; the stage's KR warp makes the first nkri
+    // (64 with two CTAs per SM, 128 with one), the stage's converter group
+    // the rest
     const int ni = 4 * (int)p.Rpad;
-    a.nkri = std::max(64, (ni / 4) / 64 * 64);
-    const int kipt_need = a.nkri / NKR;
-    const int cipt_need = (ni - a.nkri + NCONV - 1) / NCONV;
+    a.nkri = std::min(ni, p.ctas_per_sm == 2 ? CUD_TC_KR_ITEMS : 2 * CUD_TC_KR_ITEMS);
+    const int kipt_need = (a.nkri + KRW - 1) / KRW;
+    const int cipt_need = (ni - a.nkri + GCONV - 1) / GCONV;
     a.gen.n = 0;
     a.outer.n = 0;
     for (int m = 0; m < order; m++) {
@@ -800,15 +923,17 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     const size_t smem = tc_smem_bytes((int)p.Rpad, p.fast, p.nx, p.nb);
     int st;
     if (p.ctas_per_sm == 2) {
-        if (kipt_need <= 1 && cipt_need <= 0) st = launch_tc<1, 0, 2>(tmap, umap, a, smem, grid, s);
-        else if (kipt_need <= 1 && cipt_need <= 1) st = launch_tc<1, 1, 2>(tmap, umap, a, smem, grid, s);
-        else st = launch_tc<2, 2, 2>(tmap, umap, a, smem, grid, s);
+        if (kipt_need <= 2 && cipt_need <= 0) st = launch_tc<2, 0, 2>(tmap, umap, a, smem, grid, s);
+        else if (kipt_need <= 2 && cipt_need <= 1) st = launch_tc<2, 1, 2>(tmap, umap, a, smem, grid, s);
+        else if (kipt_need <= 2 && cipt_need <= 2) st = launch_tc<2, 2, 2>(tmap, umap, a, smem, grid, s);
+        else return CUD_ERR_UNSUPPORTED;  // two CTAs per SM only hold Rpad <= 80 (TMEM)
     } else {
-        if (kipt_need <= 2 && cipt_need <= 2) st = launch_tc<2, 2, 1>(tmap, umap, a, smem, grid, s);
-        else st = launch_tc<4, 2, 1>(tmap, umap, a, smem, grid, s);
+        if (kipt_need <= 4 && cipt_need <= 3) st = launch_tc<4, 3, 1>(tmap, umap, a, smem, grid, s);
+        else return CUD_ERR_UNSUPPORTED;  // Rpad <= 128 needs at most 4 / 3
     }
     if (st) return st;
-    k_sum_tc_partials<<<(unsigned)((p.Q * a.Rp + 31) / 32), 256, 0, s>>>(a.part, (int)p.splits, p.Q, R, a.Rp, out);
+    k_sum_tc_partials<<<(unsigned)((p.Q * a.Rp + 31) / 32), 256, 0, s>>>(a.part, (int)p.splits, p.Q, R, a.Rp,
+                                                                         a.error, out);
     CUD_CHECK_LAUNCH("mttkrp_tc reduce");
     return CUD_OK;
 }
