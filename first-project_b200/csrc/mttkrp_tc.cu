@@ -87,6 +87,9 @@ struct TcArgs {
     KrFactors outer;   // kind 1: factors after the mode (one constant row per stage)
     float *part;       // [split][Q][Rp]
     int *error;        // device flag
+    const uint8_t *pb; // pre-packed B path: blk B tiles (hi, lo) of the fastest generating factor
+    long blk;          // stages per constant-row block (rows of the fastest generating factor / 32)
+    int seg;           // pre-packed B path: stages per accumulation segment (even, divides blk)
 };
 
 struct TcCtrl {
@@ -283,7 +286,8 @@ __device__ __forceinline__ void general_b_item(const TcArgs &a, const TcCtrl &sm
 // the product over the slower generating factors (digits of kappa / rows0)
 // and the outer factors (digits of s) of their row for column r (32-bit
 // digit arithmetic, as above).
-__device__ __forceinline__ float kr_const_row(const TcArgs &a, const TcCtrl &sm, long g, int r) {
+template <class Ctrl>
+__device__ __forceinline__ float kr_const_row(const TcArgs &a, const Ctrl &sm, long g, int r) {
     const uint32_t gs = (uint32_t)g, ps = (uint32_t)a.psteps;
     uint32_t k0, s;
     if (a.kind == 0) { k0 = gs * BKS; s = 0; }
@@ -710,6 +714,349 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     if (warp == 0) ptx::tmem_dealloc(tbase, a.tmem_cols);
 }
 
+// ---------------------------------------------------------------- pre-packed B path
+//
+// On the fast path the stage's Khatri-Rao rows are U0's 32 rows for the
+// stage times one constant row c (the other factors), and c only changes
+// from one block of blk = rows0 / 32 stages to the next.  With segments
+// that never straddle a block, the segment's accumulation can use the
+// unscaled U0 rows as B and apply c once, when the segment is flushed:
+// partial[q][r] += c[r] * T[q][r].  The unscaled B tiles (one per stage
+// position in a block, hi + lo, already in the MMA's canonical layout) are
+// packed once per call by k_pack_b and copied into shared memory per stage
+// by one bulk copy, so no warp builds B per stage.  Roles:
+//   * warp 0: TMA of the X tile and bulk copy of the stage's B tile;
+//   * warp 1: MMA issuer (as above);
+//   * warps 2-9: A converters in two stage-parity groups (as above), the
+//     odd group flushing segments, scaled by c;
+//   * warp 10: the constant row c of each segment into shared memory.
+constexpr int PB_THREADS = 352;
+constexpr int PB_RING = 6;  // deepest X ring = A/B ring
+
+struct PbCtrl {
+    uint64_t full_x[PB_RING], empty_x[PB_RING], full_a[PB_RING], empty_a[PB_RING];
+    uint64_t d_full[2], d_free[2], c_full[2], done;
+    const float *gU[kMaxOrder];
+    const float *oU[kMaxOrder];
+    long grows[kMaxOrder], orows[kMaxOrder];
+    alignas(16) float cvec[2][RPAD_MAX];  // constant row of the segment in D buffer b
+    uint32_t tmem_base;
+    int abort;
+};
+
+constexpr size_t PB_CTRL_BYTES = (sizeof(PbCtrl) + 1023) & ~size_t(1023);
+
+__host__ __device__ constexpr size_t pb_smem_bytes(int Rpad, int n) {
+    return 1024 + PB_CTRL_BYTES + (size_t)n * (X_STAGE_BYTES + 2 * b_tile_bytes(Rpad));
+}
+
+// B tiles of the pre-packed path: tile t holds U0 rows 32t..32t+31 for every
+// column r (zero for r >= R), hi then lo, each in the canonical layout above.
+// One thread per (tile, 8-row chunk kc, column r); consecutive threads write
+// consecutive 16-byte chunks.
+__global__ void __launch_bounds__(256) k_pack_b(const float *__restrict__ U0, long rows0, long R, int Rpad,
+                                                long blk, int prec, uint8_t *__restrict__ pb) {
+    const long n = blk * 4 * Rpad;
+    const long id = blockIdx.x * 256L + threadIdx.x;
+    if (id >= n) return;
+    const long t = id / (4 * Rpad);
+    const int rem = (int)(id - t * 4 * Rpad);
+    const int kc = rem / Rpad, r = rem - kc * Rpad;
+    float v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = (r < R) ? __ldg(U0 + 32 * t + 8 * kc + j + (long)r * rows0) : 0.f;
+    const bool three = (prec == CUD_PREC_BF16X3 || prec == CUD_PREC_DEFAULT);
+    uint4 h, l;
+    pack_b_item(v, h, l, three, prec == CUD_PREC_FP16);
+    const size_t bbytes = b_tile_bytes(Rpad);
+    uint8_t *tile = pb + (size_t)t * 2 * bbytes;
+    const size_t off = (size_t)r * 16 + (size_t)kc * Rpad * 16;
+    *reinterpret_cast<uint4 *>(tile + off) = h;
+    *reinterpret_cast<uint4 *>(tile + bbytes + off) = l;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(PB_THREADS, MINB)
+    k_mttkrp_pb(const __grid_constant__ CUtensorMap tmap, TcArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    PbCtrl &sm = *reinterpret_cast<PbCtrl *>(base);
+    const int nx = a.nx, nb = a.nb;  // equal: see the parity note at the converters
+    uint8_t *xring = base + PB_CTRL_BYTES;                 // nx X tiles
+    uint8_t *bring = xring + (size_t)nx * X_STAGE_BYTES;   // nb B tiles (hi, lo)
+    const uint32_t bbytes = (uint32_t)b_tile_bytes(a.Rpad);
+    const uint32_t bstage = 2u * bbytes;
+    const uint32_t a_col0 = 2u * (uint32_t)a.Rpad;  // two D buffers first, then the A stages
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long qtile = blockIdx.x % a.qtiles;
+    const long z = blockIdx.x / a.qtiles;
+    const long q0 = qtile * BQ;
+    const long st_beg = z * a.chunk;  // even: local and global stage parities agree
+    const long st_end = min(a.stages, st_beg + a.chunk);
+    const long nst = st_end - st_beg;
+    const int seg = a.seg;
+    // segments are aligned to multiples of seg in the global stage index, so
+    // none straddles a constant-row block; the CTA's first may be partial
+    const int sp0 = (int)(st_beg % seg);
+    const long nseg = (sp0 + nst + seg - 1) / seg;
+    volatile int *abort = &sm.abort;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < PB_RING; i++) {
+            ptx::mbar_init(&sm.full_x[i], 1);
+            ptx::mbar_init(&sm.empty_x[i], GCONV / 32);
+            ptx::mbar_init(&sm.full_a[i], GCONV / 32 + 1);  // converter group + the B copy
+            ptx::mbar_init(&sm.empty_a[i], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            ptx::mbar_init(&sm.d_full[b], 1);
+            ptx::mbar_init(&sm.d_free[b], 4);  // the flushing group's four warps
+            ptx::mbar_init(&sm.c_full[b], 1);
+        }
+        ptx::mbar_init(&sm.done, 1);
+        sm.abort = 0;
+        for (int f = 0; f < kMaxOrder; f++) {
+            sm.gU[f] = f < a.gen.n ? a.gen.U[f] : nullptr;
+            sm.grows[f] = f < a.gen.n ? a.gen.rows[f] : 1;
+            sm.oU[f] = f < a.outer.n ? a.outer.U[f] : nullptr;
+            sm.orows[f] = f < a.outer.n ? a.outer.rows[f] : 1;
+        }
+        ptx::fence_mbar_init();
+        ptx::prefetch_tmap(&tmap);
+    }
+    if (warp == 0) {
+        ptx::tmem_alloc(&sm.tmem_base, a.tmem_cols);
+        ptx::tmem_relinquish();
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tbase = sm.tmem_base;
+
+    const bool three = (a.prec == CUD_PREC_BF16X3 || a.prec == CUD_PREC_DEFAULT);
+    const bool f16 = (a.prec == CUD_PREC_FP16);
+
+    long issued_x = 0, issued_b = 0;  // copies issued (producer thread)
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            Ring xr(nx), br(nb);
+            long ks = (a.kind == 0) ? 0 : st_beg / a.psteps;
+            long kp = (a.kind == 0) ? st_beg : st_beg % a.psteps;
+            long pos = st_beg % a.blk;  // stage position in its block = B tile
+            for (long i = 0; i < nst && !*abort; i++) {
+                if (xr.use > 0 && !ptx::mbar_wait(&sm.empty_x[xr.slot], xr.prev_parity(), abort)) break;
+                uint8_t *dst = xring + (size_t)xr.slot * X_STAGE_BYTES;
+                ptx::mbar_arrive_expect_tx(&sm.full_x[xr.slot], (uint32_t)X_STAGE_BYTES);
+                if (a.kind == 0) ptx::tma_load_2d(dst, &tmap, &sm.full_x[xr.slot], (int)q0, (int)(kp * BKS));
+                else ptx::tma_load_3d(dst, &tmap, &sm.full_x[xr.slot], (int)(kp * BKS), (int)q0, (int)ks);
+                issued_x = i + 1;
+                // the slot's B tile is free once the MMA of stage i - nb is done
+                if (br.use > 0 && !ptx::mbar_wait(&sm.empty_a[br.slot], br.prev_parity(), abort)) break;
+                ptx::mbar_arrive_expect_tx(&sm.full_a[br.slot], bstage);
+                ptx::bulk_load(bring + (size_t)br.slot * bstage, a.pb + (size_t)pos * bstage, bstage,
+                               &sm.full_a[br.slot]);
+                issued_b = i + 1;
+                xr.next();
+                br.next();
+                kp++;
+                if (a.kind != 0 && kp == a.psteps) {
+                    kp = 0;
+                    ks++;
+                }
+                if (++pos == a.blk) pos = 0;  // blk divides psteps on the fast path
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = ptx::idesc_f16(f16 ? 0u : 1u, BQ, (uint32_t)a.Rpad);
+            const uint32_t lbo = (uint32_t)a.Rpad * 16u;
+            Ring ar(nb);
+            int sp = sp0;
+            long si = 0;  // segment of the CTA (0 = the first, possibly partial)
+            for (long i = 0; i < nst; i++) {
+                const int slot = ar.slot;
+                const long use = ar.use;
+                const int b = (int)(si & 1);
+                const bool seg_first = (sp == 0) || (i == 0);
+                // the segment's D buffer must have been drained (segment si - 2)
+                if (seg_first && si >= 2 &&
+                    !ptx::mbar_wait(&sm.d_free[b], (uint32_t)(((si >> 1) - 1) & 1), abort)) break;
+                if (!ptx::mbar_wait(&sm.full_a[slot], (uint32_t)(use & 1), abort)) break;
+                ptx::tc_fence_after();
+                const uint32_t d = tbase + (uint32_t)b * (uint32_t)a.Rpad;
+                const uint32_t a_hi = tbase + a_col0 + (uint32_t)slot * 32u;
+                const uint32_t a_lo = a_hi + 16u;
+                const uint32_t b_hi = ptx::smem_addr(bring + (size_t)slot * bstage);
+                const uint32_t b_lo = b_hi + bbytes;
+                uint32_t acc = seg_first ? 0u : 1u;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    uint64_t dh = ptx::smem_desc_kmajor_noswizzle(b_hi + 2 * j * lbo, lbo, 128);
+                    ptx::mma_ts_f16(d, a_hi + j * 8, dh, idesc, acc);
+                    acc = 1;
+                    if (three) {
+                        uint64_t dl = ptx::smem_desc_kmajor_noswizzle(b_lo + 2 * j * lbo, lbo, 128);
+                        ptx::mma_ts_f16(d, a_hi + j * 8, dl, idesc, 1);
+                        ptx::mma_ts_f16(d, a_lo + j * 8, dh, idesc, 1);
+                    }
+                }
+                ptx::mma_commit(&sm.empty_a[slot]);
+                if (sp == seg - 1 || i == nst - 1) ptx::mma_commit(&sm.d_full[b]);
+                ar.next();
+                if (++sp == seg) {
+                    sp = 0;
+                    si++;
+                }
+            }
+            ptx::mma_commit(&sm.done);
+            for (long it = 0; it < 40000 && !ptx::mbar_try_wait_hint(&sm.done, 0, 100000u); it++) {
+            }
+        }
+    } else if (warp < 10) {
+        // ------------------------------------------------------------ A converters
+        // Two groups of four warps, group grp converting the stages i with
+        // i % 2 == grp.  Parity waits: every wait here comes after the wait
+        // for the MMA of stage i - nb, which ran after the other group's
+        // full_x wait for that stage; with nx == nb the X slot's previous
+        // phase is therefore complete and the parity is exact.
+        const int sub = warp & 3;
+        const int grp = (warp - 2) >> 2;
+        const int row = sub * 32 + lane;
+        const uint32_t lane_off = (uint32_t)(sub * 32) << 16;
+        const long q = q0 + row;
+        float *P = a.part + (z * a.Q + q) * a.Rp;
+        long flushed = 0;
+        // Adds finished segment `sg` (TMEM buffer sg & 1) times its constant
+        // row into the partial.
+        auto flush = [&](long sg) {
+            const int b = (int)(sg & 1);
+            if (!*abort) ptx::mbar_wait(&sm.d_full[b], (uint32_t)((sg >> 1) & 1), abort);
+            if (!*abort) ptx::mbar_wait(&sm.c_full[b], (uint32_t)((sg >> 1) & 1), abort);
+            const bool ok = __all_sync(0xffffffffu, *abort == 0);  // warp-uniform tcgen05.ld
+            if (ok) {
+                ptx::tc_fence_after();
+                const uint32_t d = tbase + lane_off + (uint32_t)b * (uint32_t)a.Rpad;
+                for (int c0 = 0; c0 < a.Rpad; c0 += 16) {
+                    uint32_t v[16];
+                    ptx::tmem_ld16(d + (uint32_t)c0, v);
+                    ptx::tmem_wait_ld();
+                    if (q < a.Q) {
+#pragma unroll
+                        for (int j4 = 0; j4 < 4; j4++) {
+                            const int c = c0 + 4 * j4;
+                            if (c < a.R) {
+                                const float4 cv = *reinterpret_cast<const float4 *>(&sm.cvec[b][c]);
+                                const uint32_t *w = &v[j4 * 4];
+                                float4 val = make_float4(__uint_as_float(w[0]) * cv.x, __uint_as_float(w[1]) * cv.y,
+                                                         __uint_as_float(w[2]) * cv.z, __uint_as_float(w[3]) * cv.w);
+                                float *pp = P + c;
+                                if (sg == 0) *reinterpret_cast<float4 *>(pp) = val;
+                                else asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(pp),
+                                                  "f"(val.x), "f"(val.y), "f"(val.z), "f"(val.w)
+                                                  : "memory");  // RN
+                            }
+                        }
+                    }
+                }
+                ptx::tc_fence_before();
+            }
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.d_free[b]);
+        };
+        Ring xr(nx), ar(nb);
+        int sp = sp0 + grp;
+        long si = 0;
+        if (sp >= seg) {
+            sp -= seg;
+            si = 1;
+        }
+        if (grp) {
+            xr.next();
+            ar.next();
+        }
+        for (long i = grp; i < nst; i += GROUPS, xr.next(GROUPS), ar.next(GROUPS)) {
+            const int xslot = xr.slot, slot = ar.slot;
+            const long xuse = xr.use, use = ar.use;
+            if (use > 0 && !*abort) ptx::mbar_wait(&sm.empty_a[slot], (uint32_t)((use - 1) & 1), abort);
+            if (!*abort) ptx::mbar_wait(&sm.full_x[xslot], (uint32_t)(xuse & 1), abort);
+            __syncwarp();
+            float x[BKS];
+            const float *xs = reinterpret_cast<const float *>(xring + (size_t)xslot * X_STAGE_BYTES);
+            if (a.kind == 0) {
+#pragma unroll
+                for (int k = 0; k < BKS; k++) x[k] = xs[k * BQ + row];
+            } else {
+                const float4 *r4 = reinterpret_cast<const float4 *>(xs + row * BKS);
+#pragma unroll
+                for (int c = 0; c < BKS / 4; c++) {
+                    float4 v = r4[c ^ (row & 7)];
+                    x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+                }
+            }
+            uint32_t hi0[8], lo0[8], hi1[8], lo1[8];
+            split_half(x, 0, hi0, lo0, three, f16);
+            split_half(x, 16, hi1, lo1, three, f16);
+            // released after the split, which reads every loaded X value
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.empty_x[xslot]);
+            const uint32_t ta = tbase + lane_off + a_col0 + (uint32_t)slot * 32u;
+            ptx::tmem_st8(ta, hi0);
+            ptx::tmem_st8(ta + 8u, hi1);
+            if (three) {
+                ptx::tmem_st8(ta + 16u, lo0);
+                ptx::tmem_st8(ta + 24u, lo1);
+            }
+            ptx::tmem_wait_st();
+            ptx::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.full_a[slot]);
+            // a segment just ended (global stage index = seg - 1 mod seg, odd,
+            // so always this group's): drain the one before it
+            if (grp == FLUSH_GRP && sp == seg - 1 && si >= 1) flush(flushed++);
+            sp += GROUPS;
+            if (sp >= seg) {
+                sp -= seg;
+                si++;
+            }
+        }
+        if (grp == FLUSH_GRP)
+            while (flushed < nseg) flush(flushed++);
+    } else {
+        // ------------------------------------------------------------ constant rows
+        const long sbase = st_beg - sp0;  // global first stage of the CTA's first segment
+        for (long sg = 0; sg < nseg; sg++) {
+            const int b = (int)(sg & 1);
+            // buffer b's previous segment (sg - 2) must have been flushed
+            if (sg >= 2 && !*abort) ptx::mbar_wait(&sm.d_free[b], (uint32_t)(((sg >> 1) - 1) & 1), abort);
+            const long g0 = (sg == 0) ? st_beg : sbase + sg * seg;
+            for (int r = lane; r < a.Rpad; r += 32) sm.cvec[b][r] = (r < a.R) ? kr_const_row(a, sm, g0, r) : 0.f;
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.c_full[b]);
+        }
+    }
+
+    // ------------------------------------------------------------ teardown
+    if (threadIdx.x == 0 && *abort) {
+        for (long i = (issued_x > nx ? issued_x - nx : 0); i < issued_x; i++) {
+            const uint32_t par = (uint32_t)((i / nx) & 1);
+            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.full_x[i % nx], par, 100000u); it++) {
+            }
+        }
+        for (long i = (issued_b > nb ? issued_b - nb : 0); i < issued_b; i++) {
+            const uint32_t par = (uint32_t)((i / nb) & 1);
+            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.full_a[i % nb], par, 100000u); it++) {
+            }
+        }
+        atomicExch(a.error, 1);
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    if (warp == 0) ptx::tmem_dealloc(tbase, a.tmem_cols);
+}
+
 // out[q + Q r] = sum_z part[z][q][r] in FP64, fixed order.  A CTA owns 32
 // consecutive (q, r) slots of the padded partial rows (coalesced reads), each
 // summed by 8 lanes over the splits z = lane, lane + 8, ..., then combined
@@ -756,7 +1103,35 @@ struct TcPlan {
     long P, Q, S, Rpad, psteps, stages, qtiles, splits, chunk;
     bool fast;
     int nx, nb, ctas_per_sm;
+    bool pb;    // pre-packed B path
+    long blk;   // stages per constant-row block (fast path)
+    int seg;    // pre-packed B path: segment length
 };
+
+// Pre-packed B path launch shape: the deepest rings (X and A/B equal, at
+// most PB_RING) whose shared memory and TMEM fit two CTAs per SM, else one
+// CTA; contraction splits of an even number of stages (so local and global
+// stage parities agree) filling one wave.
+void pb_shape(TcPlan &p) {
+    constexpr size_t kTwoCtaSmem = 115712;
+    constexpr size_t kOneCtaSmem = 232448;
+    p.ctas_per_sm = 0;
+    for (int n = PB_RING; n >= 3 && !p.ctas_per_sm; n--)
+        if (pb_smem_bytes((int)p.Rpad, n) <= kTwoCtaSmem && 2 * p.Rpad + 32 * n <= 256) {
+            p.ctas_per_sm = 2;
+            p.nx = p.nb = n;
+        }
+    for (int n = PB_RING; n >= 3 && !p.ctas_per_sm; n--)
+        if (pb_smem_bytes((int)p.Rpad, n) <= kOneCtaSmem && 2 * p.Rpad + 32 * n <= 512) {
+            p.ctas_per_sm = 1;
+            p.nx = p.nb = n;
+        }
+    long want = std::max(1L, (p.ctas_per_sm * (long)kNumSMs - 2) / p.qtiles);
+    p.splits = std::min(want, p.stages);
+    p.chunk = (p.stages + p.splits - 1) / p.splits;
+    p.chunk += p.chunk & 1;
+    p.splits = (p.stages + p.chunk - 1) / p.chunk;
+}
 
 // Launch shape: two CTAs per SM when their shared memory and TMEM (two D
 // buffers + 32 columns per A stage, at most 256 each) fit with 3 or 4
@@ -806,9 +1181,30 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     // of 32, so each stage covers 32 of its rows (one TMA box)
     const long rows0 = (mode == 0) ? dims[1] : dims[0];
     p.fast = (rows0 % BKS == 0);
-    tc_shape(p);
+    p.blk = p.fast ? rows0 / BKS : 1;
+    // pre-packed B path: a segment length that is even, at least 4 (each
+    // flush adds a whole 128 x R partial tile) and divides the block
+    p.seg = 0;
+    for (int sl = 16; sl >= 4 && p.fast; sl -= 2)
+        if (p.blk % sl == 0) {
+            p.seg = sl;
+            break;
+        }
+    p.pb = p.seg > 0;
+#ifdef CUD_TC_NO_PB
+    p.pb = false;
+#endif
+    if (p.pb) pb_shape(p);
+    else tc_shape(p);
     return true;
 }
+
+// Workspace: error flag, partials [splits][Q][Rp], then (pre-packed B path)
+// the packed B tiles.
+size_t tc_part_bytes(const TcPlan &p, long R) {
+    return (sizeof(float) * (size_t)p.splits * ((R + 3) / 4 * 4) * p.Q + 255) & ~size_t(255);
+}
+size_t tc_pb_bytes(const TcPlan &p) { return p.pb ? (size_t)p.blk * 2 * b_tile_bytes((int)p.Rpad) : 0; }
 
 template <int KIPT, int CIPT, int MINB>
 int launch_tc(const CUtensorMap &tmap, const CUtensorMap &umap, const TcArgs &a, size_t smem, unsigned grid,
@@ -826,13 +1222,27 @@ int launch_tc(const CUtensorMap &tmap, const CUtensorMap &umap, const TcArgs &a,
     return CUD_OK;
 }
 
+template <int MINB>
+int launch_pb(const CUtensorMap &tmap, const TcArgs &a, size_t smem, unsigned grid, cudaStream_t s) {
+    static bool attr[64] = {false};
+    int dev = 0;
+    CUD_CHECK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !attr[dev]) {
+        CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_pb<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
+        attr[dev] = true;
+    }
+    k_mttkrp_pb<MINB><<<grid, PB_THREADS, smem, s>>>(tmap, a);
+    CUD_CHECK_LAUNCH("mttkrp_pb");
+    return CUD_OK;
+}
+
 }  // namespace
 
 int mttkrp_tc_query(int order, const long *dims, int mode, long R, int precision, size_t *ws_bytes) {
     TcPlan p;
     if (!tc_plan(order, dims, mode, R, precision, p)) return CUD_ERR_UNSUPPORTED;
     if (!encode_fn()) return CUD_ERR_UNSUPPORTED;
-    if (ws_bytes) *ws_bytes = sizeof(float) * (size_t)p.splits * ((R + 3) / 4 * 4) * p.Q + 256;
+    if (ws_bytes) *ws_bytes = 256 + tc_part_bytes(p, R) + tc_pb_bytes(p);
     return CUD_OK;
 }
 
@@ -867,10 +1277,10 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     // A misaligned fastest factor takes the general KR path; the launch shape
     // (stages, splits, shared memory) stays the planned one, so the workspace
     // sized by mttkrp_tc_query still holds.
-    const bool fast = p.fast && ((reinterpret_cast<uintptr_t>(U0) & 15) == 0);
+    const bool fast = p.fast && (p.pb || (reinterpret_cast<uintptr_t>(U0) & 15) == 0);
     CUtensorMap umap;
     memset(&umap, 0, sizeof(umap));
-    if (fast) {
+    if (fast && !p.pb) {
         // the fastest generating factor (rows0 x R, column-major): a box of
         // 32 rows x Rpad columns per stage; columns >= R read as zero
         const long rows0 = (mode == 0) ? dims[1] : dims[0];
@@ -916,7 +1326,26 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     char *w = static_cast<char *>(ws);
     a.error = reinterpret_cast<int *>(w);
     a.part = reinterpret_cast<float *>(w + 256);
+    a.blk = p.blk;
+    a.seg = p.seg;
+    a.pb = reinterpret_cast<const uint8_t *>(w + 256 + tc_part_bytes(p, R));
     CUD_CHECK(cudaMemsetAsync(a.error, 0, sizeof(int), s));
+    if (p.pb) {
+        const long rows0 = (mode == 0) ? dims[1] : dims[0];
+        const long items = p.blk * 4 * p.Rpad;
+        k_pack_b<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(U0, rows0, R, (int)p.Rpad, p.blk, precision,
+                                                                 const_cast<uint8_t *>(a.pb));
+        CUD_CHECK_LAUNCH("mttkrp_pb pack");
+        a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;
+        const unsigned grid = (unsigned)(p.qtiles * p.splits);
+        const size_t smem = pb_smem_bytes((int)p.Rpad, p.nb);
+        int st = (p.ctas_per_sm == 2) ? launch_pb<2>(tmap, a, smem, grid, s) : launch_pb<1>(tmap, a, smem, grid, s);
+        if (st) return st;
+        k_sum_tc_partials<<<(unsigned)((p.Q * a.Rp + 31) / 32), 256, 0, s>>>(a.part, (int)p.splits, p.Q, R,
+                                                                             a.Rp, a.error, out);
+        CUD_CHECK_LAUNCH("mttkrp_tc reduce");
+        return CUD_OK;
+    }
     // two D buffers + nst A stages of 32 columns, rounded to a power of two
     a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;
     unsigned grid = (unsigned)(p.qtiles * p.splits);
