@@ -89,7 +89,6 @@ struct TcArgs {
     int *error;        // device flag
     const uint8_t *pb; // pre-packed B path: blk B tiles (hi, lo) of the fastest generating factor
     long blk;          // stages per constant-row block (rows of the fastest generating factor / 32)
-    int seg;           // pre-packed B path: stages per accumulation segment (even, divides blk)
 };
 
 struct TcCtrl {
@@ -746,6 +745,24 @@ struct PbCtrl {
 
 constexpr size_t PB_CTRL_BYTES = (sizeof(PbCtrl) + 1023) & ~size_t(1023);
 
+// Segmentation of a CTA's stages on the pre-packed B path: a segment ends at
+// the end of every constant-row block, at every SEG-th stage of a block, and
+// at the CTA's last stage, so no segment straddles a block and none is
+// longer than SEG.  step() advances over one stage and tells whether it
+// ends a segment.
+struct SegTrack {
+    uint32_t pos, blk;  // position of the next stage in its block (blk < 2^31)
+    long ended;         // segments ended so far
+    __device__ SegTrack(long st_beg, long blk_) : pos((uint32_t)(st_beg % blk_)), blk((uint32_t)blk_), ended(0) {}
+    __device__ __forceinline__ bool step(long i, long nst) {
+        static_assert((SEG & (SEG - 1)) == 0, "SEG is a power of two");
+        const bool end = (pos == blk - 1) || ((pos & (SEG - 1)) == SEG - 1) || (i == nst - 1);
+        if (++pos == blk) pos = 0;
+        if (end) ended++;
+        return end;
+    }
+};
+
 __host__ __device__ constexpr size_t pb_smem_bytes(int Rpad, int n) {
     return 1024 + PB_CTRL_BYTES + (size_t)n * (X_STAGE_BYTES + 2 * b_tile_bytes(Rpad));
 }
@@ -791,14 +808,9 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
     const long qtile = blockIdx.x % a.qtiles;
     const long z = blockIdx.x / a.qtiles;
     const long q0 = qtile * BQ;
-    const long st_beg = z * a.chunk;  // even: local and global stage parities agree
+    const long st_beg = z * a.chunk;
     const long st_end = min(a.stages, st_beg + a.chunk);
     const long nst = st_end - st_beg;
-    const int seg = a.seg;
-    // segments are aligned to multiples of seg in the global stage index, so
-    // none straddles a constant-row block; the CTA's first may be partial
-    const int sp0 = (int)(st_beg % seg);
-    const long nseg = (sp0 + nst + seg - 1) / seg;
     volatile int *abort = &sm.abort;
 
     if (threadIdx.x == 0) {
@@ -873,13 +885,13 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
             const uint32_t idesc = ptx::idesc_f16(f16 ? 0u : 1u, BQ, (uint32_t)a.Rpad);
             const uint32_t lbo = (uint32_t)a.Rpad * 16u;
             Ring ar(nb);
-            int sp = sp0;
-            long si = 0;  // segment of the CTA (0 = the first, possibly partial)
+            SegTrack tr(st_beg, a.blk);
+            bool seg_first = true;
             for (long i = 0; i < nst; i++) {
                 const int slot = ar.slot;
                 const long use = ar.use;
+                const long si = tr.ended;  // segment of this stage
                 const int b = (int)(si & 1);
-                const bool seg_first = (sp == 0) || (i == 0);
                 // the segment's D buffer must have been drained (segment si - 2)
                 if (seg_first && si >= 2 &&
                     !ptx::mbar_wait(&sm.d_free[b], (uint32_t)(((si >> 1) - 1) & 1), abort)) break;
@@ -903,12 +915,9 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
                     }
                 }
                 ptx::mma_commit(&sm.empty_a[slot]);
-                if (sp == seg - 1 || i == nst - 1) ptx::mma_commit(&sm.d_full[b]);
+                seg_first = tr.step(i, nst);
+                if (seg_first) ptx::mma_commit(&sm.d_full[b]);
                 ar.next();
-                if (++sp == seg) {
-                    sp = 0;
-                    si++;
-                }
             }
             ptx::mma_commit(&sm.done);
             for (long it = 0; it < 40000 && !ptx::mbar_try_wait_hint(&sm.done, 0, 100000u); it++) {
@@ -966,12 +975,9 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
             if (lane == 0) ptx::mbar_arrive(&sm.d_free[b]);
         };
         Ring xr(nx), ar(nb);
-        int sp = sp0 + grp;
-        long si = 0;
-        if (sp >= seg) {
-            sp -= seg;
-            si = 1;
-        }
+        // the flushing group follows the segmentation of every stage
+        SegTrack tr(st_beg, a.blk);
+        long tracked = 0;  // stages the tracker has passed
         if (grp) {
             xr.next();
             ar.next();
@@ -1012,28 +1018,34 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
             ptx::tc_fence_before();
             __syncwarp();
             if (lane == 0) ptx::mbar_arrive(&sm.full_a[slot]);
-            // a segment just ended (global stage index = seg - 1 mod seg, odd,
-            // so always this group's): drain the one before it
-            if (grp == FLUSH_GRP && sp == seg - 1 && si >= 1) flush(flushed++);
-            sp += GROUPS;
-            if (sp >= seg) {
-                sp -= seg;
-                si++;
+            // drain every segment whose successor has ended by now: its MMAs
+            // were all issued, and the issuer waits for this drain before it
+            // reuses the buffer two segments on
+            if (grp == FLUSH_GRP) {
+                for (; tracked <= i; tracked++) tr.step(tracked, nst);
+                while (flushed + 1 < tr.ended) flush(flushed++);
             }
         }
-        if (grp == FLUSH_GRP)
-            while (flushed < nseg) flush(flushed++);
+        if (grp == FLUSH_GRP) {
+            for (; tracked < nst; tracked++) tr.step(tracked, nst);
+            while (flushed < tr.ended) flush(flushed++);
+        }
     } else {
         // ------------------------------------------------------------ constant rows
-        const long sbase = st_beg - sp0;  // global first stage of the CTA's first segment
-        for (long sg = 0; sg < nseg; sg++) {
-            const int b = (int)(sg & 1);
-            // buffer b's previous segment (sg - 2) must have been flushed
-            if (sg >= 2 && !*abort) ptx::mbar_wait(&sm.d_free[b], (uint32_t)(((sg >> 1) - 1) & 1), abort);
-            const long g0 = (sg == 0) ? st_beg : sbase + sg * seg;
-            for (int r = lane; r < a.Rpad; r += 32) sm.cvec[b][r] = (r < a.R) ? kr_const_row(a, sm, g0, r) : 0.f;
-            __syncwarp();
-            if (lane == 0) ptx::mbar_arrive(&sm.c_full[b]);
+        SegTrack tr(st_beg, a.blk);
+        bool seg_first = true;
+        for (long i = 0; i < nst; i++) {
+            if (seg_first) {
+                const long sg = tr.ended;
+                const int b = (int)(sg & 1);
+                // buffer b's previous segment (sg - 2) must have been drained
+                if (sg >= 2 && !*abort) ptx::mbar_wait(&sm.d_free[b], (uint32_t)(((sg >> 1) - 1) & 1), abort);
+                for (int r = lane; r < a.Rpad; r += 32)
+                    sm.cvec[b][r] = (r < a.R) ? kr_const_row(a, sm, st_beg + i, r) : 0.f;
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(&sm.c_full[b]);
+            }
+            seg_first = tr.step(i, nst);
         }
     }
 
@@ -1105,13 +1117,11 @@ struct TcPlan {
     int nx, nb, ctas_per_sm;
     bool pb;    // pre-packed B path
     long blk;   // stages per constant-row block (fast path)
-    int seg;    // pre-packed B path: segment length
 };
 
 // Pre-packed B path launch shape: the deepest rings (X and A/B equal, at
 // most PB_RING) whose shared memory and TMEM fit two CTAs per SM, else one
-// CTA; contraction splits of an even number of stages (so local and global
-// stage parities agree) filling one wave.
+// CTA; contraction splits filling one wave.
 void pb_shape(TcPlan &p) {
     constexpr size_t kTwoCtaSmem = 115712;
     constexpr size_t kOneCtaSmem = 232448;
@@ -1129,7 +1139,6 @@ void pb_shape(TcPlan &p) {
     long want = std::max(1L, (p.ctas_per_sm * (long)kNumSMs - 2) / p.qtiles);
     p.splits = std::min(want, p.stages);
     p.chunk = (p.stages + p.splits - 1) / p.splits;
-    p.chunk += p.chunk & 1;
     p.splits = (p.stages + p.chunk - 1) / p.chunk;
 }
 
@@ -1182,15 +1191,9 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     const long rows0 = (mode == 0) ? dims[1] : dims[0];
     p.fast = (rows0 % BKS == 0);
     p.blk = p.fast ? rows0 / BKS : 1;
-    // pre-packed B path: a segment length that is even, at least 4 (each
-    // flush adds a whole 128 x R partial tile) and divides the block
-    p.seg = 0;
-    for (int sl = 16; sl >= 4 && p.fast; sl -= 2)
-        if (p.blk % sl == 0) {
-            p.seg = sl;
-            break;
-        }
-    p.pb = p.seg > 0;
+    // pre-packed B path: blocks of at least 2 stages (each segment flush
+    // adds a whole 128 x R partial tile, at least every other stage)
+    p.pb = p.fast && p.blk >= 2;
 #ifdef CUD_TC_NO_PB
     p.pb = false;
 #endif
@@ -1327,7 +1330,6 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     a.error = reinterpret_cast<int *>(w);
     a.part = reinterpret_cast<float *>(w + 256);
     a.blk = p.blk;
-    a.seg = p.seg;
     a.pb = reinterpret_cast<const uint8_t *>(w + 256 + tc_part_bytes(p, R));
     CUD_CHECK(cudaMemsetAsync(a.error, 0, sizeof(int), s));
     if (p.pb) {
