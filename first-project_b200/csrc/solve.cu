@@ -247,167 +247,235 @@ __global__ void __launch_bounds__(256) k_fit(FitArgs a) {
     }
 }
 
-// Fused factor update:  U = M * Vinv (FP64 accumulation; skipped when Vinv
-// is null, then U = M), G = U^T U, and optionally the fit.  Each CTA owns a
-// contiguous block of rows, walks it 16 rows at a time (the rows staged in
-// shared memory as doubles), keeps its share of the R x R Gram in
-// registers, and writes one partial Gram (+ its part of <M, U>).  The last
-// CTA to finish (atomic ticket) sums the partials in CTA order --
-// deterministic -- writes G, resets the ticket and, if asked, the fit.
+// Factor update in two passes, wide enough to occupy the GPU for the small
+// I of CP factors.  Pass 1 (k_update_rows): each CTA takes a contiguous
+// block of rows, 16 at a time staged in shared memory; U = M * Vinv with
+// FP64 accumulation (skipped when Vinv is null: U = M), the CTA's partial
+// Gram sum_i u_i u_i^T (upper triangle, e = q (q + 1) / 2 + p for p <= q)
+// and its part of <M, U>, written as one partial per CTA.  Pass 2
+// (k_update_reduce): one thread per triangle entry sums the partials in CTA
+// order (deterministic), writes G (both halves), and, for the fit, each
+// CTA's share of ||Xhat||^2 = sum_pq prod_m G_m[p, q] (off-diagonal entries
+// twice); the last CTA (atomic ticket) combines those in order and writes
+// the fit.
 constexpr int UPD_RB = 16;
-constexpr int UPD_STAGE_V = 64;  // V^-1 staged in shared memory up to this R
+constexpr int UPD_STAGE_V = 64;    // V^-1 staged in shared memory up to this R
 constexpr int SU_LD = UPD_RB + 1;  // sU column stride (odd: conflict-free Gram reads)
+constexpr int UPD_RED = 256;       // threads of the reduce pass
 
-template <int NT, int NACC>
-__global__ void __launch_bounds__(NT) k_update(UpdateArgs a) {
-    // shared: sU (UPD_RB x R FP64), sM (UPD_RB x R FP32, this chunk of M),
+// (p, q), p <= q, of upper-triangle entry e = q (q + 1) / 2 + p
+__device__ __forceinline__ void tri_pq(long e, int &p, int &q) {
+    q = (int)((sqrt(8.0 * (double)e + 1.0) - 1.0) * 0.5);
+    while ((long)(q + 1) * (q + 2) / 2 <= e) q++;
+    while ((long)q * (q + 1) / 2 > e) q--;
+    p = (int)(e - (long)q * (q + 1) / 2);
+}
+
+template <int NT, int NACC, int UPT>
+__global__ void __launch_bounds__(NT) k_update_rows(UpdateArgs a) {
+    // shared: sU (SU_LD x R FP64), sM (UPD_RB x R FP32, this chunk of M),
     // sV (R x R FP64, V^-1 staged when R <= UPD_STAGE_V)
     extern __shared__ double smem_d[];
-    __shared__ int s_last;
     __shared__ double s_red[NT / 32];
     const int R = a.R;
     const long I = a.I;
-    double *sU = smem_d;  // SU_LD x R
+    double *sU = smem_d;
     float *sM = reinterpret_cast<float *>(sU + SU_LD * R);
     double *sV = sU + SU_LD * R + (UPD_RB * R + 1) / 2;
     const bool stage_v = a.Vinv && R <= UPD_STAGE_V;
     if (stage_v)
         for (int e = threadIdx.x; e < R * R; e += NT) sV[e] = a.Vinv[e];
     const double *V = stage_v ? sV : a.Vinv;
-    const long rpb = (I + gridDim.x - 1) / gridDim.x;
+    const long rpb = ((I + gridDim.x - 1) / gridDim.x + UPD_RB - 1) / UPD_RB * UPD_RB;
     const long r0 = blockIdx.x * rpb, r1 = min(I, r0 + rpb);
+    // U = M V^-1: thread t owns column c = t % R of the rows i = g, g + ng,
+    // ... (g = t / R, ng = NT / R groups; at most UPT rows): independent FMA
+    // chains that share each V^-1 load
+    const int ng = NT / R;
+    const int cu = threadIdx.x % R, gu = threadIdx.x / R;
     double acc[NACC];
 #pragma unroll
     for (int k = 0; k < NACC; k++) acc[k] = 0.0;
-    const int p0 = threadIdx.x % R, q0 = threadIdx.x / R, dp = NT % R, dq = NT / R;
+    int p0, q0;  // this thread's first triangle entry e = tid
+    tri_pq(threadIdx.x, p0, q0);
     double inner = 0.0;
     for (long c0 = r0; c0 < r1; c0 += UPD_RB) {
         const int nr = (int)min((long)UPD_RB, r1 - c0);
-        // this chunk's rows of M, coalesced, then everything from shared memory
         for (int e = threadIdx.x; e < UPD_RB * R; e += NT) {
             const int i = e % UPD_RB, c = e / UPD_RB;
             sM[e] = (i < nr) ? a.M[c0 + i + I * c] : 0.f;
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < UPD_RB * R; e += NT) {
-            const int i = e % UPD_RB, c = e / UPD_RB;
-            double u = 0.0;
-            if (i < nr) {
-                const long gi = c0 + i;
-                if (a.Vinv) {
-                    double s = 0.0;
-                    for (int r = 0; r < R; r++) s = fma((double)sM[i + UPD_RB * r], V[r + R * c], s);
-                    float uf = (float)s;
-                    a.U[gi + I * c] = uf;
-                    u = (double)uf;
-                } else {
-                    u = (double)sM[e];
+        if (a.Vinv) {
+            if (gu < ng) {
+                double u[UPT];
+#pragma unroll
+                for (int k = 0; k < UPT; k++) u[k] = 0.0;
+                for (int r = 0; r < R; r++) {
+                    // V^-1 is symmetric: column cu read along consecutive
+                    // lanes, free of bank conflicts
+                    const double v = V[cu + R * r];
+#pragma unroll
+                    for (int k = 0; k < UPT; k++)
+                        if (gu + k * ng < UPD_RB) u[k] = fma((double)sM[gu + k * ng + UPD_RB * r], v, u[k]);
                 }
-                if (a.fit_out) inner += (double)sM[e] * u;
+#pragma unroll
+                for (int k = 0; k < UPT; k++) {
+                    const int i = gu + k * ng;
+                    if (i < UPD_RB) {
+                        double ud = 0.0;
+                        if (i < nr) {
+                            ud = (double)(float)u[k];
+                            if (a.fit_out) inner += (double)sM[i + UPD_RB * cu] * ud;
+                        }
+                        sU[i + SU_LD * cu] = ud;
+                    }
+                }
             }
-            sU[i + SU_LD * c] = u;
+        } else {
+            for (int e = threadIdx.x; e < UPD_RB * R; e += NT) {
+                const int i = e % UPD_RB, c = e / UPD_RB;
+                const double ud = (i < nr) ? (double)sM[e] : 0.0;
+                if (a.fit_out) inner += (double)sM[e] * ud;
+                sU[i + SU_LD * c] = ud;
+            }
         }
         __syncthreads();
-        // Gram entries e = tid + NT k, (p, q) = (e mod R, e / R) stepped
-        // incrementally (no division per entry)
+        // this chunk's rows of U, coalesced (16 consecutive rows per column)
+        if (a.Vinv)
+            for (int e = threadIdx.x; e < UPD_RB * R; e += NT) {
+                const int i = e % UPD_RB, c = e / UPD_RB;
+                if (i < nr) a.U[c0 + i + I * c] = (float)sU[i + SU_LD * c];
+            }
+        // triangle entries e = tid + NT k, (p, q) stepped incrementally
         {
             int p = p0, q = q0;
 #pragma unroll
             for (int k = 0; k < NACC; k++) {
                 if (q < R) {
-                    double s = acc[k];
+                    double sacc = acc[k];
 #pragma unroll
-                    for (int i = 0; i < UPD_RB; i++) s = fma(sU[i + SU_LD * p], sU[i + SU_LD * q], s);
-                    acc[k] = s;
+                    for (int i = 0; i < UPD_RB; i++) sacc = fma(sU[i + SU_LD * p], sU[i + SU_LD * q], sacc);
+                    acc[k] = sacc;
                 }
-                p += dp;
-                q += dq;
-                if (p >= R) { p -= R; q++; }
+                p += NT;
+                while (p > q && q < R) {
+                    p -= q + 1;
+                    q++;
+                }
             }
         }
         __syncthreads();
     }
-    const long stride = (long)R * R + 1;
+    const int T = R * (R + 1) / 2;
+    const long stride = (long)T + 1;
     double *mine = a.gpart + blockIdx.x * stride;
 #pragma unroll
     for (int k = 0; k < NACC; k++) {
         const int e = threadIdx.x + NT * k;
-        if (e < R * R) mine[e] = acc[k];
+        if (e < T) mine[e] = acc[k];
     }
     for (int o = 16; o > 0; o >>= 1) inner += __shfl_xor_sync(0xffffffffu, inner, o);
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = inner;
-    __threadfence();  // every thread's partial-Gram stores, device-wide
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < NT / 32; w++) t += s_red[w];
-        mine[R * R] = t;
-        __threadfence();
-        unsigned ticket = atomicAdd(a.counter, 1u);
-        s_last = (ticket == gridDim.x - 1);
+        mine[T] = t;
     }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    // last CTA: fixed-order sum of the partials, 8 independent loads in
-    // flight per element (lanes b = j mod 8, combined in a fixed tree)
-    for (long e = threadIdx.x; e < stride; e += NT) {
+}
+
+__global__ void __launch_bounds__(UPD_RED) k_update_reduce(UpdateArgs a, int nparts) {
+    __shared__ double s_red[UPD_RED / 32];
+    __shared__ int s_last;
+    const int R = a.R;
+    const int T = R * (R + 1) / 2;
+    const long stride = (long)T + 1;
+    const long e = blockIdx.x * (long)UPD_RED + threadIdx.x;
+    double *hat_part = a.gpart + (size_t)nparts * stride;  // one per reduce CTA, then <M, U>
+    double hat = 0.0;
+    if (e < stride) {
+        // fixed-order sum of the partials, 8 independent loads in flight
         double p8[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        unsigned b = 0;
-        for (; b + 8 <= gridDim.x; b += 8) {
+        int b = 0;
+        for (; b + 8 <= nparts; b += 8) {
 #pragma unroll
             for (int j = 0; j < 8; j++) p8[j] += __ldcg(a.gpart + (b + j) * stride + e);
         }
 #pragma unroll
-        for (int j = 0; j < 8; j++)  // tail: constant indices keep p8 in registers
-            if (b + j < gridDim.x) p8[j] += __ldcg(a.gpart + (b + j) * stride + e);
-        const double s = ((p8[0] + p8[1]) + (p8[2] + p8[3])) + ((p8[4] + p8[5]) + (p8[6] + p8[7]));
-        if (e < (long)R * R) a.G_out[e] = s;
-        else s_red[0] = s;  // inner product (written by exactly one thread)
+        for (int j = 0; j < 8; j++)
+            if (b + j < nparts) p8[j] += __ldcg(a.gpart + (b + j) * stride + e);
+        const double sum = ((p8[0] + p8[1]) + (p8[2] + p8[3])) + ((p8[4] + p8[5]) + (p8[6] + p8[7]));
+        if (e < T) {
+            int p, q;
+            tri_pq(e, p, q);
+            a.G_out[p + R * q] = sum;
+            a.G_out[q + R * p] = sum;
+            if (a.fit_out) {
+                double pr = 1.0;
+                for (int m = 0; m < a.nG; m++) pr *= (m == a.mode) ? sum : a.Gall[m][p + R * q];
+                hat = (p == q) ? pr : 2.0 * pr;
+            }
+        } else if (a.fit_out) {
+            hat_part[gridDim.x] = sum;  // <M, U>
+        }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) atomicExch(a.counter, 0u);
     if (!a.fit_out) return;
-    const double in = s_red[0];
-    __syncthreads();
-    double hat = 0.0;
-    for (int e = threadIdx.x; e < R * R; e += NT) {
-        double p = 1.0;
-        for (int m = 0; m < a.nG; m++) p *= (m == a.mode) ? __ldcg(a.G_out + e) : a.Gall[m][e];
-        hat += p;
-    }
     for (int o = 16; o > 0; o >>= 1) hat += __shfl_xor_sync(0xffffffffu, hat, o);
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = hat;
     __syncthreads();
     if (threadIdx.x == 0) {
         double h = 0.0;
-        for (int w = 0; w < NT / 32; w++) h += s_red[w];
-        double res2 = a.normx2 - 2.0 * in + h;
-        double fit = 1.0 - sqrt(res2 > 0.0 ? res2 : 0.0) / sqrt(a.normx2);
-        a.fit_out[1] = a.fit_out[0];
-        a.fit_out[0] = fit;
-        a.fit_out[2] = in;
-        a.fit_out[3] = h;
+        for (int w = 0; w < UPD_RED / 32; w++) h += s_red[w];
+        hat_part[blockIdx.x] = h;
+        __threadfence();
+        const unsigned ticket = atomicAdd(a.counter, 1u);
+        s_last = (ticket == gridDim.x - 1);
     }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    double h = 0.0;
+    for (unsigned b = 0; b < gridDim.x; b++) h += __ldcg(hat_part + b);
+    const double in = __ldcg(hat_part + gridDim.x);
+    const double res2 = a.normx2 - 2.0 * in + h;
+    const double fit = 1.0 - sqrt(res2 > 0.0 ? res2 : 0.0) / sqrt(a.normx2);
+    a.fit_out[1] = a.fit_out[0];
+    a.fit_out[0] = fit;
+    a.fit_out[2] = in;
+    a.fit_out[3] = h;
+    atomicExch(a.counter, 0u);
 }
 
 }  // namespace
 
-// At least 64 rows per CTA: the last CTA sums one partial Gram per CTA
-// serially, so fewer, fuller CTAs finish sooner for the I_n of CP factors.
-int update_blocks(long I) { return (int)std::max(1L, std::min((long)kNumSMs, (I + 63) / 64)); }
+// Pass-1 CTAs: 16-row chunks, at most two per SM, and few enough that the
+// partial Grams stay within about 32 MB.
+int update_blocks(long I, long R) {
+    const long byrows = (I + UPD_RB - 1) / UPD_RB;
+    const long cap = std::max(8L, 4000000L / (R * (R + 1) / 2 + 1));
+    return (int)std::max(1L, std::min(std::min(byrows, 2L * kNumSMs), cap));
+}
 
-size_t update_ws_doubles(long I, long R) { return (size_t)update_blocks(I) * (size_t)(R * R + 1); }
+static long update_red_blocks(long R) { return (R * (R + 1) / 2 + 1 + UPD_RED - 1) / UPD_RED; }
+
+size_t update_ws_doubles(long I, long R) {
+    return (size_t)update_blocks(I, R) * (size_t)(R * (R + 1) / 2 + 1) + (size_t)update_red_blocks(R) + 2;
+}
 
 int factor_update(const UpdateArgs &a, cudaStream_t s) {
-    const int nb = update_blocks(a.I);
+    const int nb = update_blocks(a.I, a.R);
     const size_t smem = sizeof(double) * SU_LD * a.R + sizeof(float) * (UPD_RB * a.R + 2) +
                         (a.R <= UPD_STAGE_V ? sizeof(double) * a.R * a.R : 0);
-    if (a.R <= 32) k_update<256, 4><<<nb, 256, smem, s>>>(a);
-    else if (a.R <= 64) k_update<256, 16><<<nb, 256, smem, s>>>(a);
-    else if (a.R <= 160) k_update<512, 50><<<nb, 512, smem, s>>>(a);
+    // NACC = ceil(R (R + 1) / 2 / NT) triangle entries per thread and
+    // UPT = ceil(16 / (NT / R)) rows per thread of U = M V^-1, at the largest R
+    if (a.R <= 32) k_update_rows<256, 3, 2><<<nb, 256, smem, s>>>(a);
+    else if (a.R <= 64) k_update_rows<256, 9, 4><<<nb, 256, smem, s>>>(a);
+    else if (a.R <= 160) k_update_rows<512, 26, 6><<<nb, 512, smem, s>>>(a);
     else return CUD_ERR_UNSUPPORTED;
-    CUD_CHECK_LAUNCH("factor_update");
+    CUD_CHECK_LAUNCH("factor_update rows");
+    k_update_reduce<<<(unsigned)update_red_blocks(a.R), UPD_RED, 0, s>>>(a, nb);
+    CUD_CHECK_LAUNCH("factor_update reduce");
     return CUD_OK;
 }
 
