@@ -772,9 +772,10 @@ __host__ __device__ constexpr size_t pb_smem_bytes(int Rpad, int n) {
 // One thread per (tile, 8-row chunk kc, column r); consecutive threads write
 // consecutive 16-byte chunks.
 __global__ void __launch_bounds__(256) k_pack_b(const float *__restrict__ U0, long rows0, long R, int Rpad,
-                                                long blk, int prec, uint8_t *__restrict__ pb) {
+                                                long blk, int prec, uint8_t *__restrict__ pb, int *error) {
     const long n = blk * 4 * Rpad;
     const long id = blockIdx.x * 256L + threadIdx.x;
+    if (id == 0) *error = 0;
     if (id >= n) return;
     const long t = id / (4 * Rpad);
     const int rem = (int)(id - t * 4 * Rpad);
@@ -1331,12 +1332,12 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     a.part = reinterpret_cast<float *>(w + 256);
     a.blk = p.blk;
     a.pb = reinterpret_cast<const uint8_t *>(w + 256 + tc_part_bytes(p, R));
-    CUD_CHECK(cudaMemsetAsync(a.error, 0, sizeof(int), s));
     if (p.pb) {
+        // the pack kernel also clears the error flag (no separate memset)
         const long rows0 = (mode == 0) ? dims[1] : dims[0];
         const long items = p.blk * 4 * p.Rpad;
         k_pack_b<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(U0, rows0, R, (int)p.Rpad, p.blk, precision,
-                                                                 const_cast<uint8_t *>(a.pb));
+                                                                 const_cast<uint8_t *>(a.pb), a.error);
         CUD_CHECK_LAUNCH("mttkrp_pb pack");
         a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;
         const unsigned grid = (unsigned)(p.qtiles * p.splits);
@@ -1348,6 +1349,7 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
         CUD_CHECK_LAUNCH("mttkrp_tc reduce");
         return CUD_OK;
     }
+    CUD_CHECK(cudaMemsetAsync(a.error, 0, sizeof(int), s));
     // two D buffers + nst A stages of 32 columns, rounded to a power of two
     a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;
     unsigned grid = (unsigned)(p.qtiles * p.splits);
