@@ -3,31 +3,31 @@
 // Around mode n the FP32 tensor is a (P, Q, S) array; the result is
 // M[q, r] = sum_kappa X(q, kappa) * KR(kappa, r), with kappa running over the
 // other modes.  Per CTA: one tile of 128 rows q (the MMA's M) and a
-// contiguous range of 32-deep contraction stages, pipelined 3-4 deep between
-// four warp roles:
-//   * warp 0 (TMA): the 128 x 32 FP32 tile of X, in its native layout, into
+// contiguous range of 32-deep contraction stages, pipelined 3-6 deep between
+// warp roles:
+//   * a TMA warp: the 128 x 32 FP32 tile of X, in its native layout, into
 //     shared memory (mode 0: rows contiguous, a 2-D box over (q, s); other
 //     modes: kappa contiguous, a 3-D box over (p, q, s) with 128-byte
 //     swizzle);
-//   * warps 2-5 (A converters): each thread reads its row (= its TMEM lane),
-//     splits every value into BF16 hi + lo (x = hi + lo + O(2^-16 x)) and
-//     stores both into tensor memory as the MMA's A operand -- X crosses
-//     shared memory once;
-//   * warps 6-7 (KR producers): the stage's 32 Khatri-Rao rows.  The stage's
-//     kappa run over 32 consecutive rows of the fastest generating factor
-//     while the other factors contribute one constant row, so the TMA warp
-//     brings those 32 rows x R of the factor into shared memory with the X
-//     tile, and each producer thread reads two 128-bit vectors of one column,
-//     scales them by the constant row (recomputed once per block of stages),
-//     splits and stores 16 bytes per operand into the K-major canonical B
-//     layout (general factor shapes: computed from global memory);
-//   * warp 1 (MMA): tcgen05.mma kind::f16, FP32 accumulation in TMEM:
+//   * eight A-converter warps in two stage-parity groups (one warp per TMEM
+//     lane quarter each): a thread reads its row (= its TMEM lane), splits
+//     every value into BF16 hi + lo (x = hi + lo + O(2^-16 x)) and stores
+//     both into tensor memory as the MMA's A operand -- X crosses shared
+//     memory once;
+//   * the B operand (the stage's 32 Khatri-Rao rows), two ways.  The stage's
+//     kappa run over 32 consecutive rows of the fastest generating factor U0
+//     while the other factors contribute one constant row c.  Pre-packed B
+//     path (k_mttkrp_pb): c is applied per accumulation segment at the flush,
+//     so B is U0's unscaled rows, packed once per call into the MMA's layout
+//     and bulk-copied per stage.  Khatri-Rao path (k_mttkrp_tc, the other
+//     shapes): Khatri-Rao warps and the converters build B each stage;
+//   * an MMA warp: tcgen05.mma kind::f16, FP32 accumulation in TMEM:
 //     D += Xhi*KRhi + Xhi*KRlo + Xlo*KRhi  (BF16X3), or one product (BF16,
 //     FP16).
 // The tensor core's FP32 accumulation truncates, so long accumulation chains
-// drift low; the CTA's stage range is therefore cut into segments of SEG
-// stages, each accumulated in its own TMEM buffer (two, alternating), and
-// the A converters add each finished segment into the CTA's FP32 partial in
+// drift low; the CTA's stage range is therefore cut into segments of at most
+// SEG stages, each accumulated in its own TMEM buffer (two, alternating), and
+// the converters add each finished segment into the CTA's FP32 partial in
 // global memory with round-to-nearest reductions (`red.add`, fire and
 // forget; each partial element has one owning thread, so the order of the
 // adds is fixed and the result deterministic).  A small second kernel sums the
@@ -36,7 +36,7 @@
 //
 // Every wait is bounded: an expired wait raises a CTA-wide abort flag, the
 // roles drain and the TMEM is freed before the CTA exits, and the kernel's
-// error flag is set.
+// error flag is set (the reduce then writes NaN).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
