@@ -56,7 +56,8 @@ int gemm_tc_bf16(const __nv_bfloat16 *A, long lda, const __nv_bfloat16 *B, long 
 // iteration (subspace.cu): U (n x r, FP32) in ascending eigenvalue order;
 // CUD_ERR_NOT_CONVERGED if it did not settle within max_iters.
 size_t subspace_ws_doubles(long n, long r);
-int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, int max_iters, cudaStream_t s);
+int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, size_t ws_doubles, int max_iters,
+                         cudaStream_t s);
 
 // ||X - [[U]]||^2 and ||X||^2 into out2[0..1] (device, FP64), one pass
 // over X (residual.cu); ws holds cp_residual_ws_bytes.

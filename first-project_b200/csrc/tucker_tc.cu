@@ -108,7 +108,46 @@ __global__ void k_to_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict
 unsigned gfor(long n) { return (unsigned)std::min<long>((n + 255) / 256, 16L * kNumSMs); }
 
 // X viewed as (P, Q, S) -> X_(view) rows of Q, the rest contiguous (BF16).
+// Same unfolding for P a multiple of 8, in the source's memory order: item
+// (u, c) = 8 consecutive floats c of source row u = q + Q s (two 16-byte
+// loads, coalesced), written as 8 BF16 hi (and lo) values to row q, column
+// block s of the unfolding (one 16-byte store each).  32-bit index
+// arithmetic (the caller checks that the item count fits).
+__global__ void __launch_bounds__(256) k_unfold_runs8(const float *__restrict__ X, unsigned P8, unsigned Q,
+                                                      unsigned S, unsigned items, __nv_bfloat16 *hi,
+                                                      __nv_bfloat16 *lo) {
+    const unsigned long P = 8ul * P8;
+    for (unsigned it = blockIdx.x * 256u + threadIdx.x; it < items; it += gridDim.x * 256u) {
+        const unsigned u = it / P8, c = it - u * P8;
+        const unsigned sidx = u / Q, q = u - sidx * Q;
+        const float4 *src = reinterpret_cast<const float4 *>(X + (unsigned long)u * P + 8ul * c);
+        const float4 a = __ldcs(src), b = __ldcs(src + 1);
+        const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const __nv_bfloat162 hh = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+            const float2 hf = __bfloat1622float2(hh);
+            const __nv_bfloat162 ll = __floats2bfloat162_rn(v[2 * j] - hf.x, v[2 * j + 1] - hf.y);
+            h[j] = *reinterpret_cast<const uint32_t *>(&hh);
+            l[j] = *reinterpret_cast<const uint32_t *>(&ll);
+        }
+        const unsigned long o = (unsigned long)q * P * S + (unsigned long)sidx * P + 8ul * c;
+        *reinterpret_cast<uint4 *>(hi + o) = make_uint4(h[0], h[1], h[2], h[3]);
+        if (lo) *reinterpret_cast<uint4 *>(lo + o) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+}
+
 int unfold_bf16(const float *X, long P, long Q, long S, __nv_bfloat16 *hi, __nv_bfloat16 *lo, cudaStream_t s) {
+    const long items = P / 8 * Q * S;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(hi) |
+                           reinterpret_cast<uintptr_t>(lo)) & 15) == 0;
+    if (P > 1 && P % 8 == 0 && aligned && items < 0xffffffffL && Q < 0xffffffffL && S < 0xffffffffL) {
+        const unsigned grid = (unsigned)std::min<long>((items + 255) / 256, 16L * kNumSMs);
+        k_unfold_runs8<<<grid, 256, 0, s>>>(X, (unsigned)(P / 8), (unsigned)Q, (unsigned)S, (unsigned)items, hi, lo);
+        CUD_CHECK_LAUNCH("unfold_bf16");
+        return CUD_OK;
+    }
     if (P == 1) {
         const long tiles = ((Q + 31) / 32) * ((S + 31) / 32);
         k_unfold_t<<<(unsigned)std::min<long>(tiles, 16L * kNumSMs), 256, 0, s>>>(X, Q, S, hi, lo);
@@ -211,7 +250,7 @@ int gram_tc(const TcWork &w, long I, long K, bool use_lo, cudaStream_t s) {
 // eigenvalue), else the full FP64 Jacobi eigensolver.
 int top_vectors(const TcWork &w, long I, long r, float *U, cudaStream_t s) {
     if (subspace_ws_doubles(I, r) <= (size_t)I * I) {
-        const int sst = top_eigvecs_subspace(w.g64, I, r, U, w.V, 300, s);
+        const int sst = top_eigvecs_subspace(w.g64, I, r, U, w.V, (size_t)I * I, 300, s);
         if (sst == CUD_OK) return CUD_OK;
         if (sst != CUD_ERR_NOT_CONVERGED && sst != CUD_ERR_UNSUPPORTED) return sst;
     }
