@@ -358,19 +358,20 @@ def leg_batched(cd, torch, stream, sptr, n=4096):
 
 def leg_warmstart(cd, torch, n_train, n_eval):
     """Learned warm start: 64^3 rank-8 smooth-factor tensors, network trained
-    on n_train ALS solutions the library generates (fresh tensors), then
-    sweeps and time to each tensor's reference fit - 1e-4 from HOSVD, learned
-    and judged (better of the two after one sweep) starts on n_eval held-out
-    tensors."""
+    on n_train ALS solutions the library generates (fresh tensors, 10 epochs
+    over them), then sweeps and time to each tensor's reference fit - 1e-4
+    from random, HOSVD, learned and judged (better of HOSVD and learned after
+    one sweep) starts on n_eval held-out tensors."""
     import warmstart
     w = warmstart.WarmStart(I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    losses = w.train(n_train, batch=256, lr=1e-3, chunk=4096, label_sweeps=3, log_every=64)
+    losses = w.train(n_train, batch=256, lr=3e-4, chunk=4096, label_sweeps=3, log_every=64, epochs=10,
+                     warmup=400)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     ev = w.evaluate(n_eval, id0=10 ** 9)
-    ev["train"] = {"samples": n_train, "seconds": round(train_s, 2),
+    ev["train"] = {"samples": n_train, "epochs": 10, "seconds": round(train_s, 2),
                    "loss_first": round(losses[0][1], 6) if losses else None,
                    "loss_last": round(losses[-1][1], 6) if losses else None}
     w.model.close()

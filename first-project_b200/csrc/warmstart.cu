@@ -693,11 +693,15 @@ extern "C" int cud_ws_model_create(int in_dim, int hidden, int out_dim, int max_
         delete m;
         return set_status(CUD_ERR_INVALID_ARGUMENT);
     }
-    // He-uniform weights (fan-in), zero biases
+    // He-uniform hidden weights (fan-in), zero biases, and a zero output
+    // layer: the network starts at the zero prediction and its first
+    // gradients into the hidden layers are small.  (He-initialised output
+    // weights made the first Adam steps drive nearly all of the second
+    // layer's ReLUs dead, leaving a constant predictor.)
     const float b1 = sqrtf(6.f / (float)D), b2 = sqrtf(6.f / (float)H);
     k_ws_init_uniform<<<grid_for(H * D), 256>>>(m->P[0], H * D, b1, seed);
     k_ws_init_uniform<<<grid_for(H * H), 256>>>(m->P[2], H * H, b2, seed + 1);
-    k_ws_init_uniform<<<grid_for(O * H), 256>>>(m->P[4], O * H, b2, seed + 2);
+    cudaMemsetAsync(m->P[4], 0, sizeof(float) * (size_t)O * H, 0);  // checked by the synchronise below
     int st = ws_refresh_bf16(m, nullptr);
     if (st == CUD_OK && cudaDeviceSynchronize() != cudaSuccess) st = CUD_ERR_CUDA;
     if (st) {

@@ -147,11 +147,35 @@ class WarmStart:
         return T.view(b.n, self.out_dim)
 
     # ---------------------------------------------------------------- training
-    def train(self, n_train, batch=256, lr=1e-3, chunk=2048, label_sweeps=3, id0=0, log_every=0):
-        """One pass over n_train freshly generated tensors (ids id0..): per
-        chunk, generate, label by ALS, then one Adam step per minibatch."""
+    def train(self, n_train, batch=256, lr=1e-3, chunk=2048, label_sweeps=3, id0=0, log_every=0,
+              epochs=1, lr_final=None, shuffle_seed=0, warmup=0):
+        """Trains on n_train freshly generated tensors (ids id0..): per chunk,
+        generate, label by ALS, then one Adam step per minibatch; with
+        epochs > 1 the minibatches (features and targets) stay on the device
+        and are replayed epochs - 1 more times in a seeded shuffled order.
+        The learning rate rises linearly over the first `warmup` steps, then
+        decays from lr to lr_final (default lr / 20) on a cosine over all
+        steps."""
+        import math
+        lr_final = lr / 20 if lr_final is None else lr_final
+        steps_total = epochs * (n_train // batch)
         losses = []
         step = 0
+        keep = [] if epochs > 1 else None
+
+        def rate():
+            t = min(1.0, step / max(1, steps_total - 1))
+            r = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * t))
+            return r * min(1.0, (step + 1) / warmup) if warmup else r
+
+        def one(inp, inp_t, tgt):
+            nonlocal step
+            want = log_every and step % log_every == 0
+            loss = self.model.train_step(inp, inp_t, tgt, rate(), want_loss=bool(want))
+            if want:
+                losses.append((step, loss))
+            step += 1
+
         for c0 in range(0, n_train, chunk):
             n = min(chunk, n_train - c0)
             n -= n % batch
@@ -167,11 +191,15 @@ class WarmStart:
             T = self.targets(b, xn_all, label_sweeps)
             for k, t0 in enumerate(range(0, n, batch)):
                 inp, inp_t = feats[k]
-                want = log_every and step % log_every == 0
-                loss = self.model.train_step(inp, inp_t, T[t0:t0 + batch].contiguous(), lr, want_loss=bool(want))
-                if want:
-                    losses.append((step, loss))
-                step += 1
+                tgt = T[t0:t0 + batch].contiguous()
+                one(inp, inp_t, tgt)
+                if keep is not None:
+                    keep.append((inp, inp_t, tgt))
+            del b
+        rng = np.random.default_rng(shuffle_seed)
+        for _ in range(1, epochs):
+            for k in rng.permutation(len(keep)):
+                one(*keep[k])
         return losses
 
     # ---------------------------------------------------------------- evaluation
@@ -190,6 +218,12 @@ class WarmStart:
     def hosvd_init(self, b):
         cd._check(_lib.cud_ws_hosvd_init(_p(b.X), b.n, self.I, self.R, _p(b.U), None), "ws_hosvd_init")
 
+    def random_init(self, b, seed=77):
+        """Seeded standard-normal factors (the plain random start)."""
+        g = torch.Generator(device="cuda").manual_seed(seed)
+        n = b.n * 3 * self.I * self.R
+        b.U[:n].copy_(torch.randn(n, device="cuda", generator=g))
+
     def judged_init(self, b):
         """Learned factors, judged against HOSVD: one ALS sweep from each, and
         each tensor keeps the start with the better fit (its factors after
@@ -207,16 +241,16 @@ class WarmStart:
         return float(keep_h.float().mean().item())
 
     def evaluate(self, n_eval, id0, margin=1e-4, max_sweeps=200, ref_sweeps=200):
-        """Sweeps and time for HOSVD-init and learned-init ALS to reach, per
-        tensor, the fit of a long ALS run from the generating factors minus
-        `margin`.  Times include the initialisation (Grams + eigensolves, or
-        sketches + network) and the ALS; the device work is timed with CUDA
-        events."""
+        """Sweeps and time for random-, HOSVD-, learned- and judged-init ALS
+        to reach, per tensor, the fit of a long ALS run from the generating
+        factors minus `margin`.  Times include the initialisation (Grams +
+        eigensolves, or sketches + network) and the ALS; the device work is
+        timed with CUDA events."""
         b, _ = self.batch(n_eval, id0)
         ref_fits, _, _ = cd.cp_als_batched(b, max_sweeps=ref_sweeps, tol=1e-9)
         targets = [f - margin for f in ref_fits]
         out = {"n": n_eval, "margin": margin, "reference_fit_mean": float(np.mean(ref_fits))}
-        for name, init in (("hosvd", self.hosvd_init), ("learned", self.learned_init),
+        for name, init in (("random", self.random_init), ("hosvd", self.hosvd_init), ("learned", self.learned_init),
                            ("judged", self.judged_init)):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -130,8 +130,38 @@ def test_mlp_gradients_match_oracle(cd, ws):
 
 
 def test_training_reduces_loss(cd, ws):
+    """The network starts at the zero prediction (zero output layer); eight
+    epochs over 4096 tensors must take the loss well below it, with the
+    hidden units alive (the predictions depend on the input)."""
     w = ws.WarmStart(I=16, R=4, S=8, hidden=128, seed=21, max_batch=64)
-    losses = w.train(4096, batch=64, lr=1e-3, chunk=1024, label_sweeps=2, log_every=8)
-    first = np.mean([l for _, l in losses[:4]])
-    last = np.mean([l for _, l in losses[-4:]])
-    assert np.isfinite(last) and last < 0.8 * first
+    losses = w.train(4096, batch=64, lr=1e-3, chunk=1024, label_sweeps=2, log_every=8, epochs=8, warmup=20)
+    first = np.mean([l for _, l in losses[:2]])
+    last = np.mean([l for _, l in losses[-8:]])
+    assert np.isfinite(last) and last < 0.8 * first, (first, last)
+    b, _ = w.batch(64, id0=10 ** 6)
+    inp, _, _ = w.features(b.X, 0, 64)
+    Y = torch.empty((64, w.out_dim), device="cuda")
+    w.model.predict(inp, Y)
+    assert float(Y.std(0).mean()) > 1e-3
+
+
+def test_trained_network_beats_random_start(cd, ws):
+    """What the trained network gains: on held-out tensors of the 64^3
+    rank-8 smooth-factor workload, ALS from its predicted factors reaches each
+    tensor's target fit (a long ALS run from the generating factors, minus
+    1e-4) in fewer sweeps, and more often within the sweep limit, than ALS
+    from a random start.  (Against the HOSVD start it does not gain on this
+    workload; the judged start keeps HOSVD as the fallback.)"""
+    w = ws.WarmStart(I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256)
+    w.train(102400, batch=256, lr=3e-4, chunk=4096, label_sweeps=3, epochs=10, warmup=400)
+    b, _ = w.batch(1024, id0=10 ** 9)
+    ref, _, _ = cd.cp_als_batched(b, max_sweeps=200, tol=1e-9)
+    targets = [f - 1e-4 for f in ref]
+    res = {}
+    for name, init in (("random", w.random_init), ("learned", w.learned_init)):
+        init(b)
+        fits, sweeps, _ = cd.cp_als_batched_target(b, targets, max_sweeps=200)
+        res[name] = (float(np.mean(sweeps)), float(np.mean([f >= t for f, t in zip(fits, targets)])))
+    w.model.close()
+    assert res["learned"][0] < res["random"][0] - 5, res
+    assert res["learned"][1] > res["random"][1], res
