@@ -34,6 +34,15 @@ namespace {
 
 constexpr int BMAXD = 96;    // largest mode size handled (smem sizing)
 constexpr int BMAXR = 16;    // largest rank handled
+constexpr int BSPLIT = 4;    // most thread groups splitting one contraction
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 struct TensorMeta {
     long xoff;          // offset of X (elements) in the packed tensor buffer
@@ -64,9 +73,9 @@ struct BatchArgs {
 // shared memory layout (floats / doubles), sized for BMAXD x BMAXR
 struct BatchSmem {
     float F[3][BMAXD * BMAXR];       // factors, column-major I_m x R
-    float slice[BMAXD * (BMAXD + 1)];// one frontal slice, row stride I + 1
+    float slice[2][BMAXD * (BMAXD + 1)];  // two frontal slices (double buffer), row stride I + 1
     float M[BMAXD * BMAXR];          // MTTKRP result of the current mode
-    float red3[BMAXR * (BMAXD / 2)]; // mode-3 per-slice partials (rank x row pair)
+    float red3[BSPLIT * BMAXR * (BMAXD / 2)]; // mode-3 per-slice partials (group x rank x row pair)
     double V[BMAXR * BMAXR];         // normal matrix / its inverse
     double rowk[BMAXR], colk[BMAXR];
     double red[32];
@@ -85,7 +94,12 @@ __device__ void load_factors(BatchSmem &sm, const BatchArgs &a, const TensorMeta
 
 // M (I_mode x R) = MTTKRP of mode `mode` with the factors in shared memory.
 // Thread items: (row pair, 4 ranks) with rows = i (mode 1) or j (modes 2, 3);
-// at most (96 / 2) * 4 = 192 items, IPB = ceil(192 / NT) per thread.
+// when the items leave threads idle, S <= BSPLIT groups of threads split the
+// inner contraction (over j, or over i) and their partials are added at the
+// end (modes 1, 2) or per slice (mode 3) in group order.  The frontal slices
+// stream through two shared-memory buffers with cp.async: slice k + 1 loads
+// while slice k is contracted.  (A deeper ring measured slower: the
+// contraction's instruction issue, not the load latency, sets the pace.)
 template <int NT>
 __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
     constexpr int IPB = (BMAXD / 2 * (BMAXR / 4) + NT - 1) / NT;
@@ -97,22 +111,44 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
     const int npair = (rows + 1) / 2;
     const int rq = (R + 3) / 4;
     const int items = npair * rq;
+    const int S = max(1, min(BSPLIT, NT / max(1, items)));
+    const int L = (mode == 0) ? J : I;  // contraction length within a slice
+    // this thread: item it = tid % items' (u = 0 when split), group g
+    const int g = (S > 1) ? (int)threadIdx.x / items : 0;
+    const int l0 = g * L / S, l1 = (g + 1) * L / S;
     float acc[IPB][2][4];
 #pragma unroll
     for (int u = 0; u < IPB; u++)
 #pragma unroll
         for (int c = 0; c < 4; c++) { acc[u][0][c] = 0.f; acc[u][1][c] = 0.f; }
-    for (int k = 0; k < K; k++) {
-        __syncthreads();
+    auto issue = [&](int k) {  // slice k into buffer k & 1, as one cp.async group
         const float *src = X + (long)k * I * J;
+        float *dst = sm.slice[k & 1];
+        int i = threadIdx.x % I, j = threadIdx.x / I;
+        const int di = NT % I, dj = NT / I;
         for (int e = threadIdx.x; e < I * J; e += NT) {
-            const int i = e % I, j = e / I;
-            sm.slice[i + ld * j] = src[e];
+            cp_async4(&dst[i + ld * j], src + e);
+            i += di;
+            j += dj;
+            if (i >= I) { i -= I; j++; }
+        }
+        cp_async_commit();
+    };
+    __syncthreads();  // the previous user of the slice buffers is done
+    issue(0);
+    for (int k = 0; k < K; k++) {
+        if (k + 1 < K) {
+            issue(k + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
+        const float *sl = sm.slice[k & 1];
 #pragma unroll
         for (int u = 0; u < IPB; u++) {
-            const int it = threadIdx.x + NT * u;
+            const int it = (S > 1) ? ((u == 0 && (int)threadIdx.x < S * items) ? (int)threadIdx.x % items : items)
+                                   : (int)threadIdx.x + NT * u;
             if (it >= items) continue;
             const int rp = (it % npair) * 2;
             const int r0 = (it / npair) * 4;
@@ -120,9 +156,9 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
             if (mode == 0) {
                 // T[i, r] = sum_j X[i, j] B[j, r]
                 const float *Bf = sm.F[1];
-                for (int j = 0; j < J; j++) {
-                    const float x0 = sm.slice[rp + ld * j];
-                    const float x1 = (rp + 1 < I) ? sm.slice[rp + 1 + ld * j] : 0.f;
+                for (int j = l0; j < l1; j++) {
+                    const float x0 = sl[rp + ld * j];
+                    const float x1 = (rp + 1 < I) ? sl[rp + 1 + ld * j] : 0.f;
 #pragma unroll
                     for (int c = 0; c < 4; c++) {
                         const int r = r0 + c;
@@ -134,9 +170,9 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
             } else {
                 // T[j, r] = sum_i X[i, j] A[i, r]
                 const float *Af = sm.F[0];
-                for (int i = 0; i < I; i++) {
-                    const float x0 = sm.slice[i + ld * rp];
-                    const float x1 = (rp + 1 < J) ? sm.slice[i + ld * (rp + 1)] : 0.f;
+                for (int i = l0; i < l1; i++) {
+                    const float x0 = sl[i + ld * rp];
+                    const float x1 = (rp + 1 < J) ? sl[i + ld * (rp + 1)] : 0.f;
 #pragma unroll
                     for (int c = 0; c < 4; c++) {
                         const int r = r0 + c;
@@ -156,7 +192,7 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
                     acc[u][1][c] = fmaf(t2[1][c], w, acc[u][1][c]);
                 }
             } else {
-                // this pair's share of M[k, r] = sum_j T[j, r] B[j, r]
+                // this pair's (and group's) share of M[k, r] = sum_j T[j, r] B[j, r]
                 const float *Bf = sm.F[1];
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
@@ -166,35 +202,51 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
                         v = t2[0][c] * Bf[rp + J * r];
                         if (rp + 1 < J) v = fmaf(t2[1][c], Bf[rp + 1 + J * r], v);
                     }
-                    sm.red3[(r0 + c) * (BMAXD / 2) + rp / 2] = v;
+                    sm.red3[(g * BMAXR + r0 + c) * (BMAXD / 2) + rp / 2] = v;
                 }
             }
         }
         if (mode == 2) {
-            // fixed-order sum over the row pairs (deterministic)
+            // sum over groups and row pairs: one warp per rank, lanes over
+            // the pairs, then a fixed shuffle tree (deterministic)
             __syncthreads();
-            for (int r = threadIdx.x; r < R; r += NT) {
+            const int lane = threadIdx.x & 31;
+            for (int r = threadIdx.x >> 5; r < R; r += NT / 32) {
                 float v = 0.f;
-                for (int p2 = 0; p2 < npair; p2++) v += sm.red3[r * (BMAXD / 2) + p2];
-                sm.M[k + K * r] = v;
+                for (int gg = 0; gg < S; gg++)
+                    for (int p2 = lane; p2 < npair; p2 += 32) v += sm.red3[(gg * BMAXR + r) * (BMAXD / 2) + p2];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) sm.M[k + K * r] = v;
             }
         }
+        __syncthreads();  // slice k's buffer is refilled by the next issue
     }
     if (mode < 2) {
+        // groups' partials added in group order through red3 (mode 3 does
+        // not use it now): group 0 writes, the others add in turn
+        for (int gg = 0; gg < S; gg++) {
 #pragma unroll
-        for (int u = 0; u < IPB; u++) {
-            const int it = threadIdx.x + NT * u;
-            if (it >= items) continue;
-            const int rp = (it % npair) * 2;
-            const int r0 = (it / npair) * 4;
+            for (int u = 0; u < IPB; u++) {
+                const int it = (S > 1) ? ((u == 0 && (int)threadIdx.x < S * items) ? (int)threadIdx.x % items : items)
+                                       : (int)threadIdx.x + NT * u;
+                if (it >= items || g != gg) continue;
+                const int rp = (it % npair) * 2;
+                const int r0 = (it / npair) * 4;
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const int r = r0 + c;
-                if (r < R) {
-                    sm.M[rp + Q * r] = acc[u][0][c];
-                    if (rp + 1 < Q) sm.M[rp + 1 + Q * r] = acc[u][1][c];
+                for (int c = 0; c < 4; c++) {
+                    const int r = r0 + c;
+                    if (r < R) {
+                        if (gg == 0) {
+                            sm.M[rp + Q * r] = acc[u][0][c];
+                            if (rp + 1 < Q) sm.M[rp + 1 + Q * r] = acc[u][1][c];
+                        } else {
+                            sm.M[rp + Q * r] += acc[u][0][c];
+                            if (rp + 1 < Q) sm.M[rp + 1 + Q * r] += acc[u][1][c];
+                        }
+                    }
                 }
             }
+            __syncthreads();
         }
     }
     __syncthreads();
