@@ -191,6 +191,185 @@ __global__ void __launch_bounds__(GTHREADS, 1)
     if (warp == 1) ptx::tmem_dealloc(tbase, (uint32_t)BN);
 }
 
+// ---------------------------------------------------------------- skinny N
+// N <= 32 with many rows (the TTM chain's products, N = rank): one CTA per
+// SM loops over 128-row tiles; the whole B (N x K, K <= SK_KMAX) is loaded
+// once into shared memory, A streams through an SK_ST-deep ring, and the
+// accumulators alternate between two TMEM buffers so the epilogue of one
+// tile overlaps the MMAs of the next.
+constexpr int SK_BN = 32;
+constexpr int SK_ST = 8;
+constexpr int SK_KMAX = 1024;
+
+struct SkCtrl {
+    uint64_t full[SK_ST], empty[SK_ST], b_full, d_full[2], d_free[2];
+    uint32_t tmem_base;
+    int abort;
+};
+
+__host__ __device__ constexpr size_t sk_smem_bytes(long kblocks) {
+    return 1024 + GCTRL_BYTES + (size_t)kblocks * SK_BN * GBK * 2 + (size_t)SK_ST * GBM * GBK * 2;
+}
+
+__global__ void __launch_bounds__(GTHREADS, 1)
+    k_gemm_skinny(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g,
+                  long mt) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    SkCtrl &sm = *reinterpret_cast<SkCtrl *>(base);
+    constexpr uint32_t A_BYTES = GBM * GBK * 2;
+    constexpr uint32_t B_BYTES = SK_BN * GBK * 2;
+    const long nkb = g.kblocks;
+    uint8_t *bsm = base + GCTRL_BYTES;                    // nkb B tiles
+    uint8_t *aring = bsm + (size_t)nkb * B_BYTES;          // SK_ST A tiles (1024-aligned: B_BYTES is)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    volatile int *abort = &sm.abort;
+    // this CTA's tiles: t = blockIdx.x + gridDim.x * j
+    const long ntile = (mt - blockIdx.x + gridDim.x - 1) / gridDim.x;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < SK_ST; i++) {
+            ptx::mbar_init(&sm.full[i], 1);
+            ptx::mbar_init(&sm.empty[i], 1);
+        }
+        ptx::mbar_init(&sm.b_full, 1);
+        for (int b = 0; b < 2; b++) {
+            ptx::mbar_init(&sm.d_full[b], 1);
+            ptx::mbar_init(&sm.d_free[b], 4);  // the four epilogue warps
+        }
+        sm.abort = 0;
+        ptx::fence_mbar_init();
+        ptx::prefetch_tmap(&ta);
+        ptx::prefetch_tmap(&tb);
+    }
+    if (warp == 1) {
+        ptx::tmem_alloc(&sm.tmem_base, 2 * SK_BN);
+        ptx::tmem_relinquish();
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tbase = sm.tmem_base;
+
+    long issued = 0;
+    if (warp == 0) {
+        if (lane == 0) {
+            ptx::mbar_arrive_expect_tx(&sm.b_full, (uint32_t)(nkb * B_BYTES));
+            for (long kb = 0; kb < nkb; kb++)
+                ptx::tma_load_2d(bsm + (size_t)kb * B_BYTES, &tb, &sm.b_full, (int)(kb * GBK), 0);
+            long i = 0;  // stage counter over all tiles
+            for (long j = 0; j < ntile && !*abort; j++) {
+                const long m0 = (blockIdx.x + gridDim.x * j) * GBM;
+                for (long kb = 0; kb < nkb && !*abort; kb++, i++) {
+                    const int slot = (int)(i % SK_ST);
+                    const long use = i / SK_ST;
+                    if (use > 0 && !ptx::mbar_wait(&sm.empty[slot], (uint32_t)((use - 1) & 1), abort)) break;
+                    ptx::mbar_arrive_expect_tx(&sm.full[slot], A_BYTES);
+                    ptx::tma_load_2d(aring + (size_t)slot * A_BYTES, &ta, &sm.full[slot], (int)(kb * GBK), (int)m0);
+                    issued = i + 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = ptx::idesc_f16(1u, GBM, (uint32_t)SK_BN);
+            bool ok = ptx::mbar_wait(&sm.b_full, 0u, abort);
+            long i = 0;
+            for (long j = 0; j < ntile && ok; j++) {
+                const int b = (int)(j & 1);
+                // the buffer's previous tile (j - 2) must have been drained
+                if (j >= 2 && !ptx::mbar_wait(&sm.d_free[b], (uint32_t)(((j >> 1) - 1) & 1), abort)) break;
+                const uint32_t d = tbase + (uint32_t)b * SK_BN;
+                for (long kb = 0; kb < nkb; kb++, i++) {
+                    const int slot = (int)(i % SK_ST);
+                    const long use = i / SK_ST;
+                    if (!ptx::mbar_wait(&sm.full[slot], (uint32_t)(use & 1), abort)) { ok = false; break; }
+                    ptx::tc_fence_after();
+                    const uint32_t sa = ptx::smem_addr(aring + (size_t)slot * A_BYTES);
+                    const uint32_t sb = ptx::smem_addr(bsm + (size_t)kb * B_BYTES);
+#pragma unroll
+                    for (int k = 0; k < GBK / 16; k++) {
+                        const uint64_t da = ptx::smem_desc_kmajor_sw128(sa + 32u * k, 1024u);
+                        const uint64_t db = ptx::smem_desc_kmajor_sw128(sb + 32u * k, 1024u);
+                        ptx::mma_ss_f16(d, da, db, idesc, (kb > 0 || k > 0) ? 1u : 0u);
+                    }
+                    ptx::mma_commit(&sm.empty[slot]);
+                }
+                if (!ok) break;
+                ptx::mma_commit(&sm.d_full[b]);
+            }
+        }
+    } else {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
+        const int sub = warp & 3;
+        const uint32_t lane_off = (uint32_t)(sub * 32) << 16;
+        const bool plain = g.e.alpha == 1.f && !g.e.bias && !g.e.mask && !g.e.relu && !g.e.out_bf16_2;
+        const bool simple_bf16 = plain && g.e.out_bf16 && !g.e.out_f32;
+        const bool simple_f32 = plain && g.e.out_f32 && !g.e.f32_accumulate && !g.e.out_bf16;
+        for (long j = 0; j < ntile; j++) {
+            const int b = (int)(j & 1);
+            const long m = (blockIdx.x + gridDim.x * j) * GBM + sub * 32 + lane;
+            bool ok = true;
+            if (!*abort) ok = ptx::mbar_wait(&sm.d_full[b], (uint32_t)((j >> 1) & 1), abort);
+            ok = __all_sync(0xffffffffu, ok && *abort == 0);
+            if (!ok) break;
+            ptx::tc_fence_after();
+            uint32_t v[32];
+            ptx::tmem_ld32(tbase + lane_off + (uint32_t)b * SK_BN, v);
+            ptx::tmem_wait_ld();
+            ptx::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&sm.d_free[b]);  // the values are in registers
+            if (m < g.M) {
+                if (simple_bf16) {
+                    // plain BF16 output: walk the row's outputs by pointer
+                    __nv_bfloat16 *p = static_cast<__nv_bfloat16 *>(g.e.out_bf16) + m * g.e.bf16_ldm;
+                    const long step = g.e.bf16_ldn;
+#pragma unroll
+                    for (int n = 0; n < SK_BN; n++) {
+                        if (n < g.N) *p = __float2bfloat16_rn(__uint_as_float(v[n]));
+                        p += step;
+                    }
+                } else if (simple_f32) {
+                    float *p = g.e.out_f32 + m * g.e.f32_ldm;
+                    const long step = g.e.f32_ldn;
+#pragma unroll
+                    for (int n = 0; n < SK_BN; n++) {
+                        if (n < g.N) *p = __uint_as_float(v[n]);
+                        p += step;
+                    }
+                } else {
+#pragma unroll
+                    for (int n = 0; n < SK_BN; n++)
+                        if (n < g.N) epi_store(g.e, m, n, __uint_as_float(v[n]));
+                }
+            }
+        }
+    }
+
+    // ------------------------------------------------------------ teardown
+    if (threadIdx.x == 0 && *abort) {
+        for (long i = (issued > SK_ST ? issued - SK_ST : 0); i < issued; i++) {
+            const uint32_t par = (uint32_t)((i / SK_ST) & 1);
+            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.full[i % SK_ST], par, 100000u); it++) {
+            }
+        }
+        for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.b_full, 0u, 100000u); it++) {
+        }
+        atomicExch(g.error, 1);
+    }
+    if (threadIdx.x == 32) {
+        // every MMA issued must finish before TMEM is freed (bounded)
+        ptx::mma_commit(&sm.b_full);  // b_full phase 1 completes once the issued MMAs have
+        for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.b_full, 1u, 100000u); it++) {
+        }
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    if (warp == 1) ptx::tmem_dealloc(tbase, 2 * SK_BN);
+}
+
 // Sums the split partials (fixed order) and applies the epilogue.
 __global__ void __launch_bounds__(256) k_gemm_splitk_epi(const float *__restrict__ part, int splits, long M, long N,
                                                           GemmEpi e) {
@@ -247,6 +426,14 @@ GemmPlan gemm_plan(long M, long N, long K) {
     return p;
 }
 
+// The skinny path: N <= 32, K <= SK_KMAX, and at least two tiles per SM.
+bool skinny_ok(long M, long N, long K) {
+#ifdef CUD_GEMM_NO_SKINNY
+    return false;
+#endif
+    return N <= SK_BN && K <= SK_KMAX && (M + GBM - 1) / GBM >= 2 * kNumSMs;
+}
+
 template <int BN>
 int launch_gemm(const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &g, dim3 grid, cudaStream_t s) {
     static bool attr[64] = {false};
@@ -267,7 +454,7 @@ int launch_gemm(const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &g,
 size_t gemm_tc_ws_bytes(long M, long N, long K) {
     GemmPlan p = gemm_plan(M, N, K);
     size_t b = 256;
-    if (p.splits > 1) b += sizeof(float) * (size_t)p.splits * M * N;
+    if (p.splits > 1 && !skinny_ok(M, N, K)) b += sizeof(float) * (size_t)p.splits * M * N;
     return b;
 }
 
@@ -279,6 +466,31 @@ int gemm_tc_bf16(const __nv_bfloat16 *A, long lda, const __nv_bfloat16 *B, long 
     if (M > 0x7fffffffL || N > 0x7fffffffL || K > 0x7fffffffL) return CUD_ERR_UNSUPPORTED;
     GemmPlan p = gemm_plan(M, N, K);
     CUtensorMap ta, tb;
+    if (skinny_ok(M, N, K)) {
+        if (!encode_bf16_kmajor(ta, A, M, K, lda, GBM) || !encode_bf16_kmajor(tb, B, N, K, ldb, SK_BN))
+            return CUD_ERR_UNSUPPORTED;
+        GemmArgs g;
+        g.M = M; g.N = N; g.K = K;
+        g.kblocks = (K + GBK - 1) / GBK;
+        g.kb_per_split = g.kblocks;
+        g.e = e;
+        g.error = reinterpret_cast<int *>(ws);
+        g.part = nullptr;
+        CUD_CHECK(cudaMemsetAsync(g.error, 0, sizeof(int), s));
+        const long mt = (M + GBM - 1) / GBM;
+        const size_t smem = sk_smem_bytes(g.kblocks);
+        static bool attr[64] = {false};
+        int dev = 0;
+        CUD_CHECK(cudaGetDevice(&dev));
+        if (dev >= 0 && dev < 64 && !attr[dev]) {
+            CUD_CHECK(cudaFuncSetAttribute(k_gemm_skinny, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sk_smem_bytes(SK_KMAX / GBK)));
+            attr[dev] = true;
+        }
+        k_gemm_skinny<<<(unsigned)std::min<long>(mt, kNumSMs), GTHREADS, smem, s>>>(ta, tb, g, mt);
+        CUD_CHECK_LAUNCH("gemm_tc skinny");
+        return CUD_OK;
+    }
     if (!encode_bf16_kmajor(ta, A, M, K, lda, GBM) || !encode_bf16_kmajor(tb, B, N, K, ldb, p.BN))
         return CUD_ERR_UNSUPPORTED;
     GemmArgs g;

@@ -51,6 +51,53 @@ __global__ void __launch_bounds__(256) k_unfold_t(const float *__restrict__ X, l
     }
 }
 
+// The same (Q, S) transpose for Q % 4 == 0, S % 8 == 0 and 16-byte aligned
+// buffers: 64 x 64 tiles, 16-byte loads (a warp reads two 256-byte column
+// runs) and 16-byte stores of 8 BF16 values (lane pairs fill 32-byte
+// sectors of 16 output rows).  Row stride 68 keeps the float4 shared stores
+// conflict-free; the column reads are at most 2-way.
+__global__ void __launch_bounds__(256) k_unfold_t64(const float *__restrict__ X, long Q, long S,
+                                                    __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+    __shared__ __align__(16) float tile[64][68];
+    const long tq = (Q + 63) / 64, ts = (S + 63) / 64;
+    const int t = threadIdx.x;
+    for (long tt = blockIdx.x; tt < tq * ts; tt += gridDim.x) {
+        const long q0 = (tt % tq) * 64, s0 = (tt / tq) * 64;
+        const int q4 = (t & 15) * 4;
+        const bool qin = q0 + q4 < Q;
+        float4 v[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int sl = (t >> 4) + 16 * i;
+            v[i] = (qin && s0 + sl < S) ? __ldcs(reinterpret_cast<const float4 *>(X + q0 + q4 + Q * (s0 + sl)))
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; i++) *reinterpret_cast<float4 *>(&tile[(t >> 4) + 16 * i][q4]) = v[i];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int u = t + 256 * i, p = u >> 1;
+            const int ql = p & 63, c = 2 * (p >> 6) + (u & 1);
+            const long q = q0 + ql, sb = s0 + 8 * c;
+            if (q >= Q || sb >= S) continue;
+            uint32_t h[4], l[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float a = tile[8 * c + 2 * j][ql], b = tile[8 * c + 2 * j + 1][ql];
+                const __nv_bfloat162 hh = __floats2bfloat162_rn(a, b);
+                const float2 hf = __bfloat1622float2(hh);
+                const __nv_bfloat162 ll = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+                h[j] = *reinterpret_cast<const uint32_t *>(&hh);
+                l[j] = *reinterpret_cast<const uint32_t *>(&ll);
+            }
+            *reinterpret_cast<uint4 *>(hi + q * S + sb) = make_uint4(h[0], h[1], h[2], h[3]);
+            if (lo) *reinterpret_cast<uint4 *>(lo + q * S + sb) = make_uint4(l[0], l[1], l[2], l[3]);
+        }
+    }
+}
+
 // View X as (P, Q, S), P > 1: out[q*(P*S) + p + P*s] = X[p + P*q + P*Q*s];
 // each (q, s) pair is a run of P contiguous values on both sides.
 __global__ void __launch_bounds__(256) k_unfold_runs(const float *__restrict__ X, long P, long Q, long S,
@@ -148,7 +195,10 @@ int unfold_bf16(const float *X, long P, long Q, long S, __nv_bfloat16 *hi, __nv_
         CUD_CHECK_LAUNCH("unfold_bf16");
         return CUD_OK;
     }
-    if (P == 1) {
+    if (P == 1 && Q % 4 == 0 && S % 8 == 0 && aligned) {
+        const long tiles = ((Q + 63) / 64) * ((S + 63) / 64);
+        k_unfold_t64<<<(unsigned)std::min<long>(tiles, 8L * kNumSMs), 256, 0, s>>>(X, Q, S, hi, lo);
+    } else if (P == 1) {
         const long tiles = ((Q + 31) / 32) * ((S + 31) / 32);
         k_unfold_t<<<(unsigned)std::min<long>(tiles, 16L * kNumSMs), 256, 0, s>>>(X, Q, S, hi, lo);
     } else {

@@ -16,7 +16,9 @@ def ints(shape, lo=-4, hi=5, seed=0):
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (200, 300, 1000), (1000, 64, 6144),
                                    (256, 512, 6144), (64, 1536, 512), (512, 512, 65536),
-                                   (7, 9, 24)])
+                                   (7, 9, 24),
+                                   # skinny N, many rows: the persistent N <= 32 path
+                                   (40000, 16, 128), (38000, 32, 512), (50001, 5, 1000), (45056, 32, 1024)])
 def test_gemm_integer_exact(cd, M, N, K):
     A = ints((M, K), seed=M + K)
     B = ints((N, K), seed=N + 7 * K)
@@ -79,3 +81,16 @@ def test_gemm_rejects_bad_leading_dimension(cd):
     C = torch.empty((16, 16), device="cuda")
     with pytest.raises(cd.CudError):
         cd.gemm_bf16(A, B, out_f32=C)
+
+
+def test_gemm_skinny_epilogue_strided_bf16(cd):
+    """The persistent skinny path with the TTM epilogue: BF16 output with
+    the rank index slowest (column-major C)."""
+    M, N, K = 40960, 16, 256
+    A = ints((M, K), -3, 4, seed=11)
+    B = ints((N, K), -3, 4, seed=12)
+    ref = (A @ B.T).float()
+    Ct = torch.empty((N, M), device="cuda", dtype=torch.bfloat16)
+    cd.gemm_bf16(A.to(torch.bfloat16).cuda(), B.to(torch.bfloat16).cuda(), out_bf16=("T", Ct))
+    torch.cuda.synchronize()
+    assert torch.equal(Ct.cpu().T.float(), ref.to(torch.bfloat16).float())
