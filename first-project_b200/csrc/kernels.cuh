@@ -54,10 +54,13 @@ int gemm_tc_bf16(const __nv_bfloat16 *A, long lda, const __nv_bfloat16 *B, long 
 
 // Top-r eigenvectors of a symmetric PSD FP64 n x n matrix by subspace
 // iteration (subspace.cu): U (n x r, FP32) in ascending eigenvalue order;
-// CUD_ERR_NOT_CONVERGED if it did not settle within max_iters.
+// CUD_ERR_NOT_CONVERGED if it did not settle within max_iters.  With U0
+// (n x r, FP32, may alias U) the iteration starts from U0's columns instead
+// of a random block, and falls back to the random start if they are
+// numerically rank-deficient.
 size_t subspace_ws_doubles(long n, long r);
 int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, size_t ws_doubles, int max_iters,
-                         cudaStream_t s);
+                         cudaStream_t s, const float *U0 = nullptr);
 
 // ||X - [[U]]||^2 and ||X||^2 into out2[0..1] (device, FP64), one pass
 // over X (residual.cu); ws holds cp_residual_ws_bytes.

@@ -37,6 +37,13 @@ __global__ void k_si_init(double *V, long n, int r) {
     }
 }
 
+// V (n x r) = the given FP32 start block.
+__global__ void k_si_init_from(const float *__restrict__ U0, double *V, long n, int r) {
+    const long total = n * r;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x)
+        V[e] = (double)U0[e];
+}
+
 // Y (n x r) = G (n x n) V (n x r), column-major.
 __global__ void __launch_bounds__(256) k_si_apply(const double *__restrict__ G, const double *__restrict__ V,
                                                   long n, int r, double *__restrict__ Y) {
@@ -140,6 +147,8 @@ __global__ void __launch_bounds__(256) k_si_ritz(const double *V, const double *
     }
     __syncthreads();
     const int m = (r + 1) & ~1;
+    // stop at a relative off-diagonal norm of 1e-13: rounding alone keeps it
+    // near r * eps, so a test at eps itself would run every sweep
     for (int sweep = 0; sweep < 40; sweep++) {
         if (threadIdx.x == 0) {
             double off = 0.0, tot = 0.0;
@@ -147,7 +156,7 @@ __global__ void __launch_bounds__(256) k_si_ritz(const double *V, const double *
                 tot += H[e] * H[e];
                 if (e % r != e / r) off += H[e] * H[e];
             }
-            off_s = (off <= 1e-30 * tot) ? -1.0 : off;
+            off_s = (off <= 1e-26 * tot) ? -1.0 : off;
         }
         __syncthreads();
         if (off_s < 0) break;
@@ -446,6 +455,8 @@ __global__ void __launch_bounds__(SI_OT) k_si_ritz_smem(const double *__restrict
     }
     __syncthreads();
     const int m = (r + 1) & ~1;
+    // stop at a relative off-diagonal norm of 1e-13: rounding alone keeps it
+    // near r * eps, so a test at eps itself would run every sweep
     for (int sweep = 0; sweep < 40; sweep++) {
         // off-diagonal and total squared norms, reduced over the block
         {
@@ -470,7 +481,7 @@ __global__ void __launch_bounds__(SI_OT) k_si_ritz_smem(const double *__restrict
                     o2 += cs_red[w];
                     t2 += cs_red[SI_OT / 32 + w];
                 }
-                off_s = (o2 <= 1e-30 * t2) ? -1.0 : o2;
+                off_s = (o2 <= 1e-26 * t2) ? -1.0 : o2;
             }
             __syncthreads();
         }
@@ -542,7 +553,7 @@ size_t subspace_ws_doubles(long n, long r) { return 3 * (size_t)n * r + 8; }  //
 // ws_doubles allows (at most 8).  Each step forms G^2 V (two split
 // products), then orthonormalises and measures the subspace change.
 static int top_eigvecs_fast(const double *G, long n, long r, float *U, double *ws, size_t ws_doubles,
-                            int max_iters, cudaStream_t s) {
+                            int max_iters, cudaStream_t s, const float *U0) {
     const long nr = n * r;
     const long room = ((long)ws_doubles - 2 * nr - 8) / (2 * nr);
     const int nks = (int)std::max(0L, std::min(8L, room));
@@ -567,7 +578,8 @@ static int top_eigvecs_fast(const double *G, long n, long r, float *U, double *w
     const dim3 ga((unsigned)((n + 127) / 128), (unsigned)nks);
     const unsigned gi = (unsigned)std::min<long>((nr + 255) / 256, 4L * kNumSMs);
     CUD_CHECK(cudaMemsetAsync(fail, 0, sizeof(int), s));
-    k_si_init<<<gi, 256, 0, s>>>(Y, n, (int)r);
+    if (U0) k_si_init_from<<<gi, 256, 0, s>>>(U0, Y, n, (int)r);
+    else k_si_init<<<gi, 256, 0, s>>>(Y, n, (int)r);
     k_si_orth<<<1, SI_OT, smem, s>>>(Y, 1, nullptr, n, (int)r, 2, V, scal, fail);
     CUD_CHECK_LAUNCH("subspace init");
     int extra = -1;  // iterations still to run after the tolerance is met
@@ -593,11 +605,10 @@ static int top_eigvecs_fast(const double *G, long n, long r, float *U, double *w
     return CUD_ERR_NOT_CONVERGED;
 }
 
-int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, size_t ws_doubles, int max_iters,
-                         cudaStream_t s) {
-    if (r <= 0 || r > SI_RMAX || r > n) return CUD_ERR_UNSUPPORTED;
+static int subspace_run(const double *G, long n, long r, float *U, double *ws, size_t ws_doubles, int max_iters,
+                        cudaStream_t s, const float *U0) {
     if (r <= SI_FR && n <= 4 * SI_OT && si_fast_smem(n, r) <= 200 * 1024) {
-        const int st = top_eigvecs_fast(G, n, r, U, ws, ws_doubles, max_iters, s);
+        const int st = top_eigvecs_fast(G, n, r, U, ws, ws_doubles, max_iters, s, U0);
         if (st != CUD_ERR_UNSUPPORTED) return st;
     }
     double *V = ws, *Y = ws + n * r, *Wr = ws + 2 * n * r, *scal = ws + 3 * n * r;
@@ -606,7 +617,8 @@ int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, 
     if (!h) return CUD_ERR_NO_MEMORY;
     const unsigned gb = (unsigned)std::min<long>((n * r + 255) / 256, 4L * kNumSMs);
     CUD_CHECK(cudaMemsetAsync(fail, 0, sizeof(int), s));
-    k_si_init<<<gb, 256, 0, s>>>(V, n, (int)r);
+    if (U0) k_si_init_from<<<gb, 256, 0, s>>>(U0, V, n, (int)r);
+    else k_si_init<<<gb, 256, 0, s>>>(V, n, (int)r);
     k_si_cholqr<<<1, 256, 0, s>>>(V, n, (int)r, fail);
     k_si_cholqr<<<1, 256, 0, s>>>(V, n, (int)r, fail);
     CUD_CHECK_LAUNCH("subspace init");
@@ -630,6 +642,18 @@ int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, 
         }
     }
     return CUD_ERR_NOT_CONVERGED;
+}
+
+int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, size_t ws_doubles, int max_iters,
+                         cudaStream_t s, const float *U0) {
+    if (r <= 0 || r > SI_RMAX || r > n) return CUD_ERR_UNSUPPORTED;
+    if (U0) {
+        // U is written only on success: a failed warm start (a rank-
+        // deficient start block) retries from the random block
+        const int st = subspace_run(G, n, r, U, ws, ws_doubles, max_iters, s, U0);
+        if (st != CUD_ERR_NOT_CONVERGED) return st;
+    }
+    return subspace_run(G, n, r, U, ws, ws_doubles, max_iters, s, nullptr);
 }
 
 }  // namespace cud

@@ -103,7 +103,7 @@ int tucker_tc_factors(const float *X, int order, const long *dims, const long *r
 int tucker_tc_core(const float *X, int order, const long *dims, const long *ranks, float *const *U, float *core,
                    bool three, cudaStream_t s);
 int tucker_tc_hooi_sweep(const float *X, int order, const long *dims, const long *ranks, float *const *U,
-                         bool three, cudaStream_t s, int *worst);
+                         bool three, bool u0_set, cudaStream_t s, int *worst);
 
 }  // namespace cud
 
@@ -159,7 +159,7 @@ extern "C" int cud_tucker_hooi(const float *X, int order, const long *dims, cons
         // initial U_2..U_N from the Grams (tucker_hooi.cu:45-75), U_1 too when no sweep runs
         int st = tucker_tc_factors(X, order, dims, ranks, U, sweeps > 0 ? 1 : 0, three, s, &worst);
         for (int it = 0; it < sweeps && st == CUD_OK; it++)
-            st = tucker_tc_hooi_sweep(X, order, dims, ranks, U, three, s, &worst);
+            st = tucker_tc_hooi_sweep(X, order, dims, ranks, U, three, it > 0, s, &worst);
         if (st == CUD_OK) st = tucker_tc_core(X, order, dims, ranks, U, core, three, s);
         if (st) return set_status(st);
         CUD_CHECK(cudaStreamSynchronize(s));

@@ -297,10 +297,11 @@ int gram_tc(const TcWork &w, long I, long K, bool use_lo, cudaStream_t s) {
 
 // U (I x r, FP32) = eigenvectors of the r largest eigenvalues of w.g64:
 // subspace iteration (fast when the Gram has a gap after its r-th
-// eigenvalue), else the full FP64 Jacobi eigensolver.
-int top_vectors(const TcWork &w, long I, long r, float *U, cudaStream_t s) {
+// eigenvalue), else the full FP64 Jacobi eigensolver.  warm: start the
+// subspace iteration from U's current columns.
+int top_vectors(const TcWork &w, long I, long r, float *U, cudaStream_t s, bool warm = false) {
     if (subspace_ws_doubles(I, r) <= (size_t)I * I) {
-        const int sst = top_eigvecs_subspace(w.g64, I, r, U, w.V, (size_t)I * I, 300, s);
+        const int sst = top_eigvecs_subspace(w.g64, I, r, U, w.V, (size_t)I * I, 300, s, warm ? U : nullptr);
         if (sst == CUD_OK) return CUD_OK;
         if (sst != CUD_ERR_NOT_CONVERGED && sst != CUD_ERR_UNSUPPORTED) return sst;
     }
@@ -404,9 +405,11 @@ int tucker_tc_core(const float *X, int order, const long *dims, const long *rank
 }
 
 // One HOOI sweep: for each mode n, U_n = top eigenvectors of the Gram of
-// Y = X x_{m != n} U_m^T.
+// Y = X x_{m != n} U_m^T.  The eigensolver starts from the current U_n (the
+// previous sweep's, or the HOSVD one), which is already close to the new
+// subspace; U_0 is not set before the first sweep (u0_set false).
 int tucker_tc_hooi_sweep(const float *X, int order, const long *dims, const long *ranks, float *const *U,
-                         bool three, cudaStream_t s, int *worst) {
+                         bool three, bool u0_set, cudaStream_t s, int *worst) {
     TcWork w;
     int st = tc_alloc(order, dims, ranks, three, w);
     if (st) return st;
@@ -435,7 +438,7 @@ int tucker_tc_hooi_sweep(const float *X, int order, const long *dims, const long
         k_transpose_bf16<<<(unsigned)std::min<long>(tiles, 16L * kNumSMs), 256, 0, s>>>(Y, dims[n], R, Rp, w.uh);
         CUD_CHECK_LAUNCH("hooi transpose");
         if ((st = gram_tc(w, dims[n], Rp, false, s))) return st;
-        st = top_vectors(w, dims[n], ranks[n], U[n], s);
+        st = top_vectors(w, dims[n], ranks[n], U[n], s, n > 0 || u0_set);
         if (st == CUD_ERR_NOT_CONVERGED) *worst = st;
         else if (st) return st;
     }
