@@ -556,9 +556,18 @@ __device__ __forceinline__ void cl_jacobi(double *Hs, double *Mb, double *Ws, in
 // Y (n x r) = orth(sum of the nks partial slices) by two CholQR passes;
 // with Vold, also scal[0] = r - ||Vold^T Y||_F^2.  *fail = 1 (and Y not
 // written) when a Gram is not numerically positive definite.
+//
+// With st (a step of the iteration), the convergence test runs here, so
+// the host can queue several steps and read the state once: st[0] done
+// (later launches return at once), st[1] the steps still to run after the
+// gap first fell below the tolerance, plus one (0: not yet), st[2] steps
+// taken, st[3] the step whose iterate is final.  The state is read on entry
+// by every CTA and written by CTA 0 only after the cluster's last barrier,
+// so all CTAs of a launch see the same value.
 __global__ void __cluster_dims__(CL_N, 1, 1) __launch_bounds__(CL_T)
     k_si_orth_cl(const double *__restrict__ part, int nks, const double *__restrict__ Vold, long n, int r,
-                 double *__restrict__ Y, double *scal, int *fail) {
+                 double *__restrict__ Y, double *scal, int *fail, int *st) {
+    if (st && st[0]) return;
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double smc[];
     __shared__ double pub[128], dsh[32], wred[CL_T / 32];
@@ -577,7 +586,10 @@ __global__ void __cluster_dims__(CL_N, 1, 1) __launch_bounds__(CL_T)
         cl_sum(cl, rb, r, true, C);
         if (!cl_chol_inv(C, T, r, pub, dsh)) {  // the same verdict in every CTA
             cl.sync();                              // peers may still read this CTA's buffers
-            if (rank == 0 && threadIdx.x == 0) *fail = 1;
+            if (rank == 0 && threadIdx.x == 0) {
+                *fail = 1;
+                if (st) st[0] = 1;
+            }
             return;
         }
         cl_transform(src, T, nl, dst);
@@ -610,6 +622,18 @@ __global__ void __cluster_dims__(CL_N, 1, 1) __launch_bounds__(CL_T)
         Y[(i0 + i) + n * a] = ya[i * CL_RS + a];
     }
     cl.sync();  // keep this CTA's buffers alive until every peer has read them
+    if (st && rank == 0 && threadIdx.x == 0) {
+        // one more step after the gap first falls below the tolerance
+        const int step = st[2] + 1;
+        int extra = st[1] - 1;
+        if (extra < 0 && scal[0] < 1e-13 * (double)r) extra = 1;
+        if (extra >= 0 && extra-- == 0) {
+            st[0] = 1;
+            st[3] = step;
+        }
+        st[1] = extra + 1;
+        st[2] = step;
+    }
 }
 
 // Rayleigh-Ritz: H = V^T (G V) (G V = the sum of the partial slices),
@@ -656,7 +680,8 @@ __global__ void __cluster_dims__(CL_N, 1, 1) __launch_bounds__(CL_T)
 constexpr int AP_KB = 64;  // rows of V staged per pass
 __global__ void __launch_bounds__(256) k_si_apply_cols(const double *__restrict__ G, const double *__restrict__ V,
                                                        int nin, long n, int r, long kchunk,
-                                                       double *__restrict__ part) {
+                                                       double *__restrict__ part, const int *st) {
+    if (st && st[0]) return;  // the iteration has converged (k_si_orth_cl)
     __shared__ double sv[AP_KB][SI_FR + 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long i = blockIdx.x * 32L + lane;
@@ -675,7 +700,7 @@ __global__ void __launch_bounds__(256) k_si_apply_cols(const double *__restrict_
         __syncthreads();
         if (i < n && 4 * w < r) {
             const double *g = G + i + n * kb;
-#pragma unroll 8
+#pragma unroll 16
             for (int kk = 0; kk < nk; kk++) {
                 const double gv = g[n * kk];
 #pragma unroll
@@ -732,32 +757,41 @@ static int top_eigvecs_fast(const double *G, long n, long r, float *U, double *w
     double *V = ws, *Y = ws + nr, *part = ws + 2 * nr, *part2 = ws + (2 + nks) * nr,
            *scal = ws + (2 + 2 * nks) * nr;
     int *fail = reinterpret_cast<int *>(scal + 2);
+    int *st = reinterpret_cast<int *>(scal + 3);  // 4 ints: done, extra + 1, steps, final step
     double *h = pinned_scalars();
     if (!h) return CUD_ERR_NO_MEMORY;
     const long kchunk = (n + nks - 1) / nks;
     const dim3 ga((unsigned)((n + 31) / 32), (unsigned)nks);
     const unsigned gi = (unsigned)std::min<long>((nr + 255) / 256, 4L * kNumSMs);
-    CUD_CHECK(cudaMemsetAsync(fail, 0, sizeof(int), s));
+    CUD_CHECK(cudaMemsetAsync(fail, 0, 3 * sizeof(double), s));  // fail and the state
     if (U0) k_si_init_from<<<gi, 256, 0, s>>>(U0, Y, n, (int)r);
     else k_si_init<<<gi, 256, 0, s>>>(Y, n, (int)r);
-    k_si_orth_cl<<<CL_N, CL_T, smem, s>>>(Y, 1, nullptr, n, (int)r, V, scal, fail);
+    k_si_orth_cl<<<CL_N, CL_T, smem, s>>>(Y, 1, nullptr, n, (int)r, V, scal, fail, nullptr);
     CUD_CHECK_LAUNCH("subspace init");
-    int extra = -1;  // iterations still to run after the tolerance is met
-    for (int it = 0; it < max_iters; it++) {
-        // two products per orthonormalisation (G^2 V): the columns' condition
-        // grows by (lambda_1 / lambda_r)^2 per step, well inside CholQR2's range
-        k_si_apply_cols<<<ga, 256, 0, s>>>(G, V, 1, n, (int)r, kchunk, part2);
-        k_si_apply_cols<<<ga, 256, 0, s>>>(G, part2, nks, n, (int)r, kchunk, part);
-        k_si_orth_cl<<<CL_N, CL_T, smem, s>>>(part, nks, V, n, (int)r, Y, scal, fail);
-        CUD_CHECK_LAUNCH("subspace step");
-        std::swap(V, Y);
-        CUD_CHECK(cudaMemcpyAsync(h, scal, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    // steps are queued SI_BATCH at a time; the state is read once per batch
+    // and the launches after convergence return at once.  Step j (from 1)
+    // writes buffer j % 2 (buffer 0 = the initial V).
+    constexpr int SI_BATCH = 4;
+    for (int queued = 0; queued < max_iters;) {
+        const int nb = std::min(SI_BATCH, max_iters - queued);
+        for (int b = 0; b < nb; b++) {
+            // two products per orthonormalisation (G^2 V): the columns' condition
+            // grows by (lambda_1 / lambda_r)^2 per step, well inside CholQR2's range
+            k_si_apply_cols<<<ga, 256, 0, s>>>(G, V, 1, n, (int)r, kchunk, part2, st);
+            k_si_apply_cols<<<ga, 256, 0, s>>>(G, part2, nks, n, (int)r, kchunk, part, st);
+            k_si_orth_cl<<<CL_N, CL_T, smem, s>>>(part, nks, V, n, (int)r, Y, scal, fail, st);
+            std::swap(V, Y);
+        }
+        CUD_CHECK_LAUNCH("subspace steps");
+        queued += nb;
+        CUD_CHECK(cudaMemcpyAsync(h, scal + 2, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
         CUD_CHECK(cudaStreamSynchronize(s));
-        if (reinterpret_cast<int *>(h + 2)[0]) return CUD_ERR_NOT_CONVERGED;  // rank-deficient iterate
-        if (extra < 0 && h[0] < 1e-13 * (double)r) extra = 1;
-        if (extra >= 0 && extra-- == 0) {
-            k_si_apply_cols<<<ga, 256, 0, s>>>(G, V, 1, n, (int)r, kchunk, part);
-            k_si_ritz_cl<<<CL_N, CL_T, smem, s>>>(part, nks, V, n, (int)r, U);
+        const int *hs = reinterpret_cast<const int *>(h);  // fail, pad, done, extra + 1, steps, final
+        if (hs[0]) return CUD_ERR_NOT_CONVERGED;          // rank-deficient iterate
+        if (hs[2]) {
+            const double *Vf = ws + ((hs[5] % 2) ? nr : 0);
+            k_si_apply_cols<<<ga, 256, 0, s>>>(G, Vf, 1, n, (int)r, kchunk, part, nullptr);
+            k_si_ritz_cl<<<CL_N, CL_T, smem, s>>>(part, nks, Vf, n, (int)r, U);
             CUD_CHECK_LAUNCH("subspace ritz");
             return CUD_OK;
         }
