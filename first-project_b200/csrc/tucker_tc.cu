@@ -14,7 +14,8 @@
 // the other modes contiguous) come from one convert-and-unfold kernel.
 //
 // Precision: BF16 -> Grams from one BF16 GEMM; BF16X3 / DEFAULT -> Grams
-// from the three-term split (hi hi + hi lo + lo hi).  TTMs are BF16 in both.
+// from the three-term split (hi hi + hi lo + lo hi, the last term the
+// transpose of the middle one).  TTMs are BF16 in both.
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"
@@ -282,15 +283,31 @@ GemmEpi epi_f32(float *out, long ldm, long ldn, int accumulate) {
 
 // Gram (I x I, FP64 into w.g64) of the rows of the I x K BF16 operands:
 // hi hi^T, plus hi lo^T + lo hi^T when use_lo.
+// g64 = HH + P + P^T in FP64 (P = hi lo^T; its transpose is lo hi^T).
+__global__ void k_gram_finish(const float *__restrict__ HH, const float *__restrict__ P, long I,
+                              double *__restrict__ g64) {
+    const long n2 = I * I;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n2; e += (long)gridDim.x * blockDim.x) {
+        const long m = e / I, n = e - m * I;
+        g64[e] = (double)HH[e] + (double)P[e] + (double)P[n * I + m];
+    }
+}
+
+// The Gram of the unfolding in FP64.  BF16x3: hi hi^T + hi lo^T + lo hi^T,
+// where the last term is the transpose of the middle one, so two GEMMs
+// (one pass less over the operands) and a finishing sum; P goes to w.V,
+// which the eigensolver only uses afterwards.
 int gram_tc(const TcWork &w, long I, long K, bool use_lo, cudaStream_t s) {
     if (gemm_tc_ws_bytes(I, I, K) > w.gws_bytes) return CUD_ERR_INVALID_ARGUMENT;
     int st = gemm_tc_bf16(w.uh, K, w.uh, K, I, I, K, epi_f32(w.g32, I, 1, 0), w.gws, s);
     if (st) return st;
     if (use_lo && w.ul) {
-        if ((st = gemm_tc_bf16(w.uh, K, w.ul, K, I, I, K, epi_f32(w.g32, I, 1, 1), w.gws, s))) return st;
-        if ((st = gemm_tc_bf16(w.ul, K, w.uh, K, I, I, K, epi_f32(w.g32, I, 1, 1), w.gws, s))) return st;
+        float *P = reinterpret_cast<float *>(w.V);
+        if ((st = gemm_tc_bf16(w.uh, K, w.ul, K, I, I, K, epi_f32(P, I, 1, 0), w.gws, s))) return st;
+        k_gram_finish<<<gfor(I * I), 256, 0, s>>>(w.g32, P, I, w.g64);
+    } else {
+        k_f32_to_f64<<<gfor(I * I), 256, 0, s>>>(w.g32, w.g64, I * I);
     }
-    k_f32_to_f64<<<gfor(I * I), 256, 0, s>>>(w.g32, w.g64, I * I);
     CUD_CHECK_LAUNCH("gram_tc");
     return CUD_OK;
 }
