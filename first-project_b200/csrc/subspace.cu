@@ -851,3 +851,14 @@ int top_eigvecs_subspace(const double *G, long n, long r, float *U, double *ws, 
 }
 
 }  // namespace cud
+
+extern "C" int cud_syev_top(const double *G, long n, long r, float *U, const float *U0, int max_iters,
+                            void *stream) {
+    if (n <= 0 || r <= 0 || r > n || !G || !U || max_iters <= 0) return cud::set_status(CUD_ERR_INVALID_ARGUMENT);
+    // room for the fast path's eight k slices of partial products
+    const size_t wsd = std::max(cud::subspace_ws_doubles(n, r), (size_t)18 * (size_t)n * (size_t)r + 8);
+    int st;
+    double *ws = static_cast<double *>(cud::scratch(cud::kSlotEig, wsd * sizeof(double), &st));
+    if (!ws) return cud::set_status(st);
+    return cud::set_status(cud::top_eigvecs_subspace(G, n, r, U, ws, wsd, max_iters, cud::as_stream(stream), U0));
+}

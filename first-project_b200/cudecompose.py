@@ -106,6 +106,7 @@ _sig("cud_mttkrp", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _v
 _sig("cud_unfold_gram", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _i, _vp])
 _sig("cud_mttkrp_path", [_i, ctypes.POINTER(_l), _i, _l, _i])
 _sig("cud_syev_jacobi", [_vp, _l, _vp, _vp, _i, _vp])
+_sig("cud_syev_top", [_vp, _l, _l, _vp, _vp, _i, _vp])
 _sig("cud_cp_default_options", [ctypes.POINTER(CpOptions)], None)
 _sig("cud_cp_als", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
                     ctypes.POINTER(CpOptions), ctypes.POINTER(CpResult), _vp])
@@ -313,6 +314,14 @@ def syev_jacobi(A, n, W, V, max_sweeps=60, stream=None):
     return _check(_lib.cud_syev_jacobi(_ptr(A), n, _ptr(W), _ptr(V), max_sweeps,
                                        _stream(stream)), "syev_jacobi",
                   allow=(OK, ERR_NOT_CONVERGED))
+
+
+def syev_top(G, n, r, U, U0=None, max_iters=300, stream=None):
+    """U (n x r, FP32, column-major) = the r leading eigenvectors of the
+    symmetric PSD FP64 n x n matrix G, ascending eigenvalue order; U0 seeds
+    the iteration.  Returns OK or ERR_NOT_CONVERGED."""
+    return _check(_lib.cud_syev_top(_ptr(G), n, r, _ptr(U), _ptr(U0), max_iters, _stream(stream)),
+                  "syev_top", allow=(OK, ERR_NOT_CONVERGED))
 
 
 def cp_default_options() -> CpOptions:

@@ -164,6 +164,17 @@ int cud_unfold_gram(const float *X, int order, const long *dims, int mode, doubl
  * (column j pairs with W[j]).  max_sweeps bounds the iteration. */
 int cud_syev_jacobi(double *A, long n, double *W, double *V, int max_sweeps, void *stream);
 
+/* Extension (replaces the partial cusolverDnSsyevdx call at
+ * src/tucker_hosvd.cu:43-61, which asks for the leading eigenpairs only):
+ * the r leading eigenvectors of the symmetric positive semi-definite n x n
+ * FP64 matrix G (column-major; G is not modified) by subspace iteration,
+ * into U (n x r, FP32, column-major) in ascending eigenvalue order (the
+ * largest last).  U0 (n x r, FP32; may be NULL or alias U) seeds the
+ * iteration instead of a random block.  Returns CUD_ERR_NOT_CONVERGED when
+ * the subspace did not settle within max_iters steps (U is then not
+ * written) and CUD_ERR_UNSUPPORTED for r > 64. */
+int cud_syev_top(const double *G, long n, long r, float *U, const float *U0, int max_iters, void *stream);
+
 /* ---- decompositions ----------------------------------------------------- */
 
 typedef struct cud_cp_options {
