@@ -300,6 +300,46 @@ def leg_tucker(cd, torch, stream, sptr):
     return out
 
 
+def leg_streamed(cd, torch, dims=(512, 512, 512), R=64, slab=64, sweeps=2):
+    """Out-of-core CP-ALS (streamed.py): the 512^3 tensor in pinned host
+    memory, every mode's MTTKRP streaming it in slabs of `slab` frontal
+    slices (BF16x3), copies overlapped with compute on two device buffers."""
+    import streamed
+    X, _ = cd.make_cp_tensor(dims, R, seed=1000)
+    init = cd.make_init(dims, R, seed=2000)
+    Xh = X.cpu().pin_memory()
+    del X
+    torch.cuda.synchronize()
+    sc = streamed.StreamedCP(cd, Xh, dims, R, [u.clone() for u in init], slab=slab,
+                             precision=cd.PREC_BF16X3, nbuf=2)
+    sc.sweep()  # warm
+    torch.cuda.synchronize()
+    b0 = sc.h2d_bytes
+    e0, e1 = _events(torch)
+    e0.record(sc.ops.compute)
+    for _ in range(sweeps):
+        sc.sweep()
+    e1.record(sc.ops.compute)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3 / sweeps
+    h2d = (sc.h2d_bytes - b0) / sweeps
+    # the host link alone: one slab-sized pinned copy loop over the tensor
+    buf = torch.empty(Xh.numel() // dims[-1] * slab, device="cuda")
+    n = buf.numel()
+    c0, c1 = _events(torch)
+    c0.record()
+    for k in range(0, Xh.numel(), n):
+        buf[: min(n, Xh.numel() - k)].copy_(Xh[k:k + n], non_blocking=True)
+    c1.record()
+    c1.synchronize()
+    copy_gbs = 4 * Xh.numel() / (c0.elapsed_time(c1) * 1e-3) / 1e9
+    fit = sc.fit()
+    return {"dims": list(dims), "rank": R, "slab_slices": slab, "buffers": 2, "precision": "bf16x3",
+            "seconds_per_sweep": round(sec, 5), "h2d_bytes_per_sweep": int(h2d),
+            "h2d_gbs": round(h2d / sec / 1e9, 2), "host_copy_gbs": round(copy_gbs, 2),
+            "link_bound_fraction": round((h2d / (copy_gbs * 1e9)) / sec, 3), "fit": round(fit, 6)}
+
+
 def np_prod(xs):
     p = 1
     for x in xs:
@@ -511,7 +551,7 @@ def main():
                     help="time only the MTTKRP kernels (profiling runs) and exit")
     ap.add_argument("--kreps", type=int, default=10, help="timed MTTKRP launches per mode")
     ap.add_argument("--kwarm", type=int, default=3, help="untimed MTTKRP launches per mode")
-    ap.add_argument("--legs", default="cp128,order4,tucker,batched,warmstart",
+    ap.add_argument("--legs", default="cp128,order4,tucker,batched,warmstart,streamed",
                     help="side workloads to add as extra keys (comma list, or 'none')")
     ap.add_argument("--ws-train", type=int, default=204800, help="warm-start training samples")
     ap.add_argument("--ws-eval", type=int, default=4096, help="warm-start held-out tensors")
@@ -566,8 +606,30 @@ def main():
             cd.mttkrp(X, dims, U, mode, R, outs[mode], prec, stream=sptr)
         e1.record(stream)
         e1.synchronize()
-        ms = e0.elapsed_time(e1) / reps
+        ms_eager = e0.elapsed_time(e1) / reps
+        # the same calls replayed from a CUDA graph on the same stream: each
+        # call still launches its B pack, the MTTKRP and the split reduce;
+        # the graph removes the host launch gaps between them
+        ms, timing = ms_eager, "eager"
+        try:
+            stream.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                for _ in range(reps):
+                    cd.mttkrp(X, dims, U, mode, R, outs[mode], prec, stream=sptr)
+            with torch.cuda.stream(stream):
+                g.replay()
+                e0.record(stream)
+                g.replay()
+                e1.record(stream)
+            e1.synchronize()
+            ms, timing = e0.elapsed_time(e1) / reps, "graph"
+            del g
+        except RuntimeError:
+            pass
+        stream.synchronize()
         kern[mode] = {"ms": round(ms, 5), "gbs": round(mttkrp_bytes(dims, R, mode) / ms / 1e6, 1),
+                      "timing": timing, "ms_eager": round(ms_eager, 5),
                       "path": cd.mttkrp_path(dims, mode, R, prec)}
     if args.only_mttkrp:
         if rank == 0:
@@ -622,7 +684,9 @@ def main():
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
-                     "kernel": "MTTKRP (mean over the 3 modes)", "per_mode": kern},
+                     "kernel": "MTTKRP call (B pack + tensor-core MTTKRP + split reduce, CUDA-graph replay "
+                               "of 10 calls), mean over the 3 modes",
+                     "per_mode": kern},
         "gpu_launches": kps * args.steps if kps and kps > 0 else None,
         "kernels_per_sweep": kps, "fit_after_timed_sweeps": round(fit_now, 8),
         "clocks": clk.summary(),
@@ -701,7 +765,8 @@ def main():
                "order4": lambda: leg_order4(cd, torch, stream, sptr),
                "tucker": lambda: leg_tucker(cd, torch, stream, sptr),
                "batched": lambda: leg_batched(cd, torch, stream, sptr),
-               "warmstart": lambda: leg_warmstart(cd, torch, args.ws_train, args.ws_eval)}
+               "warmstart": lambda: leg_warmstart(cd, torch, args.ws_train, args.ws_eval),
+               "streamed": lambda: leg_streamed(cd, torch)}
         for name in legs:
             if name not in fns:
                 continue
