@@ -18,7 +18,8 @@
 //     converged and skipped by later sweeps.
 // The host captures `sweeps_per_graph` sweeps (queue reset + kernel) in one
 // CUDA graph and replays it until every tensor has converged or hit the
-// sweep limit.  The CTA size and the CTAs per SM come from a small autotuner
+// sweep limit.  The CTA size, the CTAs per SM and the MTTKRP register tile's
+// height come from a small autotuner
 // (batched_tune) that times one sweep per candidate on the batch itself and
 // caches the winner per batch shape class.
 #include <map>
@@ -34,7 +35,7 @@ namespace {
 
 constexpr int BMAXD = 96;    // largest mode size handled (smem sizing)
 constexpr int BMAXR = 16;    // largest rank handled
-constexpr int BSPLIT = 4;    // most thread groups splitting one contraction
+constexpr int B_RED3 = 2 * BMAXR * BMAXD;  // mode-3 partials: 2 RT groups x ranks x BMAXD / RT row groups
 
 __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
@@ -73,9 +74,9 @@ struct BatchArgs {
 // shared memory layout (floats / doubles), sized for BMAXD x BMAXR
 struct BatchSmem {
     float F[3][BMAXD * BMAXR];       // factors, column-major I_m x R
-    float slice[2][BMAXD * (BMAXD + 1)];  // two frontal slices (double buffer), row stride I + 1
+    float slice[2][BMAXD * (BMAXD + 1) + 4];  // two frontal slices (double buffer), row stride I + 1
     float M[BMAXD * BMAXR];          // MTTKRP result of the current mode
-    float red3[BSPLIT * BMAXR * (BMAXD / 2)]; // mode-3 per-slice partials (group x rank x row pair)
+    float red3[B_RED3];              // mode-3 per-slice partials (group x rank x row group)
     double V[BMAXR * BMAXR];         // normal matrix / its inverse
     double rowk[BMAXR], colk[BMAXR];
     double red[32];
@@ -93,34 +94,46 @@ __device__ void load_factors(BatchSmem &sm, const BatchArgs &a, const TensorMeta
 }
 
 // M (I_mode x R) = MTTKRP of mode `mode` with the factors in shared memory.
-// Thread items: (row pair, 4 ranks) with rows = i (mode 1) or j (modes 2, 3);
-// when the items leave threads idle, S <= BSPLIT groups of threads split the
-// inner contraction (over j, or over i) and their partials are added at the
-// end (modes 1, 2) or per slice (mode 3) in group order.  The frontal slices
-// stream through two shared-memory buffers with cp.async: slice k + 1 loads
-// while slice k is contracted.  (A deeper ring measured slower: the
-// contraction's instruction issue, not the load latency, sets the pace.)
-template <int NT>
+// Thread items: (RT consecutive rows, 4 ranks) with rows = i (mode 1) or j
+// (modes 2, 3) -- an RT x 4 register tile, RT x 4 FMAs per RT + 4 shared
+// loads; RT (2 or 4) is the autotuner's tile height.  The loads are not
+// guarded: rows past the mode's end read the slice's padding column or the
+// next column, ranks past R read the factor arrays' spare columns (all
+// inside the buffers since BMAXD is a multiple of RT), and those products
+// only reach accumulators that are never stored.  When the items leave
+// threads idle, S <= 2 RT groups of threads split the inner contraction
+// (over j, or over i) and their partials are added at the end (modes 1, 2)
+// or per slice (mode 3) in group order.  The frontal slices stream through
+// two shared-memory buffers with cp.async: slice k + 1 loads while slice k
+// is contracted.  (A deeper ring measured slower: the contraction's
+// instruction issue, not the load latency, sets the pace.)
+template <int NT, int RT>
 __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
-    constexpr int IPB = (BMAXD / 2 * (BMAXR / 4) + NT - 1) / NT;
+    constexpr int GS = 2 * RT;          // most groups splitting one contraction
+    constexpr int NGM = BMAXD / RT;     // row groups at most
+    constexpr int IPB = (NGM * (BMAXR / 4) + NT - 1) / NT;
+    static_assert(BMAXD % RT == 0, "row tiles must divide BMAXD");
+    static_assert(GS * BMAXR * NGM <= B_RED3, "mode-3 partials");
     const int I = t.dims[0], J = t.dims[1], K = t.dims[2], R = t.R;
     const int ld = I + 1;
     const float *X = a.X + t.xoff;
     const int Q = t.dims[mode];
     const int rows = (mode == 0) ? I : J;
-    const int npair = (rows + 1) / 2;
+    const int ngrp = (rows + RT - 1) / RT;
     const int rq = (R + 3) / 4;
-    const int items = npair * rq;
-    const int S = max(1, min(BSPLIT, NT / max(1, items)));
+    const int items = ngrp * rq;
+    const int S = max(1, min(GS, NT / max(1, items)));
     const int L = (mode == 0) ? J : I;  // contraction length within a slice
     // this thread: item it = tid % items' (u = 0 when split), group g
     const int g = (S > 1) ? (int)threadIdx.x / items : 0;
     const int l0 = g * L / S, l1 = (g + 1) * L / S;
-    float acc[IPB][2][4];
+    float acc[IPB][RT][4];
 #pragma unroll
     for (int u = 0; u < IPB; u++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) { acc[u][0][c] = 0.f; acc[u][1][c] = 0.f; }
+        for (int v = 0; v < RT; v++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[u][v][c] = 0.f;
     auto issue = [&](int k) {  // slice k into buffer k & 1, as one cp.async group
         const float *src = X + (long)k * I * J;
         float *dst = sm.slice[k & 1];
@@ -150,71 +163,79 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
             const int it = (S > 1) ? ((u == 0 && (int)threadIdx.x < S * items) ? (int)threadIdx.x % items : items)
                                    : (int)threadIdx.x + NT * u;
             if (it >= items) continue;
-            const int rp = (it % npair) * 2;
-            const int r0 = (it / npair) * 4;
-            float t2[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+            const int rg = it % ngrp;
+            const int rp = rg * RT;
+            const int r0 = (it / ngrp) * 4;
+            float t2[RT][4];
+#pragma unroll
+            for (int v = 0; v < RT; v++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) t2[v][c] = 0.f;
             if (mode == 0) {
                 // T[i, r] = sum_j X[i, j] B[j, r]
-                const float *Bf = sm.F[1];
+                const float *xp = sl + rp;
+                const float *bp = sm.F[1] + J * r0;
+#pragma unroll 2
                 for (int j = l0; j < l1; j++) {
-                    const float x0 = sl[rp + ld * j];
-                    const float x1 = (rp + 1 < I) ? sl[rp + 1 + ld * j] : 0.f;
+                    float x[RT], b[4];
 #pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const int r = r0 + c;
-                        const float b = (r < R) ? Bf[j + J * r] : 0.f;
-                        t2[0][c] = fmaf(x0, b, t2[0][c]);
-                        t2[1][c] = fmaf(x1, b, t2[1][c]);
-                    }
+                    for (int v = 0; v < RT; v++) x[v] = xp[v + ld * j];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) b[c] = bp[j + J * c];
+#pragma unroll
+                    for (int v = 0; v < RT; v++)
+#pragma unroll
+                        for (int c = 0; c < 4; c++) t2[v][c] = fmaf(x[v], b[c], t2[v][c]);
                 }
             } else {
                 // T[j, r] = sum_i X[i, j] A[i, r]
-                const float *Af = sm.F[0];
+                const float *xp = sl + ld * rp;
+                const float *ap = sm.F[0] + I * r0;
+#pragma unroll 2
                 for (int i = l0; i < l1; i++) {
-                    const float x0 = sl[i + ld * rp];
-                    const float x1 = (rp + 1 < J) ? sl[i + ld * (rp + 1)] : 0.f;
+                    float x[RT], av[4];
 #pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const int r = r0 + c;
-                        const float av = (r < R) ? Af[i + I * r] : 0.f;
-                        t2[0][c] = fmaf(x0, av, t2[0][c]);
-                        t2[1][c] = fmaf(x1, av, t2[1][c]);
-                    }
+                    for (int v = 0; v < RT; v++) x[v] = xp[i + ld * v];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) av[c] = ap[i + I * c];
+#pragma unroll
+                    for (int v = 0; v < RT; v++)
+#pragma unroll
+                        for (int c = 0; c < 4; c++) t2[v][c] = fmaf(x[v], av[c], t2[v][c]);
                 }
             }
             if (mode < 2) {
-                const float *Cf = sm.F[2];
+                const float *cp = sm.F[2] + K * r0 + k;
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    const int r = r0 + c;
-                    const float w = (r < R) ? Cf[k + K * r] : 0.f;
-                    acc[u][0][c] = fmaf(t2[0][c], w, acc[u][0][c]);
-                    acc[u][1][c] = fmaf(t2[1][c], w, acc[u][1][c]);
+                    const float w = cp[K * c];
+#pragma unroll
+                    for (int v = 0; v < RT; v++) acc[u][v][c] = fmaf(t2[v][c], w, acc[u][v][c]);
                 }
             } else {
-                // this pair's (and group's) share of M[k, r] = sum_j T[j, r] B[j, r]
+                // this row group's (and thread group's) share of M[k, r] = sum_j T[j, r] B[j, r]
                 const float *Bf = sm.F[1];
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
                     const int r = r0 + c;
                     float v = 0.f;
-                    if (r < R) {
-                        v = t2[0][c] * Bf[rp + J * r];
-                        if (rp + 1 < J) v = fmaf(t2[1][c], Bf[rp + 1 + J * r], v);
-                    }
-                    sm.red3[(g * BMAXR + r0 + c) * (BMAXD / 2) + rp / 2] = v;
+                    if (r < R)
+#pragma unroll
+                        for (int w = 0; w < RT; w++)
+                            if (rp + w < J) v = fmaf(t2[w][c], Bf[rp + w + J * r], v);
+                    sm.red3[(g * BMAXR + r0 + c) * NGM + rg] = v;
                 }
             }
         }
         if (mode == 2) {
-            // sum over groups and row pairs: one warp per rank, lanes over
-            // the pairs, then a fixed shuffle tree (deterministic)
+            // sum over groups and row groups: one warp per rank, lanes over
+            // the row groups, then a fixed shuffle tree (deterministic)
             __syncthreads();
             const int lane = threadIdx.x & 31;
             for (int r = threadIdx.x >> 5; r < R; r += NT / 32) {
                 float v = 0.f;
                 for (int gg = 0; gg < S; gg++)
-                    for (int p2 = lane; p2 < npair; p2 += 32) v += sm.red3[(gg * BMAXR + r) * (BMAXD / 2) + p2];
+                    for (int p2 = lane; p2 < ngrp; p2 += 32) v += sm.red3[(gg * BMAXR + r) * NGM + p2];
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
                 if (lane == 0) sm.M[k + K * r] = v;
             }
@@ -222,28 +243,26 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
         __syncthreads();  // slice k's buffer is refilled by the next issue
     }
     if (mode < 2) {
-        // groups' partials added in group order through red3 (mode 3 does
-        // not use it now): group 0 writes, the others add in turn
+        // groups' partials added in group order: group 0 writes, the others
+        // add in turn
         for (int gg = 0; gg < S; gg++) {
 #pragma unroll
             for (int u = 0; u < IPB; u++) {
                 const int it = (S > 1) ? ((u == 0 && (int)threadIdx.x < S * items) ? (int)threadIdx.x % items : items)
                                        : (int)threadIdx.x + NT * u;
                 if (it >= items || g != gg) continue;
-                const int rp = (it % npair) * 2;
-                const int r0 = (it / npair) * 4;
+                const int rp = (it % ngrp) * RT;
+                const int r0 = (it / ngrp) * 4;
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
                     const int r = r0 + c;
-                    if (r < R) {
-                        if (gg == 0) {
-                            sm.M[rp + Q * r] = acc[u][0][c];
-                            if (rp + 1 < Q) sm.M[rp + 1 + Q * r] = acc[u][1][c];
-                        } else {
-                            sm.M[rp + Q * r] += acc[u][0][c];
-                            if (rp + 1 < Q) sm.M[rp + 1 + Q * r] += acc[u][1][c];
-                        }
-                    }
+                    if (r < R)
+#pragma unroll
+                        for (int v = 0; v < RT; v++)
+                            if (rp + v < Q) {
+                                if (gg == 0) sm.M[rp + v + Q * r] = acc[u][v][c];
+                                else sm.M[rp + v + Q * r] += acc[u][v][c];
+                            }
                 }
             }
             __syncthreads();
@@ -300,7 +319,7 @@ __device__ void normal_inverse_small(BatchSmem &sm, const BatchArgs &a, const Te
     }
 }
 
-template <int NT>
+template <int NT, int RT>
 __global__ void __launch_bounds__(NT) k_batch_sweep(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BatchSmem &sm = *reinterpret_cast<BatchSmem *>(smem_raw);
@@ -320,7 +339,7 @@ __global__ void __launch_bounds__(NT) k_batch_sweep(BatchArgs a) {
         __syncthreads();
         double inner = 0.0;
         for (int mode = 0; mode < 3; mode++) {
-            mttkrp_small<NT>(sm, a, t, mode);
+            mttkrp_small<NT, RT>(sm, a, t, mode);
             normal_inverse_small<NT>(sm, a, t, mode);
             // U_mode = M V^-1 (FP64 accumulation), into shared and global memory
             const int Q = t.dims[mode];
@@ -421,29 +440,37 @@ struct BatchState {
     int *fallbacks = nullptr;
 };
 
-template <int NT>
+template <int NT, int RT>
 int launch_sweep(const BatchArgs &a, int ctas_per_sm, cudaStream_t s) {
     static bool attr[64] = {false};
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && !attr[dev]) {
-        CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NT, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(BatchSmem)));
         attr[dev] = true;
     }
     CUD_CHECK(cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s));
-    k_batch_sweep<NT><<<kNumSMs * ctas_per_sm, NT, sizeof(BatchSmem), s>>>(a);
+    k_batch_sweep<NT, RT><<<kNumSMs * ctas_per_sm, NT, sizeof(BatchSmem), s>>>(a);
     CUD_CHECK_LAUNCH("batched sweep");
     return CUD_OK;
 }
 
-int launch_cfg(const BatchArgs &a, int threads, int ctas_per_sm, cudaStream_t s) {
-    return threads == 128 ? launch_sweep<128>(a, ctas_per_sm, s) : launch_sweep<256>(a, ctas_per_sm, s);
+// Launch shape: threads per CTA, CTAs per SM, rows of the MTTKRP register
+// tile.
+struct BatchCfg {
+    int threads, ctas, rt;
+};
+
+int launch_cfg(const BatchArgs &a, const BatchCfg &c, cudaStream_t s) {
+    if (c.rt == 4)
+        return c.threads == 128 ? launch_sweep<128, 4>(a, c.ctas, s) : launch_sweep<256, 4>(a, c.ctas, s);
+    return c.threads == 128 ? launch_sweep<128, 2>(a, c.ctas, s) : launch_sweep<256, 2>(a, c.ctas, s);
 }
 
-// Autotuner cache: shape class -> (threads, CTAs per SM)
+// Autotuner cache: shape class -> launch shape
 std::mutex g_tune_mu;
-std::map<long, std::pair<int, int>> g_tune;
+std::map<long, BatchCfg> g_tune;
 
 long shape_class(int n, const int *dims, const int *ranks) {
     // bucket the mean element count and mean rank; plus the batch size order
@@ -521,9 +548,9 @@ int batched_impl(int ntensors, const long *dims, const long *ranks, const float 
     k_batch_setup<<<std::min(ntensors, kNumSMs * 4), 256, 0, s>>>(a.meta, ntensors, X, U);
     CUD_CHECK_LAUNCH("batched setup");
 
-    // tile shape from the autotuner (threads per CTA, CTAs per SM)
+    // launch shape from the autotuner (threads per CTA, CTAs per SM, tile rows)
     long key = shape_class(ntensors, hd.data(), hr.data());
-    std::pair<int, int> cfg(256, 2);
+    BatchCfg cfg{256, 2, 4};
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(key);
@@ -543,7 +570,7 @@ int batched_impl(int ntensors, const long *dims, const long *ranks, const float 
     st = CUD_OK;
     if (opt.use_graph) {
         if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) st = CUD_ERR_CUDA;
-        for (int i = 0; i < per && st == CUD_OK; i++) st = launch_cfg(a, cfg.first, cfg.second, cs);
+        for (int i = 0; i < per && st == CUD_OK; i++) st = launch_cfg(a, cfg, cs);
         cudaError_t e = cudaStreamEndCapture(cs, &graph);
         if (st == CUD_OK && e != cudaSuccess) st = cuda_status(e, "batched capture");
         if (st == CUD_OK) {
@@ -558,7 +585,7 @@ int batched_impl(int ntensors, const long *dims, const long *ranks, const float 
         if (exec) {
             if (cudaGraphLaunch(exec, cs) != cudaSuccess) { st = CUD_ERR_CUDA; break; }
         } else {
-            for (int i = 0; i < per && st == CUD_OK; i++) st = launch_cfg(a, cfg.first, cfg.second, cs);
+            for (int i = 0; i < per && st == CUD_OK; i++) st = launch_cfg(a, cfg, cs);
         }
         launched += per;
         done_sweeps += per;
@@ -618,9 +645,12 @@ extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *r
         hr[t] = (int)ranks[t];
     }
     long key = shape_class(ntensors, hd.data(), hr.data());
-    const int cand[][2] = {{128, 2}, {128, 3}, {128, 4}, {256, 1}, {256, 2}, {256, 3}};
+    const int shapes[][2] = {{128, 2}, {128, 3}, {128, 4}, {256, 1}, {256, 2}, {256, 3}};
+    std::vector<BatchCfg> cand;
+    for (int rt : {2, 4})
+        for (auto &sh : shapes) cand.push_back({sh[0], sh[1], rt});
     float best = 1e30f;
-    std::pair<int, int> bestc(256, 2);
+    BatchCfg bestc{256, 2, 4};
     cudaStream_t s = as_stream(stream);
     cudaEvent_t e0, e1;
     CUD_CHECK(cudaEventCreate(&e0));
@@ -628,7 +658,7 @@ extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *r
     for (auto &c : cand) {
         {
             std::lock_guard<std::mutex> lk(g_tune_mu);
-            g_tune[key] = {c[0], c[1]};
+            g_tune[key] = c;
         }
         cud_cp_options opt;
         cud_cp_default_options(&opt);
@@ -644,7 +674,7 @@ extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *r
         if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return set_status(st); }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) { best = ms; bestc = {c[0], c[1]}; }
+        if (ms < best) { best = ms; bestc = c; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -652,7 +682,7 @@ extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *r
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune[key] = bestc;
     }
-    if (threads) *threads = bestc.first;
-    if (ctas_per_sm) *ctas_per_sm = bestc.second;
+    if (threads) *threads = bestc.threads;
+    if (ctas_per_sm) *ctas_per_sm = bestc.ctas;
     return set_status(CUD_OK);
 }

@@ -266,9 +266,11 @@ int cud_cp_als_batched_target(int ntensors, const long *dims, const long *ranks,
                               int *kernel_launches, void *stream);
 
 /* Extension: autotunes the batched sweep's launch shape (threads per CTA,
- * CTAs per SM) for this batch's shape class by timing two sweeps per
- * candidate; U_scratch is a copy of the factors (overwritten).  The choice
- * is cached per shape class and used by later cud_cp_als_batched calls. */
+ * CTAs per SM, and the rows of the MTTKRP register tile, 2 or 4) for this
+ * batch's shape class by timing two sweeps per candidate; U_scratch is a
+ * copy of the factors (overwritten).  The choice is cached per shape class
+ * and used by later cud_cp_als_batched calls; threads and ctas_per_sm
+ * report the first two. */
 int cud_cp_batched_tune(int ntensors, const long *dims, const long *ranks, const float *X,
                         const long *x_offsets, float *U_scratch, const long *u_offsets, int *threads,
                         int *ctas_per_sm, void *stream);
