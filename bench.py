@@ -340,6 +340,29 @@ def leg_streamed(cd, torch, dims=(512, 512, 512), R=64, slab=64, sweeps=2):
             "link_bound_fraction": round((h2d / (copy_gbs * 1e9)) / sec, 3), "fit": round(fit, 6)}
 
 
+def run_tucker_once(cd, torch, dims, ranks):
+    """One tensor-core HOSVD and one HOOI sweep (BF16x3) on a synthetic
+    Tucker tensor of the given shape; wall times and reconstruction errors."""
+    X, _, _ = cd.make_tucker_tensor(dims, ranks, seed=20)
+    core = torch.empty(int(np_prod(ranks)), device="cuda")
+    U = [torch.empty(d * r, device="cuda") for d, r in zip(dims, ranks)]
+    rec = torch.empty_like(X)
+    out = {"dims": list(dims), "ranks": list(ranks)}
+    for method, sweeps in (("hosvd", 0), ("hooi1", 1)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if sweeps == 0:
+            cd.tucker_hosvd(X, dims, ranks, core, U, precision=cd.PREC_BF16X3)
+        else:
+            cd.tucker_hooi(X, dims, ranks, core, U, sweeps=sweeps, precision=cd.PREC_BF16X3)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        cd.gentucker(rec, core, U, dims, ranks)
+        err = float(torch.linalg.norm((X - rec).double()) / torch.linalg.norm(X.double()))
+        out[method] = {"seconds": round(dt, 5), "rel_error": float(f"{err:.4e}")}
+    return out
+
+
 def np_prod(xs):
     p = 1
     for x in xs:
@@ -549,6 +572,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--only-mttkrp", action="store_true",
                     help="time only the MTTKRP kernels (profiling runs) and exit")
+    ap.add_argument("--only-tucker", action="store_true",
+                    help="run one Tucker HOSVD and one HOOI sweep on --dims with --tucker-ranks "
+                         "(profiling runs) and exit")
+    ap.add_argument("--tucker-ranks", default="16,16,16,16")
     ap.add_argument("--kreps", type=int, default=10, help="timed MTTKRP launches per mode")
     ap.add_argument("--kwarm", type=int, default=3, help="untimed MTTKRP launches per mode")
     ap.add_argument("--legs", default="cp128,order4,tucker,batched,warmstart,streamed",
@@ -582,6 +609,11 @@ def main():
     R = args.rank
     prec = cd.PRECISIONS[args.precision]
     prec_name = "bf16x3" if prec in (cd.PREC_DEFAULT, cd.PREC_BF16X3) else args.precision
+    if args.only_tucker:
+        if rank == 0:
+            print(json.dumps(run_tucker_once(cd, torch, dims, [int(x) for x in args.tucker_ranks.split(",")])),
+                  flush=True)
+        return
     if world > 1 and not args.only_mttkrp:
         run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_name)
         return
