@@ -84,6 +84,10 @@ struct KrFactors {
 size_t mttkrp_simt_ws_bytes(int order, const long *dims, int mode, long R, int round);
 int mttkrp_simt_rounded(const float *X, int order, const long *dims, const float *const *U,
                         int mode, long R, float *out, int round, void *ws, cudaStream_t s);
+// The CUDA-core MTTKRP on FP64 data (FP64 CP-ALS); ws as sized below.
+size_t mttkrp_simt_f64_ws_bytes(int order, const long *dims, int mode, long R);
+int mttkrp_simt_f64(const double *X, int order, const long *dims, const double *const *U, int mode, long R,
+                    double *out, void *ws, cudaStream_t s);
 // Tensor-core path (mttkrp_tc.cu): CUD_OK and the workspace size when it
 // applies to this shape/precision, CUD_ERR_UNSUPPORTED otherwise.
 int mttkrp_tc_query(int order, const long *dims, int mode, long R, int precision, size_t *ws_bytes);

@@ -1,5 +1,6 @@
 // MTTKRP on CUDA cores in FP32 (the "plain FP32" path and the fallback for
-// shapes the tensor-core path does not take).  Native layout, no unfolding,
+// shapes the tensor-core path does not take), and the same kernel in FP64
+// for the FP64 CP-ALS.  Native layout, no unfolding,
 // no materialised Khatri-Rao matrix.
 //
 // Around mode n the tensor is a (P, Q, S) array (P = prod of dims before n,
@@ -10,6 +11,8 @@
 // each s, a GEMM  X_s^T (Q x P) * L(P x R)  scaled by the row Rt[s, :].  The
 // KR rows (B operand) are generated per 16-deep slice into shared memory; the
 // contraction is split across CTAs and the FP32 partials reduced in FP64.
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace cud {
@@ -18,20 +21,33 @@ namespace {
 
 constexpr int BQ = 64, BR = 64, BK = 16, NT = 256;
 
+// The same kernel serves FP32 (KrFactors) and FP64 (KrFactors64) data.
+struct KrFactors64 {
+    int n = 0;
+    const double *U[kMaxOrder];
+    long rows[kMaxOrder];
+};
+template <typename T> struct KrOf;
+template <> struct KrOf<float> { using type = KrFactors; };
+template <> struct KrOf<double> { using type = KrFactors64; };
+
+template <typename T>
 struct SimtArgs {
-    const float *X;
+    const T *X;
     long P, Q, S, R;
-    int round;        // 0: FP32 operands; 1: round X and KR rows to FP16; 2: to BF16
-    KrFactors gen;    // factors generating the B operand (fastest first)
-    KrFactors outer;  // factors generating the per-s scale (P > 1), fastest first
+    int round;        // 0: operands as given; 1: round X and KR rows to FP16; 2: to BF16 (FP32 only)
+    typename KrOf<T>::type gen;    // factors generating the B operand (fastest first)
+    typename KrOf<T>::type outer;  // factors generating the per-s scale (P > 1), fastest first
     long ksteps;      // BK-steps per s
     long steps;       // total steps = (P > 1 ? S : 1) * ksteps
     long chunk;       // steps per split
-    float *part;      // [split][R][Q]
+    T *part;          // [split][R][Q]
 };
 
-__device__ __forceinline__ float kr_value(const KrFactors &f, const long *idx, long r) {
-    float v = 1.0f;
+template <typename KR>
+__device__ __forceinline__ auto kr_value(const KR &f, const long *idx, long r) {
+    using V = std::remove_cv_t<std::remove_pointer_t<std::remove_reference_t<decltype(f.U[0])>>>;
+    V v = 1;
     for (int i = 0; i < f.n; i++) v *= f.U[i][idx[i] + r * f.rows[i]];
     return v;
 }
@@ -41,8 +57,22 @@ __device__ __forceinline__ float round_to(float v, int mode) {
     if (mode == 2) return __bfloat162float(__float2bfloat16_rn(v));
     return v;
 }
+__device__ __forceinline__ double round_to(double v, int) { return v; }
 
-__device__ __forceinline__ void decompose(const KrFactors &f, long lin, long *idx) {
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+
+__device__ __forceinline__ void load4(const float *p, float *x) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+}
+__device__ __forceinline__ void load4(const double *p, double *x) {
+    const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+}
+
+template <typename KR>
+__device__ __forceinline__ void decompose(const KR &f, long lin, long *idx) {
     for (int i = 0; i < f.n; i++) {
         long d = f.rows[i];
         idx[i] = lin % d;
@@ -56,11 +86,11 @@ __device__ __forceinline__ void decompose(const KrFactors &f, long lin, long *id
 // kKind 2: other modes, flattened contraction k = p + P s with B = KR of all
 //          other factors formed (and rounded) as one product, as the
 //          reference's public mttkrp() does before its FP16 GEMM.
-template <int kKind>
-__global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs a) {
+template <int kKind, typename T>
+__global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs<T> a) {
     constexpr bool kModeZero = (kKind != 1);
-    __shared__ __align__(16) float As[BK][BQ];
-    __shared__ __align__(16) float Bs[BK][BR];
+    __shared__ __align__(16) T As[BK][BQ];
+    __shared__ __align__(16) T Bs[BK][BR];
     __shared__ long kidx[BK][kMaxOrder];
 
     const int t = threadIdx.x;
@@ -72,11 +102,11 @@ __global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs a) {
     const long send = min(a.steps, sbeg + a.chunk);
     const int tx = t & 15, ty = t >> 4;
 
-    float acc[4][4], tot[4][4];
+    T acc[4][4], tot[4][4];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) { acc[i][j] = 0.f; tot[i][j] = 0.f; }
+        for (int j = 0; j < 4; j++) { acc[i][j] = 0; tot[i][j] = 0; }
 
     const long K = (kKind == 0) ? a.S : (kKind == 1) ? a.P : a.P * a.S;
     long cur_s = -1;
@@ -92,9 +122,9 @@ __global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs a) {
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     long r = r0 + ty * 4 + j;
-                    float w = (r < a.R) ? kr_value(a.outer, oidx, r) : 0.f;
+                    T w = (r < a.R) ? kr_value(a.outer, oidx, r) : T(0);
 #pragma unroll
-                    for (int i = 0; i < 4; i++) { tot[i][j] = fmaf(acc[i][j], w, tot[i][j]); acc[i][j] = 0.f; }
+                    for (int i = 0; i < 4; i++) { tot[i][j] = fma_t(acc[i][j], w, tot[i][j]); acc[i][j] = 0; }
                 }
             }
             cur_s = s;
@@ -112,7 +142,7 @@ __global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs a) {
             if (kModeZero) { qq = e % BQ; kk = e / BQ; }
             else { kk = e % BK; qq = e / BK; }
             long q = q0 + qq, k = k0 + kk;
-            float v = 0.f;
+            T v = 0;
             if (q < a.Q && k < K) {
                 if (kKind == 0) v = a.X[q + a.Q * k];
                 else if (kKind == 1) v = a.X[k + a.P * (q + a.Q * s)];
@@ -128,20 +158,20 @@ __global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs a) {
             int e = t + NT * i;
             int rr = e % BR, kk = e / BR;
             long r = r0 + rr, k = k0 + kk;
-            float v = 0.f;
+            T v = 0;
             if (r < a.R && k < K) v = round_to(kr_value(a.gen, kidx[kk], r), a.round);
             Bs[kk][rr] = v;
         }
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < BK; kk++) {
-            float4 av = *reinterpret_cast<const float4 *>(&As[kk][tx * 4]);
-            float4 bv = *reinterpret_cast<const float4 *>(&Bs[kk][ty * 4]);
-            float x[4] = {av.x, av.y, av.z, av.w}, y[4] = {bv.x, bv.y, bv.z, bv.w};
+            T x[4], y[4];
+            load4(&As[kk][tx * 4], x);
+            load4(&Bs[kk][ty * 4], y);
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fmaf(x[i], y[j], acc[i][j]);
+                for (int j = 0; j < 4; j++) acc[i][j] = fma_t(x[i], y[j], acc[i][j]);
         }
         __syncthreads();
     }
@@ -156,12 +186,12 @@ __global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs a) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             long r = r0 + ty * 4 + j;
-            float w = (r < a.R) ? kr_value(a.outer, oidx, r) : 0.f;
+            T w = (r < a.R) ? kr_value(a.outer, oidx, r) : T(0);
 #pragma unroll
-            for (int i = 0; i < 4; i++) tot[i][j] = fmaf(acc[i][j], w, tot[i][j]);
+            for (int i = 0; i < 4; i++) tot[i][j] = fma_t(acc[i][j], w, tot[i][j]);
         }
     }
-    float *P = a.part + z * a.R * a.Q;
+    T *P = a.part + z * a.R * a.Q;
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -171,14 +201,14 @@ __global__ void __launch_bounds__(NT) k_mttkrp_simt(SimtArgs a) {
         }
 }
 
-__global__ void k_sum_partials(const float *__restrict__ part, int splits, long n,
-                               float *__restrict__ out) {
+template <typename T>
+__global__ void k_sum_partials(const T *__restrict__ part, int splits, long n, T *__restrict__ out) {
     long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
     long stride = (long)gridDim.x * blockDim.x;
     for (long e = tid; e < n; e += stride) {
         double s = 0.0;
         for (int z = 0; z < splits; z++) s += (double)part[(long)z * n + e];
-        out[e] = (float)s;
+        out[e] = (T)s;
     }
 }
 
@@ -215,11 +245,14 @@ size_t mttkrp_simt_ws_bytes(int order, const long *dims, int mode, long R, int r
     return sizeof(float) * (size_t)p.splits * R * v.Q;
 }
 
-int mttkrp_simt_rounded(const float *X, int order, const long *dims, const float *const *U,
-                        int mode, long R, float *out, int round, void *ws, cudaStream_t s) {
+namespace {
+
+template <typename T>
+int mttkrp_simt_impl(const T *X, int order, const long *dims, const T *const *U, int mode, long R, T *out,
+                     int round, void *ws, cudaStream_t s) {
     ModeView v = mode_view(order, dims, mode);
     SimtPlan p = simt_plan(v, mode, R, round);
-    SimtArgs a;
+    SimtArgs<T> a;
     a.X = X;
     a.P = v.P; a.Q = v.Q; a.S = v.S; a.R = R;
     a.round = round;
@@ -232,7 +265,7 @@ int mttkrp_simt_rounded(const float *X, int order, const long *dims, const float
     a.outer.n = 0;
     for (int m = 0; m < order; m++) {
         if (m == mode) continue;
-        KrFactors &f = (mode_zero || m < mode) ? a.gen : a.outer;
+        auto &f = (mode_zero || m < mode) ? a.gen : a.outer;
         f.U[f.n] = U[m];
         f.rows[f.n] = dims[m];
         f.n++;
@@ -241,18 +274,33 @@ int mttkrp_simt_rounded(const float *X, int order, const long *dims, const float
     a.steps = p.steps;
     a.chunk = p.chunk;
     long splits = p.splits, qtiles = p.qtiles, rtiles = p.rtiles;
-    a.part = (float *)ws;
+    a.part = (T *)ws;
     if (!a.part) return CUD_ERR_INVALID_ARGUMENT;
     if (rtiles > 65535 || qtiles * splits > 0x7fffffffL) return CUD_ERR_UNSUPPORTED;
     dim3 grid((unsigned)(qtiles * splits), (unsigned)rtiles);
-    if (kind == 0) k_mttkrp_simt<0><<<grid, NT, 0, s>>>(a);
-    else if (kind == 1) k_mttkrp_simt<1><<<grid, NT, 0, s>>>(a);
-    else k_mttkrp_simt<2><<<grid, NT, 0, s>>>(a);
+    if (kind == 0) k_mttkrp_simt<0, T><<<grid, NT, 0, s>>>(a);
+    else if (kind == 1) k_mttkrp_simt<1, T><<<grid, NT, 0, s>>>(a);
+    else k_mttkrp_simt<2, T><<<grid, NT, 0, s>>>(a);
     CUD_CHECK_LAUNCH("mttkrp_simt");
-    k_sum_partials<<<blocks_for(R * v.Q, 256), 256, 0, s>>>(a.part, (int)splits, R * v.Q, out);
+    k_sum_partials<T><<<blocks_for(R * v.Q, 256), 256, 0, s>>>(a.part, (int)splits, R * v.Q, out);
     CUD_CHECK_LAUNCH("mttkrp_simt reduce");
     return CUD_OK;
 }
 
+}  // namespace
+
+int mttkrp_simt_rounded(const float *X, int order, const long *dims, const float *const *U,
+                        int mode, long R, float *out, int round, void *ws, cudaStream_t s) {
+    return mttkrp_simt_impl<float>(X, order, dims, U, mode, R, out, round, ws, s);
+}
+
+size_t mttkrp_simt_f64_ws_bytes(int order, const long *dims, int mode, long R) {
+    return 2 * mttkrp_simt_ws_bytes(order, dims, mode, R, 0);
+}
+
+int mttkrp_simt_f64(const double *X, int order, const long *dims, const double *const *U, int mode, long R,
+                    double *out, void *ws, cudaStream_t s) {
+    return mttkrp_simt_impl<double>(X, order, dims, U, mode, R, out, 0, ws, s);
+}
 
 }  // namespace cud

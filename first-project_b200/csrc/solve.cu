@@ -10,9 +10,10 @@ namespace cud {
 
 namespace {
 
-// G = U^T U (R x R, FP64) for U (I x R, FP32).  16x16 output tile per CTA,
-// rows staged through shared memory in chunks of 64.
-__global__ void __launch_bounds__(256) k_factor_gram(const float *__restrict__ U, long I, long R,
+// G = U^T U (R x R, FP64) for U (I x R, FP32 or FP64).  16x16 output tile
+// per CTA, rows staged through shared memory in chunks of 64.
+template <typename T>
+__global__ void __launch_bounds__(256) k_factor_gram(const T *__restrict__ U, long I, long R,
                                                      double *__restrict__ G) {
     __shared__ double sa[64][17];
     __shared__ double sb[64][17];
@@ -479,10 +480,17 @@ int factor_update(const UpdateArgs &a, cudaStream_t s) {
     return CUD_OK;
 }
 
+int factor_gram_f64(const double *U, long I, long R, double *G, cudaStream_t s) {
+    dim3 grid((unsigned)((R + 15) / 16), (unsigned)((R + 15) / 16));
+    k_factor_gram<double><<<grid, 256, 0, s>>>(U, I, R, G);
+    CUD_CHECK_LAUNCH("factor_gram_f64");
+    return CUD_OK;
+}
+
 int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s) {
     if (R > 160) {
         dim3 grid((unsigned)((R + 15) / 16), (unsigned)((R + 15) / 16));
-        k_factor_gram<<<grid, 256, 0, s>>>(U, I, R, G);
+        k_factor_gram<float><<<grid, 256, 0, s>>>(U, I, R, G);
         CUD_CHECK_LAUNCH("factor_gram");
         return CUD_OK;
     }

@@ -46,6 +46,7 @@ int factor_update(const UpdateArgs &a, cudaStream_t s);
 size_t update_ws_doubles(long I, long R);
 
 int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s);
+int factor_gram_f64(const double *U, long I, long R, double *G, cudaStream_t s);
 int normal_inverse(const NormalArgs &a, cudaStream_t s);
 // Per-device kernel attributes for normal_inverse; call before stream capture.
 int normal_inverse_prepare();

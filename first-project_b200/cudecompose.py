@@ -110,6 +110,9 @@ _sig("cud_syev_top", [_vp, _l, _l, _vp, _vp, _i, _vp])
 _sig("cud_cp_default_options", [ctypes.POINTER(CpOptions)], None)
 _sig("cud_cp_als", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
                     ctypes.POINTER(CpOptions), ctypes.POINTER(CpResult), _vp])
+_sig("cud_cp_als_f64", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
+                        ctypes.POINTER(CpOptions), ctypes.POINTER(CpResult), _vp])
+_sig("cud_mttkrp_f64", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _vp, _vp])
 _sig("cud_cp_init_curand", [_i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
                             ctypes.c_ulonglong, _vp])
 _sig("cud_cp_plan_create", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
@@ -340,6 +343,25 @@ def cp_als(X, dims, R, factors, max_sweeps=500, tol=0.0, precision=PREC_DEFAULT,
     _check(_lib.cud_cp_als(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
                            ctypes.byref(opt), ctypes.byref(res), _stream(stream)), "cp_als")
     return res
+
+
+def cp_als_f64(X, dims, R, factors, max_sweeps=500, tol=0.0, target_fit=0.0, stream=None) -> CpResult:
+    """FP64 CP-ALS (the reference's dprice/cp_als.cu and 4_cp_als.cu) on
+    float64 device tensors, factors updated in place.  Stops after
+    max_sweeps, when |fit - fit_prev| < tol (tol > 0), or when fit >=
+    target_fit (target_fit > 0)."""
+    opt = CpOptions(max_sweeps, tol, PREC_FP32, 0, 1, target_fit)
+    res = CpResult()
+    _check(_lib.cud_cp_als_f64(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
+                               ctypes.byref(opt), ctypes.byref(res), _stream(stream)), "cp_als_f64")
+    return res
+
+
+def mttkrp_f64(X, dims, factors, mode, R, out, stream=None):
+    """out (dims[mode] x R, column-major, float64) = X_(mode) (KR of the other
+    factors), all in FP64 on the CUDA cores."""
+    _check(_lib.cud_mttkrp_f64(_ptr(X), len(dims), _longs(dims), _ptrs(factors), mode, R,
+                               _ptr(out), _stream(stream)), "mttkrp_f64")
 
 
 class CpPlan:

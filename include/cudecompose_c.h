@@ -211,6 +211,22 @@ void cud_cp_default_options(cud_cp_options *opt);
 int cud_cp_als(const float *X, int order, const long *dims, long R, float *const *U,
                const cud_cp_options *opt, cud_cp_result *res, void *stream);
 
+/* The reference's FP64 variants decomposition/GPU/normal/dprice/cp_als.cu:3-212
+ * (order 3) and dprice/4_cp_als.cu:3-229 (order 4), as one general-order
+ * entry over device pointers: CP-ALS entirely in FP64 (CUDA-core MTTKRP,
+ * FP64 Grams, Hadamard, inverse with pseudo-inverse fallback, fit from the
+ * Gram identity each sweep).  X and U[m] (dims[m] x R, updated in place)
+ * are double; opt's precision, use_graph and check_every are ignored;
+ * R <= 160.  res may be NULL. */
+int cud_cp_als_f64(const double *X, int order, const long *dims, long R, double *const *U,
+                   const cud_cp_options *opt, cud_cp_result *res, void *stream);
+
+/* FP64 MTTKRP (the Khatri-Rao DGEMMs of dprice/cp_als.cu:64,72), any order
+ * and mode: out (dims[mode] x R, double) = X_(mode) (KR of the other
+ * factors), on the CUDA cores with no Khatri-Rao matrix formed. */
+int cud_mttkrp_f64(const double *X, int order, const long *dims, const double *const *U, int mode, long R,
+                   double *out, void *stream);
+
 /* Extension: a reusable CP-ALS plan -- the workspace, the Grams and the
  * captured per-sweep CUDA graph for one (X, dims, R, factors) problem, so
  * sweeps can be enqueued without synchronisation (what cud_cp_als loops
