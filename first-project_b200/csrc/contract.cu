@@ -26,11 +26,16 @@ __global__ void k_round_copy(const float *__restrict__ in, float *__restrict__ o
 
 // Y = X x_mode W  (W: J x dims[mode], row = new index).  With w_trans set,
 // W is given as its transpose (dims[mode] x J, e.g. a factor matrix U, so
-// that Y = X x_mode U^T).
-int mode_product(const float *X, int order, const long *dims, int mode, const float *W, long J,
-                 float *Y, cudaStream_t s, bool w_trans) {
+// that Y = X x_mode U^T).  FP32 or FP64 (gemm_simt / gemm_simt_f64).
+template <typename T>
+int mode_product_t(const T *X, int order, const long *dims, int mode, const T *W, long J, T *Y, cudaStream_t s,
+                   bool w_trans) {
+    auto run = [&](const GemmDescT<T> &d) {
+        if constexpr (sizeof(T) == 8) return gemm_simt_f64(d, s);
+        else return gemm_simt(d, s);
+    };
     ModeView v = mode_view(order, dims, mode);
-    GemmDesc d;
+    GemmDescT<T> d;
     if (v.P == 1) {
         d.M = J; d.N = v.S; d.Kin = v.Q;
         d.A = W;
@@ -38,27 +43,39 @@ int mode_product(const float *X, int order, const long *dims, int mode, const fl
         d.B = X; d.b_kin = 1; d.b_n = v.Q;
         d.C = Y; d.c_m = 1; d.c_n = J;
         d.splits = 1;
-        return gemm_simt(d, s);
+        return run(d);
     }
     for (long s0 = 0; s0 < v.S; s0 += 65535) {
         long nb = std::min(65535L, v.S - s0);
-        d = GemmDesc();
+        d = GemmDescT<T>();
         d.M = v.P; d.N = J; d.Kin = v.Q; d.batch = nb;
         d.A = X + s0 * v.P * v.Q; d.a_m = 1; d.a_kin = v.P; d.a_b = v.P * v.Q;
         d.B = W; d.b_b = 0;
         if (w_trans) { d.b_kin = 1; d.b_n = v.Q; } else { d.b_kin = J; d.b_n = 1; }
         d.C = Y + s0 * v.P * J; d.c_m = 1; d.c_n = v.P; d.c_b = v.P * J;
         d.splits = 1;
-        int st = gemm_simt(d, s);
+        int st = run(d);
         if (st) return st;
     }
     return CUD_OK;
 }
 
-// G (Q x Q, FP64) = X_(mode) X_(mode)^T
-int unfold_gram(const float *X, int order, const long *dims, int mode, double *G, cudaStream_t s) {
+int mode_product(const float *X, int order, const long *dims, int mode, const float *W, long J,
+                 float *Y, cudaStream_t s, bool w_trans) {
+    return mode_product_t<float>(X, order, dims, mode, W, J, Y, s, w_trans);
+}
+
+int mode_product_f64(const double *X, int order, const long *dims, int mode, const double *W, long J, double *Y,
+                     cudaStream_t s, bool w_trans) {
+    return mode_product_t<double>(X, order, dims, mode, W, J, Y, s, w_trans);
+}
+
+// G (Q x Q, FP64) = X_(mode) X_(mode)^T; for FP64 X the split-K partials
+// are FP64 as well.
+template <typename T>
+GemmDescT<T> gram_desc(const T *X, int order, const long *dims, int mode, double *G) {
     ModeView v = mode_view(order, dims, mode);
-    GemmDesc d;
+    GemmDescT<T> d;
     d.M = v.Q; d.N = v.Q;
     d.A = X; d.B = X;
     if (v.P == 1) {
@@ -71,8 +88,17 @@ int unfold_gram(const float *X, int order, const long *dims, int mode, double *G
         d.b_n = v.P; d.b_kin = 1; d.b_kout = v.P * v.Q;
     }
     d.C = G; d.c_m = 1; d.c_n = v.Q;
+    return d;
+}
+
+int unfold_gram(const float *X, int order, const long *dims, int mode, double *G, cudaStream_t s) {
+    GemmDesc d = gram_desc<float>(X, order, dims, mode, G);
     d.out_f64 = true;
     return gemm_simt(d, s);
+}
+
+int unfold_gram_f64(const double *X, int order, const long *dims, int mode, double *G, cudaStream_t s) {
+    return gemm_simt_f64(gram_desc<double>(X, order, dims, mode, G), s);
 }
 
 int round_copy(const float *in, float *out, long n, int mode, cudaStream_t s) {

@@ -26,6 +26,7 @@ constexpr int BS = 16;          // block size
 constexpr int M2 = 2 * BS;      // pair submatrix size
 constexpr int NT = 256;
 constexpr long kSpinLimit = 1L << 24;
+constexpr double kInnerTol = 4e-15 * M2;  // relative off-norm at which a pair block counts as diagonal
 
 struct EigArgs {
     double *A;          // n x n, destroyed
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(NT) k_block_jacobi(EigArgs a) {
                     S[e] = (gi < n && gj < n) ? a.A[gi + (long)n * gj] : 0.0;
                 }
                 __syncthreads();
-                inner_jacobi(S, Qs, 4e-15 * M2);
+                inner_jacobi(S, Qs, kInnerTol);
                 double *Qg = a.Q + (long)k * M2 * M2;
                 for (int e = threadIdx.x; e < M2 * M2; e += NT) Qg[e] = Qs[e];
                 __syncthreads();
@@ -337,8 +338,10 @@ int syev_jacobi(double *A, long n, double *W, double *V, int max_sweeps, cudaStr
     a.nb = nb;
     a.max_sweeps = max_sweeps > 0 ? max_sweeps : 40;
     // off(A) can only be driven to the rounding floor of the rotations,
-    // about n * eps relative to ||A||_F
-    a.tol = 4.0 * 2.22e-16 * (double)std::max(16L, n);
+    // about n * eps relative to ||A||_F, and no lower than the pair blocks'
+    // own stop (kInnerTol of each block's norm): with a tighter outer test a
+    // clustered spectrum (a near low-rank Gram) never met it
+    a.tol = std::max(4.0 * 2.22e-16 * (double)std::max(16L, n), kInnerTol);
     CUD_CHECK(cudaMemsetAsync(w + off_bar, 0, 128, s));
     void *args[] = {&a};
     CUD_CHECK(cudaLaunchCooperativeKernel((void *)k_block_jacobi, grid, NT, args, 0, s));

@@ -2,6 +2,7 @@
 // products, unfolding Grams, reconstructions).  64x64 output tile per CTA,
 // 16-deep contraction slices staged through shared memory, 4x4 register tile
 // per thread; optional split of the contraction with an FP64 reduction.
+// The same kernels run on FP32 and FP64 operands (the FP64 Tucker path).
 #include "kernels.cuh"
 
 namespace cud {
@@ -19,10 +20,21 @@ __device__ __forceinline__ Kidx split_k(long kappa, long Kin, bool two_level) {
     return {kappa % Kin, kappa / Kin};
 }
 
-template <bool kTwoLevel>
-__global__ void __launch_bounds__(NT) k_gemm(GemmDesc d, long kchunk, float *part) {
-    __shared__ __align__(16) float As[BK][BM];
-    __shared__ __align__(16) float Bs[BK][BN];
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ void load4(const float *p, float *x) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+}
+__device__ __forceinline__ void load4(const double *p, double *x) {
+    const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+}
+
+template <bool kTwoLevel, typename T>
+__global__ void __launch_bounds__(NT) k_gemm(GemmDescT<T> d, long kchunk, T *part) {
+    __shared__ __align__(16) T As[BK][BM];
+    __shared__ __align__(16) T Bs[BK][BN];
     const int t = threadIdx.x;
     const long m_tiles = (d.M + BM - 1) / BM;
     const long m0 = (blockIdx.x % m_tiles) * BM;
@@ -33,17 +45,17 @@ __global__ void __launch_bounds__(NT) k_gemm(GemmDesc d, long kchunk, float *par
     const long kbeg = (long)z * kchunk;
     const long kend = min(K, kbeg + kchunk);
 
-    const float *A = d.A + b * d.a_b;
-    const float *B = d.B + b * d.b_b;
+    const T *A = d.A + b * d.a_b;
+    const T *B = d.B + b * d.b_b;
     const bool a_mfast = (d.a_m == 1);
     const bool b_nfast = (d.b_n == 1) && (d.b_kin != 1);
 
     const int tx = t & 15, ty = t >> 4;
-    float acc[4][4];
+    T acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+        for (int j = 0; j < 4; j++) acc[i][j] = 0;
 
     for (long k0 = kbeg; k0 < kend; k0 += BK) {
 #pragma unroll
@@ -53,7 +65,7 @@ __global__ void __launch_bounds__(NT) k_gemm(GemmDesc d, long kchunk, float *par
             if (a_mfast) { mm = e % BM; kk = e / BM; }
             else { kk = e % BK; mm = e / BK; }
             long m = m0 + mm, kap = k0 + kk;
-            float v = 0.f;
+            T v = 0;
             if (m < d.M && kap < kend) {
                 Kidx ki = split_k(kap, d.Kin, kTwoLevel);
                 v = A[m * d.a_m + ki.kin * d.a_kin + ki.kout * d.a_kout];
@@ -67,7 +79,7 @@ __global__ void __launch_bounds__(NT) k_gemm(GemmDesc d, long kchunk, float *par
             if (b_nfast) { nn = e % BN; kk = e / BN; }
             else { kk = e % BK; nn = e / BK; }
             long n = n0 + nn, kap = k0 + kk;
-            float v = 0.f;
+            T v = 0;
             if (n < d.N && kap < kend) {
                 Kidx ki = split_k(kap, d.Kin, kTwoLevel);
                 v = B[ki.kin * d.b_kin + ki.kout * d.b_kout + n * d.b_n];
@@ -77,20 +89,20 @@ __global__ void __launch_bounds__(NT) k_gemm(GemmDesc d, long kchunk, float *par
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < BK; kk++) {
-            float4 a = *reinterpret_cast<const float4 *>(&As[kk][tx * 4]);
-            float4 bb = *reinterpret_cast<const float4 *>(&Bs[kk][ty * 4]);
-            float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {bb.x, bb.y, bb.z, bb.w};
+            T av[4], bv[4];
+            load4(&As[kk][tx * 4], av);
+            load4(&Bs[kk][ty * 4], bv);
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+                for (int j = 0; j < 4; j++) acc[i][j] = fma_t(av[i], bv[j], acc[i][j]);
         }
         __syncthreads();
     }
 
     if (part) {
         // partial[z][b][n][m] dense M x N
-        float *P = part + ((long)z * d.batch + b) * d.M * d.N;
+        T *P = part + ((long)z * d.batch + b) * d.M * d.N;
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -99,23 +111,24 @@ __global__ void __launch_bounds__(NT) k_gemm(GemmDesc d, long kchunk, float *par
                 if (m < d.M && n < d.N) P[m + d.M * n] = acc[i][j];
             }
     } else {
-        float *C = static_cast<float *>(d.C) + b * d.c_b;
+        T *C = static_cast<T *>(d.C) + b * d.c_b;
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 long m = m0 + tx * 4 + i, n = n0 + ty * 4 + j;
                 if (m < d.M && n < d.N) {
-                    float *c = C + m * d.c_m + n * d.c_n;
-                    float v = d.alpha * acc[i][j];
-                    if (d.beta != 0.f) v = fmaf(d.beta, *c, v);
+                    T *c = C + m * d.c_m + n * d.c_n;
+                    T v = d.alpha * acc[i][j];
+                    if (d.beta != T(0)) v = fma_t(d.beta, *c, v);
                     *c = v;
                 }
             }
     }
 }
 
-__global__ void k_gemm_reduce(GemmDesc d, int splits, const float *__restrict__ part) {
+template <typename T>
+__global__ void k_gemm_reduce(GemmDescT<T> d, int splits, const T *__restrict__ part) {
     long MN = d.M * d.N;
     long total = MN * d.batch;
     long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -129,18 +142,19 @@ __global__ void k_gemm_reduce(GemmDesc d, int splits, const float *__restrict__ 
         long off = b * d.c_b + m * d.c_m + n * d.c_n;
         if (d.out_f64) {
             double *C = static_cast<double *>(d.C);
-            C[off] = (d.beta != 0.f) ? s + (double)d.beta * C[off] : s;
+            C[off] = (d.beta != T(0)) ? s + (double)d.beta * C[off] : s;
         } else {
-            float *C = static_cast<float *>(d.C);
-            C[off] = (float)((d.beta != 0.f) ? s + (double)d.beta * C[off] : s);
+            T *C = static_cast<T *>(d.C);
+            C[off] = (T)((d.beta != T(0)) ? s + (double)d.beta * C[off] : s);
         }
     }
 }
 
 }  // namespace
 
-int gemm_simt(const GemmDesc &d0, cudaStream_t s) {
-    GemmDesc d = d0;
+template <typename T>
+int gemm_simt_impl(const GemmDescT<T> &d0, cudaStream_t s) {
+    GemmDescT<T> d = d0;
     if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return CUD_OK;
     long K = d.Kin * d.Kout;
     long tiles = ((d.M + BM - 1) / BM) * ((d.N + BN - 1) / BN);
@@ -158,10 +172,10 @@ int gemm_simt(const GemmDesc &d0, cudaStream_t s) {
     splits = (int)((K + kchunk - 1) / kchunk);
     if (splits < 1) splits = 1;
     bool need_part = d.out_f64 || splits > 1;
-    float *part = nullptr;
+    T *part = nullptr;
     if (need_part) {
         int st;
-        part = (float *)scratch(kSlotTmp2, sizeof(float) * (size_t)splits * d.batch * d.M * d.N, &st);
+        part = (T *)scratch(kSlotTmp2, sizeof(T) * (size_t)splits * d.batch * d.M * d.N, &st);
         if (!part) return st;
     }
     if (K == 0) {
@@ -169,25 +183,32 @@ int gemm_simt(const GemmDesc &d0, cudaStream_t s) {
         splits = 1;
         if (!need_part) {
             int st;
-            part = (float *)scratch(kSlotTmp2, sizeof(float) * (size_t)d.batch * d.M * d.N, &st);
+            part = (T *)scratch(kSlotTmp2, sizeof(T) * (size_t)d.batch * d.M * d.N, &st);
             if (!part) return st;
         }
-        CUD_CHECK(cudaMemsetAsync(part, 0, sizeof(float) * (size_t)d.batch * d.M * d.N, s));
-        k_gemm_reduce<<<blocks_for(d.M * d.N * d.batch, 256), 256, 0, s>>>(d, 1, part);
+        CUD_CHECK(cudaMemsetAsync(part, 0, sizeof(T) * (size_t)d.batch * d.M * d.N, s));
+        k_gemm_reduce<T><<<blocks_for(d.M * d.N * d.batch, 256), 256, 0, s>>>(d, 1, part);
         CUD_CHECK_LAUNCH("gemm_simt(K=0)");
         return CUD_OK;
     }
     dim3 grid((unsigned)tiles, (unsigned)d.batch, (unsigned)splits);
     if (d.Kout > 1)
-        k_gemm<true><<<grid, NT, 0, s>>>(d, kchunk, need_part ? part : nullptr);
+        k_gemm<true, T><<<grid, NT, 0, s>>>(d, kchunk, need_part ? part : nullptr);
     else
-        k_gemm<false><<<grid, NT, 0, s>>>(d, kchunk, need_part ? part : nullptr);
+        k_gemm<false, T><<<grid, NT, 0, s>>>(d, kchunk, need_part ? part : nullptr);
     CUD_CHECK_LAUNCH("gemm_simt");
     if (need_part) {
-        k_gemm_reduce<<<blocks_for(d.M * d.N * d.batch, 256), 256, 0, s>>>(d, splits, part);
+        k_gemm_reduce<T><<<blocks_for(d.M * d.N * d.batch, 256), 256, 0, s>>>(d, splits, part);
         CUD_CHECK_LAUNCH("gemm_simt reduce");
     }
     return CUD_OK;
+}
+
+int gemm_simt(const GemmDesc &d, cudaStream_t s) { return gemm_simt_impl<float>(d, s); }
+
+int gemm_simt_f64(const GemmDesc64 &d, cudaStream_t s) {
+    if (d.out_f64) return CUD_ERR_INVALID_ARGUMENT;  // FP64 output is the plain path here
+    return gemm_simt_impl<double>(d, s);
 }
 
 }  // namespace cud

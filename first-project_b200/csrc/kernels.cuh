@@ -12,19 +12,23 @@ namespace cud {
 // `kout` is a second contraction index (it lets a contraction run over two
 // non-adjacent tensor modes).  With out_f64 set, C is double and the partial
 // sums over `splits` chunks of the contraction are reduced in FP64.
-struct GemmDesc {
+template <typename T>
+struct GemmDescT {
     long M = 0, N = 0, Kin = 1, Kout = 1, batch = 1;
-    const float *A = nullptr;
+    const T *A = nullptr;
     long a_m = 0, a_kin = 0, a_kout = 0, a_b = 0;
-    const float *B = nullptr;
+    const T *B = nullptr;
     long b_kin = 0, b_kout = 0, b_n = 0, b_b = 0;
-    void *C = nullptr;
+    void *C = nullptr;             // T, or double when out_f64
     long c_m = 0, c_n = 0, c_b = 0;
-    float alpha = 1.0f, beta = 0.0f;
+    T alpha = 1, beta = 0;
     bool out_f64 = false;
     int splits = 0;  // 0 = choose
 };
+using GemmDesc = GemmDescT<float>;
+using GemmDesc64 = GemmDescT<double>;
 int gemm_simt(const GemmDesc &d, cudaStream_t s);
+int gemm_simt_f64(const GemmDesc64 &d, cudaStream_t s);  // FP64 operands and output
 
 // Residual/norm helper (elementwise.cu).  Synchronises the stream.
 int residual_norms(const float *X, float *X1, long n, int subtract, double *out, cudaStream_t s);
@@ -104,6 +108,10 @@ int mode_product(const float *X, int order, const long *dims, int mode, const fl
                  float *Y, cudaStream_t s, bool w_trans = false);
 // G (dims[mode]^2, FP64) = X_(mode) X_(mode)^T
 int unfold_gram(const float *X, int order, const long *dims, int mode, double *G, cudaStream_t s);
+// The same two on FP64 tensors (the FP64 Tucker path).
+int mode_product_f64(const double *X, int order, const long *dims, int mode, const double *W, long J, double *Y,
+                     cudaStream_t s, bool w_trans = false);
+int unfold_gram_f64(const double *X, int order, const long *dims, int mode, double *G, cudaStream_t s);
 
 // Symmetric eigensolver (eig.cu): A (n x n, FP64, destroyed) -> ascending W, V.
 int syev_jacobi(double *A, long n, double *W, double *V, int max_sweeps, cudaStream_t s);

@@ -113,6 +113,8 @@ _sig("cud_cp_als", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
 _sig("cud_cp_als_f64", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
                         ctypes.POINTER(CpOptions), ctypes.POINTER(CpResult), _vp])
 _sig("cud_mttkrp_f64", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _vp, _vp])
+_sig("cud_tucker_hosvd_f64", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ctypes.POINTER(_vp), _vp])
+_sig("cud_tucker_hooi_f64", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ctypes.POINTER(_vp), _i, _vp])
 _sig("cud_cp_init_curand", [_i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
                             ctypes.c_ulonglong, _vp])
 _sig("cud_cp_plan_create", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
@@ -573,6 +575,22 @@ def tucker_hooi(X, dims, ranks, core, factors, sweeps=10, precision=PREC_FP32, s
                                        _ptr(core), _ptrs(factors), sweeps, precision,
                                        _stream(stream)),
                   "tucker_hooi", allow=(OK, ERR_NOT_CONVERGED))
+
+
+def tucker_hosvd_f64(X, dims, ranks, core, factors, stream=None):
+    """FP64 HOSVD (the reference's dprice/tucker_hosvd.cu, 4_tucker_hosvd.cu)
+    on float64 device tensors."""
+    return _check(_lib.cud_tucker_hosvd_f64(_ptr(X), len(dims), _longs(dims), _longs(ranks),
+                                            _ptr(core), _ptrs(factors), _stream(stream)),
+                  "tucker_hosvd_f64", allow=(OK, ERR_NOT_CONVERGED))
+
+
+def tucker_hooi_f64(X, dims, ranks, core, factors, sweeps=10, stream=None):
+    """FP64 HOOI (the reference's dprice/tucker_hooi.cu) on float64 device
+    tensors."""
+    return _check(_lib.cud_tucker_hooi_f64(_ptr(X), len(dims), _longs(dims), _longs(ranks),
+                                           _ptr(core), _ptrs(factors), sweeps, _stream(stream)),
+                  "tucker_hooi_f64", allow=(OK, ERR_NOT_CONVERGED))
 
 
 # --------------------------------------------------------------------------

@@ -227,6 +227,18 @@ int cud_cp_als_f64(const double *X, int order, const long *dims, long R, double 
 int cud_mttkrp_f64(const double *X, int order, const long *dims, const double *const *U, int mode, long R,
                    double *out, void *stream);
 
+/* The reference's FP64 Tucker programs decomposition/GPU/normal/dprice/
+ * tucker_hosvd.cu:3-167 (order 3), 4_tucker_hosvd.cu:3-173 (order 4) and
+ * tucker_hooi.cu:3-220, as general-order entries over double device
+ * buffers: FP64 unfolding Grams (CUDA-core GEMMs), the FP64 Jacobi
+ * eigensolver (the r_n leading eigenvectors in ascending eigenvalue order,
+ * as syevd returns them) and an FP64 mode-product chain for the core.
+ * Arguments as cud_tucker_hosvd / cud_tucker_hooi, without precision. */
+int cud_tucker_hosvd_f64(const double *X, int order, const long *dims, const long *ranks, double *core,
+                         double *const *U, void *stream);
+int cud_tucker_hooi_f64(const double *X, int order, const long *dims, const long *ranks, double *core,
+                        double *const *U, int sweeps, void *stream);
+
 /* Extension: a reusable CP-ALS plan -- the workspace, the Grams and the
  * captured per-sweep CUDA graph for one (X, dims, R, factors) problem, so
  * sweeps can be enqueued without synchronisation (what cud_cp_als loops

@@ -68,3 +68,36 @@ def test_cp_als_f64_rejects_bad_arguments(cd):
         cd.cp_als_f64(X, (2, 2, 2), 0, U)
     with pytest.raises(cd.CudError):
         cd.cp_als_f64(X, (2, 2, 0), 2, U)
+
+
+def subspace_gap(u, w, d, r):
+    U = u.reshape(d, r, order="F")
+    W = w.reshape(d, r, order="F")
+    return np.linalg.norm(U @ U.T - W @ W.T)
+
+
+@pytest.mark.parametrize("dims,ranks,method", [((30, 26, 22), (4, 5, 3), "hosvd"), ((12, 11, 10, 9), (3, 3, 2, 2), "hosvd"),
+                                               ((30, 26, 22), (4, 5, 3), "hooi"), ((12, 11, 10, 9), (3, 3, 2, 2), "hooi")])
+def test_tucker_f64_matches_oracle(cd, dims, ranks, method):
+    rng = np.random.default_rng(sum(dims))
+    core0 = rng.standard_normal(int(np.prod(ranks)))
+    facs0 = [np.linalg.qr(rng.standard_normal((d, r)))[0].reshape(-1, order="F") for d, r in zip(dims, ranks)]
+    X = oracle.gentucker(core0, ranks, facs0, dims)
+    X = (X + 1e-3 * np.linalg.norm(X) / np.sqrt(X.size) * rng.standard_normal(X.size)).astype(np.float32)
+    core = torch.empty(int(np.prod(ranks)), dtype=torch.float64, device="cuda")
+    U = [torch.empty(d * r, dtype=torch.float64, device="cuda") for d, r in zip(dims, ranks)]
+    if method == "hosvd":
+        st = cd.tucker_hosvd_f64(dev64(X), dims, ranks, core, U)
+        core_or, facs_or = oracle.tucker_hosvd(X, dims, ranks)
+    else:
+        st = cd.tucker_hooi_f64(dev64(X), dims, ranks, core, U, sweeps=3)
+        core_or, facs_or = oracle.tucker_hooi(X, dims, ranks, sweeps=3)
+    torch.cuda.synchronize()
+    assert st == cd.OK
+    for u, w, d, r in zip(U, facs_or, dims, ranks):
+        assert subspace_gap(u.cpu().numpy(), w, d, r) <= 1e-9
+    g = core.cpu().numpy()
+    assert abs(np.linalg.norm(g) - np.linalg.norm(core_or)) <= 1e-10 * np.linalg.norm(core_or)
+    rec = oracle.gentucker(g, ranks, [u.cpu().numpy() for u in U], dims)
+    rec_or = oracle.gentucker(core_or, ranks, facs_or, dims)
+    assert np.linalg.norm(rec - rec_or) <= 1e-9 * np.linalg.norm(rec_or)
