@@ -148,6 +148,18 @@ extern "C" int cud_unfold_gram(const float *X, int order, const long *dims, int 
     return set_status(unfold_gram(X, order, dims, mode, G, as_stream(stream)));
 }
 
+extern "C" int cud_cross_gram(const float *A, const float *B, long P, long ma, long mb, double *G, long ldg,
+                              void *stream) {
+    if (!A || !B || !G || P <= 0 || ma <= 0 || mb <= 0 || ldg < ma) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    GemmDesc d;
+    d.M = ma; d.N = mb; d.Kin = P;
+    d.A = A; d.a_m = P; d.a_kin = 1;
+    d.B = B; d.b_n = P; d.b_kin = 1;
+    d.C = G; d.c_m = 1; d.c_n = ldg;
+    d.out_f64 = true;
+    return set_status(gemm_simt(d, as_stream(stream)));
+}
+
 extern "C" int cud_gencp(float *rec, int order, const long *dims, const float *const *U, long R,
                          void *stream) {
     if (order < 1 || order > kMaxOrder || !dims || !U || !rec || R <= 0)

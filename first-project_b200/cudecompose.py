@@ -106,6 +106,7 @@ _sig("cud_mttkrp", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _v
 _sig("cud_unfold_gram", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _i, _vp])
 _sig("cud_mttkrp_path", [_i, ctypes.POINTER(_l), _i, _l, _i])
 _sig("cud_syev_jacobi", [_vp, _l, _vp, _vp, _i, _vp])
+_sig("cud_cross_gram", [_vp, _vp, _l, _l, _l, _vp, _l, _vp])
 _sig("cud_syev_top", [_vp, _l, _l, _vp, _vp, _i, _vp])
 _sig("cud_cp_default_options", [ctypes.POINTER(CpOptions)], None)
 _sig("cud_cp_als", [_vp, _i, ctypes.POINTER(_l), _l, ctypes.POINTER(_vp),
@@ -313,6 +314,12 @@ def mttkrp_path(dims, mode, R, precision=PREC_DEFAULT) -> str:
 def unfold_gram(X, dims, mode, G, stream=None):
     _check(_lib.cud_unfold_gram(_ptr(X), len(dims), _longs(dims), mode, _ptr(G), 0,
                                 _stream(stream)), "unfold_gram")
+
+
+def cross_gram(A, B, P, ma, mb, G, ldg, stream=None):
+    """G[i + ldg j] = sum_p A[p + P i] B[p + P j] (FP32 in, FP64 out); G may be
+    a view into a larger float64 matrix."""
+    _check(_lib.cud_cross_gram(_ptr(A), _ptr(B), P, ma, mb, _ptr(G), ldg, _stream(stream)), "cross_gram")
 
 
 def syev_jacobi(A, n, W, V, max_sweeps=60, stream=None):

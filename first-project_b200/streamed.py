@@ -17,6 +17,8 @@ cud_cp_fit_terms).
 """
 from __future__ import annotations
 
+import numpy as np
+
 from distributed import CudaOps, ShardedCP
 
 
@@ -60,14 +62,14 @@ class StreamedOps(CudaOps):
             self.copied = [torch.cuda.Event() for _ in range(self.nbuf)]
             self.used = [None] * self.nbuf
 
-    def _stream_slabs(self, Xh, dims, body):
+    def _stream_slabs(self, Xh, dims, body, first=0):
         """Calls body(s, k0, k1, slab_tensor) on the compute stream for every
-        slab, with the copies overlapped."""
+        slab from `first` on, with the copies overlapped."""
         torch = self.torch
         P = 1
         for d in dims[:-1]:
             P *= int(d)
-        ranges = slab_ranges(int(dims[-1]), self.slab)
+        ranges = slab_ranges(int(dims[-1]), self.slab)[first:]
         self._buffers(P * min(self.slab, int(dims[-1])))
 
         def issue(s):
@@ -88,7 +90,7 @@ class StreamedOps(CudaOps):
             b = s % self.nbuf
             with torch.cuda.stream(self.compute):
                 self.compute.wait_event(self.copied[b])
-                body(s, k0, k1, self.bufs[b][: (k1 - k0) * P])
+                body(first + s, k0, k1, self.bufs[b][: (k1 - k0) * P])
                 ev = torch.cuda.Event()
                 ev.record(self.compute)
                 self.used[b] = ev
@@ -154,3 +156,102 @@ class StreamedCP(ShardedCP):
     @property
     def h2d_bytes(self):
         return self.ops.h2d_bytes
+
+
+class StreamedTucker:
+    """Tucker HOSVD of a host-resident tensor, streamed slab by slab along
+    the last mode (decomposition/GPU/large/slice_tucker_hosvd.cu:3-160):
+
+    * the Grams of the modes n < N-1 are sums of the slabs' unfolding Grams
+      (:36-37), accumulated in FP64 in slab order;
+    * the last mode's Gram pairs every slab with every other (:38-40 pairs
+      every frontal slice): one pass gives the diagonal blocks, then for
+      each slab s a copy is held on the device while the slabs t > s
+      stream past, giving the blocks (s, t) and (t, s) (cud_cross_gram);
+    * the factors are the leading eigenvectors of each FP64 Gram (full
+      Jacobi, ascending order, as syevdx returns them);
+    * the core is the sum over slabs of the slab projected on every factor,
+      the last one restricted to the slab's rows (:98-104).
+
+    FP32 data and CUDA-core contractions, like the reference's slice path.
+    Host traffic: the tensor once for the leading Grams, about p^2 / 2 slabs
+    for the last mode's Gram (p slabs), once for the core."""
+
+    def __init__(self, cd, X_host, dims, slab, nbuf=2, stream=None):
+        self.cd, self.Xh, self.dims = cd, X_host, [int(d) for d in dims]
+        self.ops = StreamedOps(cd, cd.PREC_FP32, slab, nbuf=nbuf, stream=stream)
+        self.ops.dims = self.dims
+
+    @property
+    def h2d_bytes(self):
+        return self.ops.h2d_bytes
+
+    def hosvd(self, ranks, core, factors):
+        """core (prod ranks, FP32) and factors[m] (dims[m] x ranks[m], FP32,
+        column-major) are device tensors, written in place.  Returns the
+        worst eigensolver status."""
+        import torch
+        cd, ops, dims = self.cd, self.ops, self.dims
+        N = len(dims)
+        last = dims[-1]
+        P = 1
+        for d in dims[:-1]:
+            P *= d
+        ranges = slab_ranges(last, ops.slab)
+        worst = cd.OK
+        with torch.cuda.stream(ops.compute):
+            G = [torch.zeros(d * d, dtype=torch.float64, device="cuda") for d in dims]
+            tmp = torch.empty(max([d * d for d in dims[:-1]] + [1]), dtype=torch.float64, device="cuda")
+            held = torch.empty(P * min(ops.slab, last), device="cuda")
+
+            def leading(s, k0, k1, Xs):
+                sd = dims[:-1] + [k1 - k0]
+                for n in range(N - 1):
+                    cd.unfold_gram(Xs, sd, n, tmp[: dims[n] * dims[n]], stream=ops.stream)
+                    G[n].add_(tmp[: dims[n] * dims[n]])
+                cd.cross_gram(Xs, Xs, P, k1 - k0, k1 - k0, G[-1][k0 + last * k0:], last, stream=ops.stream)
+
+            ops._stream_slabs(self.Xh, dims, leading)
+            for s, (k0, k1) in enumerate(ranges[:-1]):
+                ks = k1 - k0
+                hs = held[: ks * P]
+                hs.copy_(self.Xh[k0 * P: k1 * P], non_blocking=True)  # on the compute stream
+                ops.h2d_bytes += 4 * ks * P
+
+                def cross(t, t0, t1, Xt, k0=k0, ks=ks, hs=hs):
+                    kt = t1 - t0
+                    cd.cross_gram(hs, Xt, P, ks, kt, G[-1][k0 + last * t0:], last, stream=ops.stream)
+                    cd.cross_gram(Xt, hs, P, kt, ks, G[-1][t0 + last * k0:], last, stream=ops.stream)
+
+                ops._stream_slabs(self.Xh, dims, cross, first=s + 1)
+            for n in range(N):
+                W = torch.empty(dims[n], dtype=torch.float64, device="cuda")
+                V = torch.empty(dims[n] * dims[n], dtype=torch.float64, device="cuda")
+                st = cd.syev_jacobi(G[n], dims[n], W, V, stream=ops.stream)
+                if st != cd.OK:
+                    worst = st
+                r = int(ranks[n])
+                # column-major V: its last r columns are rows n - r .. n - 1 of V.view(n, n)
+                factors[n].copy_(V.view(dims[n], dims[n])[dims[n] - r:, :].reshape(-1).float())
+            core.zero_()
+            # W_m = U_m^T (r_m x d_m, column-major) for the projections
+            Wt = [factors[m].view(int(ranks[m]), dims[m]).t().contiguous().view(-1) for m in range(N - 1)]
+
+            def project(s, k0, k1, Xs):
+                cur = dims[:-1] + [k1 - k0]
+                Y = Xs
+                for m in range(N - 1):
+                    out = list(cur)
+                    out[m] = int(ranks[m])
+                    Z = torch.empty(int(np.prod(out)), device="cuda")
+                    cd.mode_product(Y, cur, m, Wt[m], int(ranks[m]), Z, stream=ops.stream)
+                    Y, cur = Z, out
+                rl = int(ranks[-1])
+                Wl = factors[-1].view(rl, last)[:, k0:k1].t().contiguous().view(-1)
+                Z = torch.empty(core.numel(), device="cuda")
+                cd.mode_product(Y, cur, N - 1, Wl, rl, Z, stream=ops.stream)
+                core.add_(Z)
+
+            ops._stream_slabs(self.Xh, dims, project)
+        ops.compute.synchronize()
+        return worst

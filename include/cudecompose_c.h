@@ -156,6 +156,13 @@ int cud_mttkrp_path(int order, const long *dims, int mode, long R, int precision
 int cud_unfold_gram(const float *X, int order, const long *dims, int mode, double *G,
                     int precision, void *stream);
 
+/* Extension (the slice-pair SGEMMs of the reference's out-of-core HOSVD,
+ * decomposition/GPU/large/slice_tucker_hosvd.cu:38-40): a block of a Gram
+ * between two column sets, G[i + ldg j] = sum_p A[p + P i] B[p + P j] for
+ * i < ma, j < mb, FP32 operands (column-major, P rows), FP64 output. */
+int cud_cross_gram(const float *A, const float *B, long P, long ma, long mb, double *G, long ldg,
+                   void *stream);
+
 /* ---- symmetric eigensolver / small solves ------------------------------ */
 
 /* Extension (replaces cusolverDnSsyevdx at src/tucker_hosvd.cu:43-61):

@@ -56,3 +56,39 @@ def test_streamed_order4_last_mode_rows(cd):
     torch.cuda.synchronize()
     for m in range(4):
         assert rel(sc.U[m], ref.U[m]) <= 1e-4, m
+
+
+def _gap(u, w, d, r):
+    U = u.cpu().numpy().reshape(d, r, order="F").astype(np.float64)
+    W = w.cpu().numpy().reshape(d, r, order="F").astype(np.float64)
+    return np.linalg.norm(U @ U.T - W @ W.T)
+
+
+@pytest.mark.parametrize("dims,ranks,slab", [((24, 20, 30), (4, 3, 5), 7), ((10, 9, 8, 11), (3, 2, 2, 3), 4)])
+def test_streamed_hosvd_matches_in_core(cd, dims, ranks, slab):
+    """Out-of-core HOSVD (decomposition/GPU/large/slice_tucker_hosvd.cu)
+    against the device-resident FP32 HOSVD: same factor subspaces and core."""
+    X, _, _ = cd.make_tucker_tensor(dims, ranks, seed=9)
+    n = int(np.prod(ranks))
+    core = torch.empty(n, device="cuda")
+    U = [torch.empty(d * r, device="cuda") for d, r in zip(dims, ranks)]
+    cd.tucker_hosvd(X, dims, ranks, core, U, precision=cd.PREC_FP32)
+    st = streamed.StreamedTucker(cd, X.cpu().pin_memory(), dims, slab)
+    core2 = torch.empty(n, device="cuda")
+    U2 = [torch.empty(d * r, device="cuda") for d, r in zip(dims, ranks)]
+    assert st.hosvd(ranks, core2, U2) == cd.OK
+    torch.cuda.synchronize()
+    for u, w, d, r in zip(U2, U, dims, ranks):
+        assert _gap(u, w, d, r) <= 1e-5
+    rec = torch.empty(X.numel(), device="cuda")
+    rec2 = torch.empty(X.numel(), device="cuda")
+    cd.gentucker(rec, core, U, dims, ranks)
+    cd.gentucker(rec2, core2, U2, dims, ranks)
+    torch.cuda.synchronize()
+    assert rel(rec2, rec) <= 1e-5
+    # host traffic: the tensor for the leading Grams and for the core, and
+    # each slab s held once plus the later slabs streamed past it
+    P = int(np.prod(dims[:-1]))
+    r = streamed.slab_ranges(dims[-1], slab)
+    pairs = sum((k1 - k0) + sum(t1 - t0 for t0, t1 in r[s + 1:]) for s, (k0, k1) in enumerate(r[:-1]))
+    assert st.h2d_bytes == 4 * P * (2 * dims[-1] + pairs)
