@@ -1083,7 +1083,7 @@ __global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict
     const long n = Q * Rp;
     double sum = 0.0;
     if (e < n) {
-#pragma unroll 4
+#pragma unroll 16
         for (int z = zl; z < splits; z += 8) sum += (double)__ldcs(part + (long)z * n + e);
     }
     red[zl][o] = sum;
