@@ -82,6 +82,28 @@ def test_status_side_channel_without_gpu():
     assert lib.cud_get_last_error() == 0
 
 
+def test_extended_entry_points_validate_without_gpu():
+    """The FP64 programs, the subspace eigensolver and the cross-Gram block
+    reject bad arguments on the host, before any device work."""
+    lib = ctypes.CDLL(SO)
+    vp, L, I = ctypes.c_void_p, ctypes.c_long, ctypes.c_int
+    dims = (ctypes.c_long * 3)(4, 4, 4)
+    ranks = (ctypes.c_long * 3)(2, 2, 5)  # rank 5 > extent 4
+    lib.cud_syev_top.argtypes = [vp, L, L, vp, vp, I, vp]
+    assert lib.cud_syev_top(None, 8, 2, None, None, 10, None) == 1   # null G, U
+    lib.cud_cross_gram.argtypes = [vp, vp, L, L, L, vp, L, vp]
+    assert lib.cud_cross_gram(None, None, 4, 2, 2, None, 2, None) == 1
+    lib.cud_cp_als_f64.argtypes = [vp, I, vp, L, vp, vp, vp, vp]
+    assert lib.cud_cp_als_f64(None, 3, dims, 2, None, None, None, None) == 1
+    lib.cud_mttkrp_f64.argtypes = [vp, I, vp, vp, I, L, vp, vp]
+    assert lib.cud_mttkrp_f64(None, 3, dims, None, 3, 2, None, None) == 1  # mode out of range
+    lib.cud_tucker_hosvd_f64.argtypes = [vp, I, vp, vp, vp, vp, vp]
+    assert lib.cud_tucker_hosvd_f64(None, 3, dims, ranks, None, None, None) == 1
+    lib.cud_tucker_hooi_f64.argtypes = [vp, I, vp, vp, vp, vp, I, vp]
+    assert lib.cud_tucker_hooi_f64(None, 3, dims, ranks, None, None, 2, None) == 1
+    assert lib.cud_get_last_error() == 1
+
+
 def test_python_mirror_imports(cd):
     assert os.path.samefile(cd.LIB_PATH, SO)
     opt = cd.cp_default_options()
