@@ -108,3 +108,94 @@ def test_skinny_gemm_shared_memory_fits():
     kblocks = 1024 // GBK
     smem = 1024 + 1024 + kblocks * SK_BN * GBK * 2 + SK_ST * GBM * GBK * 2
     assert smem <= 232448
+
+
+# ---- mttkrp_tc.cu pre-packed-B path: launch plan, stage split, segments, B pack
+BQ, BKS, SEG, PB_RING, NSM = 128, 32, 16, 6, 148
+X_STAGE, PB_CTRL = BQ * BKS * 4, 2048
+
+
+def b_tile_bytes(rpad):
+    return rpad * BKS * 2
+
+
+def pb_plan(dims, mode, R):
+    P = int(np.prod(dims[:mode])) if mode else 1
+    Q = dims[mode]
+    S = int(np.prod(dims[mode + 1:]))
+    kind0 = mode == 0
+    rpad = max(16, -(-R // 16) * 16)
+    psteps = 1 if kind0 else -(-P // BKS)
+    stages = -(-S // BKS) if kind0 else S * psteps
+    qtiles = -(-Q // BQ)
+    rows0 = dims[1] if kind0 else dims[0]
+    assert rows0 % BKS == 0 and rows0 // BKS >= 2     # the pre-packed path
+    blk = rows0 // BKS
+    smem = lambda n: 1024 + PB_CTRL + n * (X_STAGE + 2 * b_tile_bytes(rpad))
+    cps = nring = 0
+    for n in range(PB_RING, 2, -1):
+        if smem(n) <= 115712 and 2 * rpad + 32 * n <= 256:
+            cps, nring = 2, n
+            break
+    if not cps:
+        for n in range(PB_RING, 2, -1):
+            if smem(n) <= 232448 and 2 * rpad + 32 * n <= 512:
+                cps, nring = 1, n
+                break
+    want = max(1, (cps * NSM - 2) // qtiles)
+    splits = min(want, stages)
+    chunk = -(-stages // splits)
+    splits = -(-stages // chunk)
+    return dict(stages=stages, qtiles=qtiles, blk=blk, rpad=rpad, rows0=rows0, cps=cps, nring=nring,
+                splits=splits, chunk=chunk, smem=smem(nring))
+
+
+def segments(beg, end, blk):
+    pos, out, cur = beg % blk, [], 0
+    for i in range(end - beg):
+        cur += 1
+        stop = pos == blk - 1 or (pos & (SEG - 1)) == SEG - 1 or i == end - beg - 1
+        pos = 0 if pos + 1 == blk else pos + 1
+        if stop:
+            out.append((beg + i - cur + 1, cur))
+            cur = 0
+    return out
+
+
+@pytest.mark.parametrize("dims,R", [((512, 512, 512), 64), ((384, 384, 384), 64), ((96, 96, 96, 96), 32),
+                                    ((512, 512, 512), 16), ((256, 160, 96), 128)])
+def test_mttkrp_pb_plan_partitions_stages(dims, R):
+    for mode in range(len(dims)):
+        p = pb_plan(dims, mode, R)
+        assert p["cps"] in (1, 2) and p["nring"] >= 3
+        assert p["smem"] <= (115712 if p["cps"] == 2 else 232448)
+        assert p["qtiles"] * p["splits"] <= p["cps"] * NSM          # one wave
+        assert (p["splits"] - 1) * p["chunk"] < p["stages"] <= p["splits"] * p["chunk"]
+        blk = p["blk"]
+        covered = 0
+        for z in range(p["splits"]):
+            beg, end = z * p["chunk"], min(p["stages"], (z + 1) * p["chunk"])
+            for s0, n in segments(beg, end, blk):
+                assert 1 <= n <= SEG
+                assert s0 // blk == (s0 + n - 1) // blk           # never across a constant-row block
+            covered += end - beg
+        assert covered == p["stages"]
+
+
+@pytest.mark.parametrize("rows0,R", [(512, 64), (96, 32), (64, 128), (512, 5)])
+def test_mttkrp_pack_b_in_bounds(rows0, R):
+    rpad = max(16, -(-R // 16) * 16)
+    blk = rows0 // BKS
+    bbytes = b_tile_bytes(rpad)
+    n = blk * 4 * rpad
+    ids = np.arange(n)
+    t = ids // (4 * rpad)
+    rem = ids - t * 4 * rpad
+    kc, r = rem // rpad, rem % rpad
+    row_max = (32 * t + 8 * kc + 7)[r < R].max()
+    assert row_max < rows0                                       # U0 rows read
+    off = r * 16 + kc * rpad * 16
+    assert (off + 16).max() <= bbytes                            # inside each hi / lo half
+    assert ((t * 2 + 1) * bbytes + off + 16).max() <= blk * 2 * bbytes   # inside the packed buffer
+    # each 16-byte chunk of every tile half written exactly once
+    assert len(np.unique(t * bbytes * 2 + off)) == n
