@@ -22,6 +22,7 @@
 // height come from a small autotuner
 // (batched_tune) that times one sweep per candidate on the batch itself and
 // caches the winner per batch shape class.
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -442,13 +443,13 @@ struct BatchState {
 
 template <int NT, int RT>
 int launch_sweep(const BatchArgs &a, int ctas_per_sm, cudaStream_t s) {
-    static bool attr[64] = {false};
+    static std::atomic<bool> attr[64];  // per device; zero-initialised
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !attr[dev]) {
+    if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
         CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NT, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(BatchSmem)));
-        attr[dev] = true;
+        attr[dev].store(true, std::memory_order_release);
     }
     CUD_CHECK(cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s));
     k_batch_sweep<NT, RT><<<kNumSMs * ctas_per_sm, NT, sizeof(BatchSmem), s>>>(a);

@@ -2,12 +2,12 @@
 // and the one-shot cud_cp_als built on it.
 //
 // One sweep = for each mode n: MTTKRP_n (native layout) -> V^-1 from the
-// Hadamard product of the other factors' FP64 Grams (Cholesky, pinv
-// fallback) -> U_n = M V^-1 -> Gram of U_n; then the fit from the identity
+// Hadamard product of the other factors' FP64 Grams (Gauss-Jordan inverse
+// with SPD pivots, Jacobi pseudo-inverse fallback) -> U_n = M V^-1 -> Gram of U_n; then the fit from the identity
 // ||X - Xhat||^2 = ||X||^2 - 2 <M_N, U_N> + sum prod_m G_m.  The sweep is
 // captured once into a CUDA graph and replayed; the plan owns every buffer
 // the graph touches.  Mirrors the update order and equations of
-// src/cp_als.cu:44-119 and src/cp4_als.cu:198-307, without their per-sweep
+// src/cp_als.cu:44-119 and src/cp4_als.cu:64-164, without their per-sweep
 // allocations and device synchronisations.
 #include <vector>
 #include <curand.h>

@@ -15,6 +15,7 @@
 // gridDim.z and a second kernel sums the FP32 partials in a fixed order and
 // applies the same epilogue.  Every wait is bounded (abort flag, drained
 // copies, TMEM freed, error flag set).
+#include <atomic>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -436,13 +437,13 @@ bool skinny_ok(long M, long N, long K) {
 
 template <int BN>
 int launch_gemm(const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &g, dim3 grid, cudaStream_t s) {
-    static bool attr[64] = {false};
+    static std::atomic<bool> attr[64];  // per device; zero-initialised
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !attr[dev]) {
+    if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
         CUD_CHECK(cudaFuncSetAttribute(k_gemm_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)gemm_smem_bytes(BN)));
-        attr[dev] = true;
+        attr[dev].store(true, std::memory_order_release);
     }
     k_gemm_tc<BN><<<grid, GTHREADS, gemm_smem_bytes(BN), s>>>(ta, tb, g);
     CUD_CHECK_LAUNCH("gemm_tc");
@@ -479,13 +480,13 @@ int gemm_tc_bf16(const __nv_bfloat16 *A, long lda, const __nv_bfloat16 *B, long 
         CUD_CHECK(cudaMemsetAsync(g.error, 0, sizeof(int), s));
         const long mt = (M + GBM - 1) / GBM;
         const size_t smem = sk_smem_bytes(g.kblocks);
-        static bool attr[64] = {false};
+        static std::atomic<bool> attr[64];  // per device; zero-initialised
         int dev = 0;
         CUD_CHECK(cudaGetDevice(&dev));
-        if (dev >= 0 && dev < 64 && !attr[dev]) {
+        if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
             CUD_CHECK(cudaFuncSetAttribute(k_gemm_skinny, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)sk_smem_bytes(SK_KMAX / GBK)));
-            attr[dev] = true;
+            attr[dev].store(true, std::memory_order_release);
         }
         k_gemm_skinny<<<(unsigned)std::min<long>(mt, kNumSMs), GTHREADS, smem, s>>>(ta, tb, g, mt);
         CUD_CHECK_LAUNCH("gemm_tc skinny");

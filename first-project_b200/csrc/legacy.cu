@@ -119,7 +119,7 @@ void cp_als4(dt *d_X, dt *d_A, dt *d_B, dt *d_C, dt *d_D, long a, long b, long c
     cud_cp_result res;
     int st = cud_cp_als(d_X, 4, dims, r, U, &opt, &res, nullptr);
     sync_after(st);
-    if (st == CUD_OK) print_error(res.fit);  // src/cp4_als.cu:288-296 prints the error
+    if (st == CUD_OK) print_error(res.fit);  // src/cp4_als.cu:154-162 prints the error
 }
 
 void cp_tensorcore(dt *d_X, dt *d_A, dt *d_B, dt *d_C, long a, long b, long c, long r) {

@@ -1,8 +1,10 @@
 // cud_mttkrp_noalloc: the MTTKRP entry point for callers that cannot allocate
 // device memory -- code running where cudaMalloc is forbidden or unsafe, such
-// as inside a host callback, a custom allocator's own hooks, or a process
-// whose device memory is entirely owned and pre-carved by its host
-// framework.  The regular cud_mttkrp draws its split-contraction workspace
+// as inside a custom allocator's own hooks (a cudaMalloc there re-enters the
+// allocator), or a process whose device memory is entirely owned and
+// pre-carved by its host framework.  The call launches kernels on the
+// caller's stream, so it is not for stream callbacks (cudaLaunchHostFunc),
+// where CUDA forbids API calls.  The regular cud_mttkrp draws its split-contraction workspace
 // from a growing per-device arena (cudaMalloc on first use or growth); this
 // variant runs the same kernels with the workspace taken from a fixed
 // file-scope __device__ array instead, and calls no allocating routine.
@@ -12,7 +14,11 @@
 //    (split partials: splits x R x I_mode floats, plus 256 bytes of flags)
 //    would not fit is rejected with CUD_ERR_INVALID_ARGUMENT and a message
 //    from cud_last_error_detail();
-//  * every GPU that loads the library holds the array until process exit;
+//  * every GPU that loads this module holds the array until process exit;
+//    under lazy module loading (CUDA_MODULE_LOADING=LAZY, the CUDA 12.2+
+//    default) the module -- and with it the 32 MiB -- is loaded by the first
+//    call on a device, so that call belongs at start-up, while the memory is
+//    free;
 //  * all calls on a device share the one array, which keeps the last call's
 //    contents -- each call rewrites everything it reads (the kernels
 //    overwrite every partial and clear their error flag), but calls whose

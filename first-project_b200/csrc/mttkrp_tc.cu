@@ -37,6 +37,7 @@
 // Every wait is bounded: an expired wait raises a CTA-wide abort flag, the
 // roles drain and the TMEM is freed before the CTA exits, and the kernel's
 // error flag is set (the reduce then writes NaN).
+#include <atomic>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -1193,8 +1194,12 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     p.fast = (rows0 % BKS == 0);
     p.blk = p.fast ? rows0 / BKS : 1;
     // pre-packed B path: blocks of at least 2 stages (each segment flush
-    // adds a whole 128 x R partial tile, at least every other stage)
-    p.pb = p.fast && p.blk >= 2;
+    // adds a whole 128 x R partial tile, at least every other stage).  Not
+    // for FP16: the public mttkrp rounds each whole Khatri-Rao entry,
+    // fp16(U0[x] * c[y]) (src/mttkrp.cu:21-25, 41-47, 65-69), while the
+    // packed tiles hold fp16(U0[x]) and apply c in FP32 at the flush; the
+    // Khatri-Rao-building kernel forms the product first and rounds it once.
+    p.pb = p.fast && p.blk >= 2 && precision != CUD_PREC_FP16;
 #ifdef CUD_TC_NO_PB
     p.pb = false;
 #endif
@@ -1213,13 +1218,13 @@ size_t tc_pb_bytes(const TcPlan &p) { return p.pb ? (size_t)p.blk * 2 * b_tile_b
 template <int KIPT, int CIPT, int MINB>
 int launch_tc(const CUtensorMap &tmap, const CUtensorMap &umap, const TcArgs &a, size_t smem, unsigned grid,
               cudaStream_t s) {
-    static bool attr[64] = {false};
+    static std::atomic<bool> attr[64];  // per device; zero-initialised
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !attr[dev]) {
+    if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
         CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_tc<KIPT, CIPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        232448));
-        attr[dev] = true;
+        attr[dev].store(true, std::memory_order_release);
     }
     k_mttkrp_tc<KIPT, CIPT, MINB><<<grid, NTHREADS, smem, s>>>(tmap, umap, a);
     CUD_CHECK_LAUNCH("mttkrp_tc");
@@ -1228,12 +1233,12 @@ int launch_tc(const CUtensorMap &tmap, const CUtensorMap &umap, const TcArgs &a,
 
 template <int MINB>
 int launch_pb(const CUtensorMap &tmap, const TcArgs &a, size_t smem, unsigned grid, cudaStream_t s) {
-    static bool attr[64] = {false};
+    static std::atomic<bool> attr[64];  // per device; zero-initialised
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !attr[dev]) {
+    if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
         CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_pb<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
-        attr[dev] = true;
+        attr[dev].store(true, std::memory_order_release);
     }
     k_mttkrp_pb<MINB><<<grid, PB_THREADS, smem, s>>>(tmap, a);
     CUD_CHECK_LAUNCH("mttkrp_pb");

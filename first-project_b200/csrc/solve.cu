@@ -1,8 +1,10 @@
 // The R x R side of CP-ALS, all in FP64 on the device: factor Grams, the
-// Hadamard product of Grams, Cholesky factorisation and inverse with a
-// pseudo-inverse (Jacobi eigen) fallback, the factor update U_n = M V^-1, and
+// Hadamard product of Grams, its inverse by Gauss-Jordan elimination with
+// symmetric positive pivots (a pseudo-inverse by Jacobi eigen when a pivot is
+// not positive), the factor update U_n = M V^-1, and
 // the fit from the Gram/MTTKRP identity.  Replaces the FP32 getrf/getrs +
 // geam sequence of src/cp_als.cu:53-63 (and :73-82, :92-101).
+#include <atomic>
 #include "kernels.cuh"
 #include "solve.cuh"
 
@@ -510,13 +512,13 @@ int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s) {
 }
 
 int normal_inverse_prepare() {
-    static bool attr_set[64] = {false};
+    static std::atomic<bool> attr_set[64];  // per device; zero-initialised
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (dev >= 0 && dev < 64 && !attr_set[dev].load(std::memory_order_acquire)) {
         CUD_CHECK(cudaFuncSetAttribute(k_normal_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(double) * 160 * 160)));
-        attr_set[dev] = true;
+        attr_set[dev].store(true, std::memory_order_release);
     }
     return CUD_OK;
 }

@@ -13,7 +13,8 @@
  * caller's buffers (src/tensorcore_cp.cu:136-139), cp_als4 does not reset
  * the device (src/cp4_als.cu:184), tucker_tensorcore writes U1..U3
  * (src/tucker_tensorcore.cu:84-108 leaves them unwritten), and the
- * normal-equation solve is FP64 Cholesky rather than FP32 LU.
+ * normal-equation solve is an FP64 Gauss-Jordan inverse with SPD pivots (a
+ * Jacobi pseudo-inverse when a pivot is not positive) rather than FP32 LU.
  */
 #ifndef GUARD_cudecompose_h
 #define GUARD_cudecompose_h

@@ -128,21 +128,25 @@ int cud_mttkrp_legacy(const float *X, const float *left, const float *right, flo
                       long flag, long m, long n, long k, long r, int precision, void *stream);
 
 /* The FP32 MTTKRPs inside src/cp_als.cu:46-52,66-69,85-88 and
- * src/cp4_als.cu:201-207,225-230,246-251,269-272, any order, native layout:
+ * src/cp4_als.cu:67-73,91-96,112-117,135-138, any order, native layout:
  * out (dims[mode] x R) = X_(mode) * (KR of the other factors), with no
  * unfolding or Khatri-Rao matrix materialised. */
 int cud_mttkrp(const float *X, int order, const long *dims, const float *const *U, int mode,
                long R, float *out, int precision, void *stream);
 
 /* No counterpart in the reference.  cud_mttkrp for callers that cannot
- * allocate device memory (code running inside host callbacks or allocator
- * hooks, or under a framework that owns all device memory): same arguments,
- * kernels and results, but its workspace is a fixed 32 MiB __device__ array
- * inside the library, so it calls no cudaMalloc/cudaFree.  A call needing
- * more workspace is rejected (CUD_ERR_INVALID_ARGUMENT, message in
+ * allocate device memory (code inside a custom allocator's own hooks, where
+ * cudaMalloc would re-enter the allocator, or under a framework that owns
+ * all device memory): same arguments, kernels and results, but its
+ * workspace is a fixed 32 MiB __device__ array inside the library, so it
+ * calls no cudaMalloc/cudaFree.  It launches kernels on `stream`, so it must
+ * not run inside a stream callback (CUDA forbids API calls there).  A call
+ * needing more workspace is rejected (CUD_ERR_INVALID_ARGUMENT, message in
  * cud_last_error_detail).  All calls on a device share the array: calls that
  * overlap on the GPU race and must be serialised by the caller.  The first
- * call on a device resolves the array's address; make it before any stream
+ * call on a device loads the array's module (under lazy module loading, the
+ * CUDA 12.2+ default, that commits the 32 MiB then) and resolves its
+ * address: make it at start-up, with the memory free, and before any stream
  * capture. */
 int cud_mttkrp_noalloc(const float *X, int order, const long *dims, const float *const *U,
                        int mode, long R, float *out, int precision, void *stream);
@@ -213,8 +217,9 @@ void cud_cp_default_options(cud_cp_options *opt);
 /* src/cp_als.cu:3-134 (order 3) and src/cp4_als.cu:3-186 (order 4) as one
  * general-order entry: CP-ALS from the initial factors U (host array of
  * device pointers, U[m] is dims[m] x R, updated in place).  Update order
- * U[0], U[1], ...; normal equations (Hadamard of FP64 Grams) solved by FP64
- * Cholesky with a pseudo-inverse fallback.  res may be NULL. */
+ * U[0], U[1], ...; normal equations (Hadamard of FP64 Grams) solved by an
+ * FP64 Gauss-Jordan inverse with SPD pivots, with a Jacobi pseudo-inverse
+ * fallback.  res may be NULL. */
 int cud_cp_als(const float *X, int order, const long *dims, long R, float *const *U,
                const cud_cp_options *opt, cud_cp_result *res, void *stream);
 
@@ -269,7 +274,7 @@ int cud_cp_plan_destroy(cud_cp_plan plan);
  * G = U^T U (R x R, FP64) for U (I x R). */
 int cud_factor_gram(const float *U, long I, long R, double *G, void *stream);
 /* U (I x R) = M (I x R) * V^-1 with V = Hadamard_{m != mode} G[m] (FP64
- * Cholesky, pseudo-inverse fallback).  G is a host array of `order` device
+ * Gauss-Jordan with SPD pivots, Jacobi pseudo-inverse fallback).  G is a host array of `order` device
  * pointers (R x R each); work holds 3 R^2 doubles + 16 bytes. */
 int cud_cp_solve(const float *M, long I, long R, int order, const double *const *G, int mode,
                  float *U, double *work, void *stream);

@@ -376,7 +376,7 @@ int or_lu_solve(double *S, long R, double *Bt, long nrhs) {
     return info;
 }
 
-/* CP-ALS of src/cp_als.cu:44-119 (3rd order) and src/cp4_als.cu:198-307
+/* CP-ALS of src/cp_als.cu:44-119 (3rd order) and src/cp4_als.cu:64-164
  * (4th order), generalised to any order: for n = 0..order-1 in turn,
  *   V = Hadamard_{m != n} (U_m^T U_m),  M = MTTKRP_n,  U_n = M V^{-1}
  * with the solve by LU (use_lu=1, the reference's getrf/getrs) or by

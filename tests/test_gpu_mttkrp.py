@@ -96,6 +96,29 @@ def test_legacy_fp16_semantics_random(cd):
         assert rel(got, want) <= 1e-6
 
 
+@pytest.mark.parametrize("dims,R", [((128, 96, 64), 16), ((64, 256, 96), 32)])
+def test_fp16_rounds_whole_khatri_rao_entry(cd, dims, R):
+    """FP16 at shapes whose fastest generating factor has a multiple of 32
+    rows (>= 64): the tensor-core path must still round fp16(U0[x] * c[y]),
+    the whole Khatri-Rao entry, as src/mttkrp.cu:21-25 does."""
+    rng = np.random.default_rng(sum(dims) + R)
+    X = rng.random(int(np.prod(dims))).astype(np.float32)
+    facs = [rng.random(d * R).astype(np.float32) for d in dims]
+    # mttkrp() flag f: (left, right) = the two other factors, slower first
+    m, n, k = dims
+    A, B, C = facs
+    out = torch.empty(max(dims) * R, device="cuda")
+    for flag, (left, right) in ((1, (C, B)), (2, (C, A)), (3, (B, A))):
+        cd.mttkrp_legacy(dev_t(X), dev_t(left), dev_t(right), out, flag, m, n, k, R)
+        torch.cuda.synchronize()
+        q = dims[flag - 1]
+        got = out[: q * R].cpu().numpy().astype(np.float64)
+        want = oracle.mttkrp_legacy(X, left, right, flag, m, n, k, R, round_fp16=True)
+        # non-negative data: at most 32 truncating K16 MMAs per segment (2
+        # ulps each) plus 9 round-to-nearest flushes/roundings
+        assert rel(got, want) <= 32 * 2.0 ** -22 + 9 * 2.0 ** -24, (flag, rel(got, want))
+
+
 def test_bad_mode_rejected(cd):
     X = torch.zeros(8, device="cuda")
     out = torch.zeros(8, device="cuda")
