@@ -268,10 +268,41 @@ def leg_order4(cd, torch, stream, sptr):
             "sweep_gbs": round(sweep_bytes(dims, R) / sweep_ms / 1e6, 1), "fit_after_13_sweeps": round(fit, 8)}
 
 
+def _fp64_unfold(Xd, dims, n):
+    """Mode-n unfolding (dims[n] x rest) of a flat column-major FP64 tensor."""
+    import numpy as np
+    T = Xd.reshape(tuple(reversed(dims)))
+    return np.moveaxis(T, len(dims) - 1 - n, 0).reshape(dims[n], -1)
+
+
+def _max_angle(U, W):
+    """Largest principal angle (radians) between span(U) and span(W), W
+    orthonormal."""
+    import numpy as np
+    Q, _ = np.linalg.qr(U)
+    return float(np.arcsin(min(1.0, np.linalg.norm(Q - W @ (W.T @ Q), 2))))
+
+
+def _fp64_project(Xd, dims, facs, skip):
+    """X x_m U_m^T for every m != skip, FP64 on the host (axes reversed)."""
+    import numpy as np
+    T = Xd.reshape(tuple(reversed(dims)))
+    N = len(dims)
+    for m in range(N):
+        if m != skip:
+            T = np.moveaxis(np.tensordot(T, facs[m], axes=([N - 1 - m], [0])), -1, N - 1 - m)
+    return T
+
+
 def leg_tucker(cd, torch, stream, sptr):
     """Tucker HOSVD + 10 HOOI sweeps: 512^3 (32,32,32) and 128^4 (16^4),
     Grams on the tensor cores (three-term BF16), TTM chains in BF16, FP64
-    eigensolves; reconstruction error relative to X."""
+    eigensolves; reconstruction error relative to X, and the largest
+    principal angle of every factor against FP64 on the host: HOSVD against
+    the leading eigenvectors (numpy eigh) of the FP64 unfolding Grams, HOOI
+    against the leading eigenvectors of the FP64 Gram of X projected by the
+    other returned factors (its fixed point)."""
+    import numpy as np
     out = {}
     for dims, ranks in (((512, 512, 512), (32, 32, 32)), ((128, 128, 128, 128), (16, 16, 16, 16))):
         key = "x".join(map(str, dims)) + "_r" + str(ranks[0])
@@ -282,6 +313,13 @@ def leg_tucker(cd, torch, stream, sptr):
         U = [torch.empty(d * r, device="cuda") for d, r in zip(dims, ranks)]
         rec = torch.empty_like(X)
         res = {}
+        Xd = X.double().cpu().numpy()
+        N = len(dims)
+        W64 = []
+        for n in range(N):
+            A = _fp64_unfold(Xd, dims, n)
+            W64.append(np.linalg.eigh(A @ A.T)[1][:, dims[n] - ranks[n]:])
+            del A
         for method in ("hosvd", "hooi10"):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -294,9 +332,19 @@ def leg_tucker(cd, torch, stream, sptr):
             cd.gentucker(rec, core, U, dims, ranks, stream=sptr)
             torch.cuda.synchronize()
             err = float(torch.linalg.norm((X - rec).double()) / torch.linalg.norm(X.double()))
-            res[method] = {"seconds": round(dt, 4), "rel_error": float(f"{err:.4e}")}
+            Uh = [u.double().cpu().numpy().reshape(d, r, order="F") for u, d, r in zip(U, dims, ranks)]
+            if method == "hosvd":
+                angles = [_max_angle(Uh[n], W64[n]) for n in range(N)]
+            else:
+                angles = []
+                for n in range(N):
+                    Y = _fp64_project(Xd, dims, Uh, skip=n)
+                    A = np.moveaxis(Y, N - 1 - n, 0).reshape(dims[n], -1)
+                    angles.append(_max_angle(Uh[n], np.linalg.eigh(A @ A.T)[1][:, dims[n] - ranks[n]:]))
+            res[method] = {"seconds": round(dt, 4), "rel_error": float(f"{err:.4e}"),
+                           "max_angle_rad_per_mode": [float(f"{a:.2e}") for a in angles]}
         out[key] = res
-        del X, rec
+        del X, rec, Xd
     return out
 
 
@@ -451,6 +499,109 @@ def leg_warmstart(cd, torch, n_train, n_eval):
     return ev
 
 
+def _time_calls(torch, stream, fn, reps, warm=2):
+    """Mean ms of fn() over `reps` calls, CUDA events on `stream`."""
+    for _ in range(warm):
+        fn()
+    e0, e1 = _events(torch)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def leg_reference_gpu(cd, torch, stream, sptr, reps=10):
+    """The reference's own GPU MTTKRP timed beside ours on this GPU (a
+    baseline, outside every timed region of the library):
+    * the FP32 MTTKRP its CP-ALS programs run -- Khatri-Rao by rank-1
+      batched GEMMs, then one SGEMM against X, X2 or X3
+      (src/cp_als.cu:46-52,66-69,85-88; src/cp4_als.cu:67-73,91-96,112-117,
+      135-138), issued by oracle/ref_gpu.cu on a handle bound to the bench
+      stream -- per mode at 512^3 rank 64 and 96^4 rank 32, against our
+      cud_mttkrp in FP32 (CUDA cores) and BF16x3 (tensor cores);
+    * its public FP16 mttkrp() (src/mttkrp.cu:3-80, allocations and device
+      synchronisations per call, as shipped), host wall time per call at
+      512^3 rank 64, against our cud_mttkrp_legacy."""
+    import oracle
+    out = {}
+    for dims, R, seeds in (((512, 512, 512), 64, (40, 41)), ((96, 96, 96, 96), 32, (42, 43))):
+        key = "x".join(map(str, dims)) + f"_r{R}"
+        with torch.cuda.stream(stream):
+            X, _ = cd.make_cp_tensor(dims, R, seed=seeds[0])
+            U = cd.make_init(dims, R, seed=seeds[1])
+        stream.synchronize()
+        h = oracle.RefGpuMttkrp(torch, X, dims, U, R, stream=sptr)
+        res = {}
+        try:
+            o = torch.empty(max(dims) * R, device="cuda")
+            for mode in range(len(dims)):
+                ref_ms = _time_calls(torch, stream, lambda: h.run(mode), reps)
+                ours = {}
+                for name in ("bf16x3", "fp32"):
+                    ours[name] = _time_calls(
+                        torch, stream,
+                        lambda: cd.mttkrp(X, dims, U, mode, R, o, cd.PRECISIONS[name], stream=sptr), reps)
+                b = mttkrp_bytes(dims, R, mode)
+                res[str(mode)] = {"reference_ms": round(ref_ms, 4), "reference_gbs": round(b / ref_ms / 1e6, 1),
+                                  "ours_bf16x3_ms": round(ours["bf16x3"], 4),
+                                  "ours_bf16x3_gbs": round(b / ours["bf16x3"] / 1e6, 1),
+                                  "ours_fp32_ms": round(ours["fp32"], 4),
+                                  "speedup_bf16x3": round(ref_ms / ours["bf16x3"], 2),
+                                  "speedup_fp32": round(ref_ms / ours["fp32"], 2)}
+        finally:
+            h.close()
+        tot = {k: sum(v[k] for v in res.values()) for k in ("reference_ms", "ours_bf16x3_ms", "ours_fp32_ms")}
+        out[key] = {"per_mode": res, "all_modes_ms": {k: round(v, 4) for k, v in tot.items()},
+                    "speedup_bf16x3": round(tot["reference_ms"] / tot["ours_bf16x3_ms"], 2),
+                    "speedup_fp32": round(tot["reference_ms"] / tot["ours_fp32_ms"], 2)}
+        del X, U
+        torch.cuda.synchronize()
+    # the public FP16 mttkrp(), as shipped (host-synchronous, allocates per call)
+    if os.path.exists(oracle.REF_LIB_PATH):
+        import ctypes
+        lib = ctypes.CDLL(oracle.REF_LIB_PATH)
+        f = getattr(lib, "_Z6mttkrpPfS_S_S_lllll")
+        f.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_long] * 5
+        f.restype = None
+        m = n = k = 512
+        r = 64
+        with torch.cuda.stream(stream):
+            X, _ = cd.make_cp_tensor((m, n, k), r, seed=44)
+            A, B, C = cd.make_init((m, n, k), r, seed=45)
+        torch.cuda.synchronize()
+        o1 = torch.empty(512 * r, device="cuda")
+        o2 = torch.empty(512 * r, device="cuda")
+        pub = {}
+        for flag, (left, right) in ((1, (C, B)), (2, (C, A)), (3, (B, A))):
+            def ref_call():
+                f(X.data_ptr(), left.data_ptr(), right.data_ptr(), o1.data_ptr(), flag, m, n, k, r)
+                torch.cuda.synchronize()
+
+            def our_call():
+                cd.mttkrp_legacy(X, left, right, o2, flag, m, n, k, r, stream=sptr)
+                stream.synchronize()
+            t = {}
+            for name, fn in (("reference", ref_call), ("ours", our_call)):
+                fn()
+                fn()
+                samples = []
+                for _ in range(5):
+                    t0 = time.perf_counter()
+                    fn()
+                    samples.append(time.perf_counter() - t0)
+                t[name] = statistics.median(samples) * 1e3
+            d = (o1 - o2).double().norm() / o1.double().norm()
+            pub[str(flag)] = {"reference_ms": round(t["reference"], 3), "ours_ms": round(t["ours"], 4),
+                              "speedup": round(t["reference"] / t["ours"], 2),
+                              "rel_diff": float(f"{float(d):.2e}")}
+        out["public_fp16_mttkrp_512x512x512_r64"] = dict(pub, timing="host wall time per synchronous call, "
+                                                                      "median of 5")
+        del X, A, B, C
+    return out
+
+
 def config_dict(dims, R, precision, world=1):
     return {"workload": f"cp_als_sweep_{'x'.join(map(str, dims))}_r{R}", "dims": dims, "rank": R,
             "precision": precision, "global_batch": world, "seq_len": None,
@@ -570,6 +721,8 @@ def main():
     ap.add_argument("--cpu-slab", type=int, default=64)
     ap.add_argument("--no-ttf", action="store_true", help="skip the time-to-fit runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="skip timing the reference's own GPU MTTKRP beside ours")
     ap.add_argument("--only-mttkrp", action="store_true",
                     help="time only the MTTKRP kernels (profiling runs) and exit")
     ap.add_argument("--only-tucker", action="store_true",
@@ -808,6 +961,16 @@ def main():
                 side[name] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
             torch.cuda.synchronize()
         result["workloads"] = side
+
+    # ---- the reference's own GPU MTTKRP on this GPU, beside ours
+    if rank == 0 and world == 1 and not args.no_refgpu:
+        try:
+            with ClockSampler(local) as rclk:
+                result["reference_gpu"] = leg_reference_gpu(cd, torch, stream, sptr)
+            result["reference_gpu"]["clocks"] = rclk.summary()
+        except Exception as exc:
+            result["reference_gpu"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+        torch.cuda.synchronize()
 
     # ---- CPU baseline (rank 0, bounded sample)
     if rank == 0 and world == 1 and not args.no_cpu:

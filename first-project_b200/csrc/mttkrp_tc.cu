@@ -88,8 +88,10 @@ struct TcArgs {
     KrFactors outer;   // kind 1: factors after the mode (one constant row per stage)
     float *part;       // [split][Q][Rp]
     int *error;        // device flag
-    const uint8_t *pb; // pre-packed B path: blk B tiles (hi, lo) of the fastest generating factor
-    long blk;          // stages per constant-row block (rows of the fastest generating factor / 32)
+    const uint8_t *pb; // pre-packed B path: blk B tiles (hi, lo) of the folded factors' Khatri-Rao rows
+    long blk;          // stages per constant-row block (folded rows / 32)
+    int fold;          // pre-packed B path: factors folded into B, counted along gen then outer
+    long frows;        // pre-packed B path: product of the folded factors' rows (= 32 * blk)
 };
 
 struct TcCtrl {
@@ -731,6 +733,28 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 //     odd group flushing segments, scaled by c;
 //   * warp 10: the constant row c of each segment into shared memory.
 constexpr int PB_THREADS = 352;
+
+// The contraction position of stage g runs over l = 32 g .. 32 g + 31, with
+// digits over the factor list F = gen followed by outer (kind 1: l = p + P s
+// and P = 32 psteps).  The first `fold` factors of F are folded into the
+// packed B; the constant row is the product of the remaining factors' rows
+// at the digits of l / frows.
+template <class Ctrl>
+__device__ __forceinline__ float pb_const_row(const TcArgs &a, const Ctrl &sm, long g, int r) {
+    long lin = ((long)g * BKS) / a.frows;
+    float c = 1.f;
+    for (int f = a.fold; f < a.gen.n; f++) {
+        const long d = sm.grows[f], qd = lin / d;
+        c *= __ldg(sm.gU[f] + (lin - qd * d) + (long)r * d);
+        lin = qd;
+    }
+    for (int f = (a.fold > a.gen.n ? a.fold - a.gen.n : 0); f < a.outer.n; f++) {
+        const long d = sm.orows[f], qd = lin / d;
+        c *= __ldg(sm.oU[f] + (lin - qd * d) + (long)r * d);
+        lin = qd;
+    }
+    return c;
+}
 constexpr int PB_RING = 6;  // deepest X ring = A/B ring
 
 struct PbCtrl {
@@ -768,12 +792,14 @@ __host__ __device__ constexpr size_t pb_smem_bytes(int Rpad, int n) {
     return 1024 + PB_CTRL_BYTES + (size_t)n * (X_STAGE_BYTES + 2 * b_tile_bytes(Rpad));
 }
 
-// B tiles of the pre-packed path: tile t holds U0 rows 32t..32t+31 for every
-// column r (zero for r >= R), hi then lo, each in the canonical layout above.
-// One thread per (tile, 8-row chunk kc, column r); consecutive threads write
-// consecutive 16-byte chunks.
-__global__ void __launch_bounds__(256) k_pack_b(const float *__restrict__ U0, long rows0, long R, int Rpad,
-                                                long blk, int prec, uint8_t *__restrict__ pb, int *error) {
+// B tiles of the pre-packed path: tile t holds the Khatri-Rao rows
+// 32t..32t+31 of the folded factors (fastest first; one factor: U0's rows)
+// for every column r (zero for r >= R), hi then lo, each in the canonical
+// layout above.  A row's entries are formed as one FP32 product, the way the
+// Khatri-Rao matrix of the reference is.  One thread per (tile, 8-row chunk
+// kc, column r); consecutive threads write consecutive 16-byte chunks.
+__global__ void __launch_bounds__(256) k_pack_b(KrFactors fold, long R, int Rpad, long blk, int prec,
+                                                uint8_t *__restrict__ pb, int *error) {
     const long n = blk * 4 * Rpad;
     const long id = blockIdx.x * 256L + threadIdx.x;
     if (id == 0) *error = 0;
@@ -783,7 +809,16 @@ __global__ void __launch_bounds__(256) k_pack_b(const float *__restrict__ U0, lo
     const int kc = rem / Rpad, r = rem - kc * Rpad;
     float v[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) v[j] = (r < R) ? __ldg(U0 + 32 * t + 8 * kc + j + (long)r * rows0) : 0.f;
+    for (int j = 0; j < 8; j++) {
+        long lin = 32 * t + 8 * kc + j;
+        float p = 1.f;
+        for (int f = 0; f < fold.n; f++) {
+            const long d = fold.rows[f], qd = lin / d;
+            p *= (r < R) ? __ldg(fold.U[f] + (lin - qd * d) + (long)r * d) : 0.f;
+            lin = qd;
+        }
+        v[j] = (r < R) ? p : 0.f;
+    }
     const bool three = (prec == CUD_PREC_BF16X3 || prec == CUD_PREC_DEFAULT);
     uint4 h, l;
     pack_b_item(v, h, l, three, prec == CUD_PREC_FP16);
@@ -1043,7 +1078,7 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
                 // buffer b's previous segment (sg - 2) must have been drained
                 if (sg >= 2 && !*abort) ptx::mbar_wait(&sm.d_free[b], (uint32_t)(((sg >> 1) - 1) & 1), abort);
                 for (int r = lane; r < a.Rpad; r += 32)
-                    sm.cvec[b][r] = (r < a.R) ? kr_const_row(a, sm, st_beg + i, r) : 0.f;
+                    sm.cvec[b][r] = (r < a.R) ? pb_const_row(a, sm, st_beg + i, r) : 0.f;
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(&sm.c_full[b]);
             }
@@ -1119,6 +1154,8 @@ struct TcPlan {
     int nx, nb, ctas_per_sm;
     bool pb;    // pre-packed B path
     long blk;   // stages per constant-row block (fast path)
+    int fold;   // pre-packed B path: factors folded into B (along gen, then outer)
+    long frows; // their rows' product (= 32 blk)
 };
 
 // Pre-packed B path launch shape: the deepest rings (X and A/B equal, at
@@ -1193,12 +1230,33 @@ bool tc_plan(int order, const long *dims, int mode, long R, int precision, TcPla
     const long rows0 = (mode == 0) ? dims[1] : dims[0];
     p.fast = (rows0 % BKS == 0);
     p.blk = p.fast ? rows0 / BKS : 1;
+    p.fold = 1;
+    p.frows = rows0;
     // pre-packed B path: blocks of at least 2 stages (each segment flush
     // adds a whole 128 x R partial tile, at least every other stage).  Not
     // for FP16: the public mttkrp rounds each whole Khatri-Rao entry,
     // fp16(U0[x] * c[y]) (src/mttkrp.cu:21-25, 41-47, 65-69), while the
     // packed tiles hold fp16(U0[x]) and apply c in FP32 at the flush; the
     // Khatri-Rao-building kernel forms the product first and rounds it once.
+    // When U0's own blocks are shorter than a segment (96 rows: a flush of
+    // the whole 128 x R partial tile every 3 stages), fold the next factors
+    // of the contraction (gen, then outer) into the packed B as long as the
+    // packed tiles stay within kFoldBytes: the constant row then changes
+    // every frows / 32 stages.
+    if (p.fast && precision != CUD_PREC_FP16) {
+        constexpr long kFoldBytes = 8L << 20;
+        long fl[2 * kMaxOrder];
+        int nf = 0;
+        for (int m = 0; m < order; m++)
+            if (m != mode && (p.kind == 0 || m < mode)) fl[nf++] = dims[m];
+        for (int m = mode + 1; p.kind == 1 && m < order; m++) fl[nf++] = dims[m];
+        while (p.frows / BKS < SEG && p.fold < nf &&
+               p.frows * fl[p.fold] * p.Rpad * 4 <= kFoldBytes && p.frows * fl[p.fold] <= 0x7fffffffL) {
+            p.frows *= fl[p.fold];
+            p.fold++;
+        }
+        p.blk = p.frows / BKS;
+    }
     p.pb = p.fast && p.blk >= 2 && precision != CUD_PREC_FP16;
 #ifdef CUD_TC_NO_PB
     p.pb = false;
@@ -1336,12 +1394,23 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     a.error = reinterpret_cast<int *>(w);
     a.part = reinterpret_cast<float *>(w + 256);
     a.blk = p.blk;
+    a.fold = p.fold;
+    a.frows = p.frows;
     a.pb = reinterpret_cast<const uint8_t *>(w + 256 + tc_part_bytes(p, R));
     if (p.pb) {
         // the pack kernel also clears the error flag (no separate memset)
-        const long rows0 = (mode == 0) ? dims[1] : dims[0];
+        KrFactors fold;  // the first p.fold factors of gen ++ outer
+        fold.n = 0;
+        for (int f = 0; f < a.gen.n && fold.n < p.fold; f++, fold.n++) {
+            fold.U[fold.n] = a.gen.U[f];
+            fold.rows[fold.n] = a.gen.rows[f];
+        }
+        for (int f = 0; f < a.outer.n && fold.n < p.fold; f++, fold.n++) {
+            fold.U[fold.n] = a.outer.U[f];
+            fold.rows[fold.n] = a.outer.rows[f];
+        }
         const long items = p.blk * 4 * p.Rpad;
-        k_pack_b<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(U0, rows0, R, (int)p.Rpad, p.blk, precision,
+        k_pack_b<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(fold, R, (int)p.Rpad, p.blk, precision,
                                                                  const_cast<uint8_t *>(a.pb), a.error);
         CUD_CHECK_LAUNCH("mttkrp_pb pack");
         a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;

@@ -13,9 +13,13 @@
 // copy of X followed by N-1 such GEMMs.  Gram operands X_(n) (rows = mode n,
 // the other modes contiguous) come from one convert-and-unfold kernel.
 //
-// Precision: BF16 -> Grams from one BF16 GEMM; BF16X3 / DEFAULT -> Grams
-// from the three-term split (hi hi + hi lo + lo hi, the last term the
-// transpose of the middle one).  TTMs are BF16 in both.
+// Precision: BF16 -> Grams from one BF16 GEMM and single-term BF16 TTM
+// chains.  BF16X3 / DEFAULT -> FP32-level accuracy throughout: Grams from
+// the three-term split (hi hi + hi lo + lo hi, the last term the transpose
+// of the middle one), and every TTM step three-term as well, T U ~ Th Uh +
+// Th Ul + Tl Uh (one GEMM of Th against [Uh | Ul], one of Tl against Uh,
+// FP32 accumulation), with the chain's intermediates kept as hi/lo pairs
+// and the HOOI projection's Gram three-term.
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"
@@ -155,6 +159,48 @@ __global__ void k_to_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict
 
 unsigned gfor(long n) { return (unsigned)std::min<long>((n + 255) / 256, 16L * kNumSMs); }
 
+// a (n floats) -> hi (bf16(a)) and lo (bf16(a - hi)).
+__global__ void k_split_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict__ hi,
+                             __nv_bfloat16 *__restrict__ lo, long n) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        put_split(hi, lo, e, a[e]);
+}
+
+// Three-term TTM finish: v = F2[e] (+ F2[e + n] when the two halves of
+// Th [Uh | Ul] were written side by side), written as FP32 (fout) or split
+// into the next step's hi/lo operands.
+__global__ void k_ttm3_finish(const float *__restrict__ F2, long n, int halves, float *__restrict__ fout,
+                              __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+        const float v = halves ? F2[e] + F2[e + n] : F2[e];
+        if (fout) fout[e] = v;
+        else put_split(hi, lo, e, v);
+    }
+}
+
+// An FP32 (Q, S) matrix with q fastest -> rows of q with s contiguous, row
+// stride Sp >= S, split into BF16 hi and lo; pad columns S..Sp-1 zero.
+__global__ void __launch_bounds__(256) k_transpose_split(const float *__restrict__ X, long Q, long S, long Sp,
+                                                         __nv_bfloat16 *__restrict__ hi,
+                                                         __nv_bfloat16 *__restrict__ lo) {
+    __shared__ float tile[32][33];
+    const long tq = (Q + 31) / 32, ts = (Sp + 31) / 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (long t = blockIdx.x; t < tq * ts; t += gridDim.x) {
+        const long q0 = (t % tq) * 32, s0 = (t / tq) * 32;
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            const long q = q0 + tx, s = s0 + k;
+            tile[k][tx] = (q < Q && s < S) ? X[q + Q * s] : 0.f;
+        }
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            const long q = q0 + k, s = s0 + tx;
+            if (q < Q && s < Sp) put_split(hi, lo, q * Sp + s, tile[tx][k]);
+        }
+    }
+}
+
 // X viewed as (P, Q, S) -> X_(view) rows of Q, the rest contiguous (BF16).
 // Same unfolding for P a multiple of 8, in the source's memory order: item
 // (u, c) = 8 consecutive floats c of source row u = q + Q s (two 16-byte
@@ -215,7 +261,10 @@ struct TcWork {
     __nv_bfloat16 *xb = nullptr;       // X in BF16 (rotated as needed), total
     __nv_bfloat16 *uh = nullptr, *ul = nullptr;  // Gram operands, total each
     __nv_bfloat16 *z0 = nullptr, *z1 = nullptr;  // chain intermediates
-    __nv_bfloat16 *ub = nullptr;       // a factor in BF16
+    __nv_bfloat16 *ub = nullptr;       // a factor in BF16 (three-term: hi then lo, 2 K r)
+    __nv_bfloat16 *zl0 = nullptr, *zl1 = nullptr;  // three-term: low parts of the intermediates
+    float *f2 = nullptr;               // three-term: FP32 TTM partials, 2 zmax
+    float *yf = nullptr;               // three-term: the projection Y in FP32, zmax
     float *g32 = nullptr;              // Gram FP32
     double *g64 = nullptr, *W = nullptr, *V = nullptr;
     void *gws = nullptr;               // GEMM workspace
@@ -237,6 +286,7 @@ int tc_alloc(int order, const long *dims, const long *ranks, bool three, TcWork 
     for (int m = 0; m < order; m++) {
         gw = std::max(gw, gemm_tc_ws_bytes(dims[m], dims[m], total / dims[m]));
         gw = std::max(gw, gemm_tc_ws_bytes(total / dims[m], ranks[m], dims[m]));
+        if (three) gw = std::max(gw, gemm_tc_ws_bytes(total / dims[m], 2 * ranks[m], dims[m]));
         long rest = 1;
         for (int q = 0; q < order; q++)
             if (q != m) rest *= ranks[q];
@@ -249,7 +299,11 @@ int tc_alloc(int order, const long *dims, const long *ranks, bool three, TcWork 
     const size_t o_ul = off; off += three ? up(2 * (size_t)total) : 0;
     const size_t o_z0 = off; off += up(2 * (size_t)zmax);
     const size_t o_z1 = off; off += up(2 * (size_t)zmax);
-    const size_t o_ub = off; off += up(2 * (size_t)maxd * maxr);
+    const size_t o_ub = off; off += up(2 * 2 * (size_t)maxd * maxr);
+    const size_t o_zl0 = off; off += three ? up(2 * (size_t)zmax) : 0;
+    const size_t o_zl1 = off; off += three ? up(2 * (size_t)zmax) : 0;
+    const size_t o_f2 = off; off += three ? up(4 * 2 * (size_t)zmax) : 0;
+    const size_t o_yf = off; off += three ? up(4 * (size_t)zmax) : 0;
     const size_t o_g32 = off; off += up(4 * (size_t)maxd * maxd);
     const size_t o_g64 = off; off += up(8 * (size_t)maxd * maxd);
     const size_t o_W = off; off += up(8 * (size_t)maxd);
@@ -264,6 +318,10 @@ int tc_alloc(int order, const long *dims, const long *ranks, bool three, TcWork 
     w.z0 = (__nv_bfloat16 *)(p + o_z0);
     w.z1 = (__nv_bfloat16 *)(p + o_z1);
     w.ub = (__nv_bfloat16 *)(p + o_ub);
+    w.zl0 = three ? (__nv_bfloat16 *)(p + o_zl0) : nullptr;
+    w.zl1 = three ? (__nv_bfloat16 *)(p + o_zl1) : nullptr;
+    w.f2 = three ? (float *)(p + o_f2) : nullptr;
+    w.yf = three ? (float *)(p + o_yf) : nullptr;
     w.g32 = (float *)(p + o_g32);
     w.g64 = (double *)(p + o_g64);
     w.W = (double *)(p + o_W);
@@ -345,12 +403,38 @@ int ttm_fast(const TcWork &w, const __nv_bfloat16 *T, long K, long rest, const f
     return gemm_tc_bf16(T, K, w.ub, K, rest, r, K, e, w.gws, s);
 }
 
+// Three-term TTM over the fastest mode: (Th + Tl) (K x rest, K fastest) times
+// U (K x r, FP32) ~ Th Uh + Th Ul + Tl Uh -> (rest x r), r slowest, as FP32
+// into fout or as the hi/lo pair (zh, zl).  With 2 r <= 32 (the skinny GEMM's
+// width) Th is read once, against [Uh | Ul]; wider ranks take three GEMMs of
+// width r, accumulating in FP32.
+int ttm3_fast(const TcWork &w, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl, long K, long rest, const float *U,
+              long r, __nv_bfloat16 *zh, __nv_bfloat16 *zl, float *fout, cudaStream_t s) {
+    if (gemm_tc_ws_bytes(rest, 2 * r, K) > w.gws_bytes) return CUD_ERR_INVALID_ARGUMENT;
+    const __nv_bfloat16 *Uh = w.ub, *Ul = w.ub + K * r;
+    k_split_bf16<<<gfor(K * r), 256, 0, s>>>(U, w.ub, w.ub + K * r, K * r);
+    CUD_CHECK_LAUNCH("ttm3 factor split");
+    const bool halves = 2 * r <= 32;
+    int st;
+    if (halves) {
+        if ((st = gemm_tc_bf16(Th, K, Uh, K, rest, 2 * r, K, epi_f32(w.f2, 1, rest, 0), w.gws, s))) return st;
+    } else {
+        if ((st = gemm_tc_bf16(Th, K, Uh, K, rest, r, K, epi_f32(w.f2, 1, rest, 0), w.gws, s))) return st;
+        if ((st = gemm_tc_bf16(Th, K, Ul, K, rest, r, K, epi_f32(w.f2, 1, rest, 1), w.gws, s))) return st;
+    }
+    if ((st = gemm_tc_bf16(Tl, K, Uh, K, rest, r, K, epi_f32(w.f2, 1, rest, 1), w.gws, s))) return st;
+    k_ttm3_finish<<<gfor(rest * r), 256, 0, s>>>(w.f2, rest * r, halves ? 1 : 0, fout, zh, zl);
+    CUD_CHECK_LAUNCH("ttm3 finish");
+    return CUD_OK;
+}
+
 // Contracts modes `first`, first+1, ... (cyclically) of T -- laid out with
 // mode `first` fastest, cyclic order -- except mode `skip` (or none when
 // skip < 0, all `order` modes).  Returns the BF16 buffer holding the result
 // (or writes FP32 `final_out` at the last step) and its element count.
 int chain(const TcWork &w, const __nv_bfloat16 *T, int order, const long *dims, const long *ranks,
-          float *const *U, int first, int skip, float *final_out, const __nv_bfloat16 **res, cudaStream_t s) {
+          float *const *U, int first, int skip, float *final_out, const __nv_bfloat16 **res, cudaStream_t s,
+          const __nv_bfloat16 *Tlo = nullptr) {
     long cur[2 * kMaxOrder];  // sizes in layout order
     for (int k = 0; k < order; k++) cur[k] = dims[(first + k) % order];
     long total = 1;
@@ -363,7 +447,16 @@ int chain(const TcWork &w, const __nv_bfloat16 *T, int order, const long *dims, 
         const long rest = total / K;
         const bool last = (step == nsteps - 1);
         __nv_bfloat16 *dst = (step & 1) ? w.z1 : w.z0;
-        int st = ttm_fast(w, src, K, rest, U[m], ranks[m], dst, (last && final_out) ? final_out : nullptr, s);
+        int st;
+        if (Tlo) {
+            // three-term: the intermediates carry their low parts along
+            __nv_bfloat16 *dlo = (step & 1) ? w.zl1 : w.zl0;
+            st = ttm3_fast(w, src, Tlo, K, rest, U[m], ranks[m], dst, dlo, (last && final_out) ? final_out : nullptr,
+                           s);
+            Tlo = dlo;
+        } else {
+            st = ttm_fast(w, src, K, rest, U[m], ranks[m], dst, (last && final_out) ? final_out : nullptr, s);
+        }
         if (st) return st;
         cur[order + step] = ranks[m];
         total = rest * ranks[m];
@@ -416,9 +509,10 @@ int tucker_tc_core(const float *X, int order, const long *dims, const long *rank
     if (st) return st;
     long total = 1;
     for (int m = 0; m < order; m++) total *= dims[m];
-    if ((st = unfold_bf16(X, total, 1, 1, w.xb, nullptr, s))) return st;  // plain BF16 copy
+    // plain BF16 copy (three-term: hi into xb, lo into ul)
+    if ((st = unfold_bf16(X, total, 1, 1, w.xb, three ? w.ul : nullptr, s))) return st;
     const __nv_bfloat16 *res;
-    return chain(w, w.xb, order, dims, ranks, U, 0, -1, core, &res, s);
+    return chain(w, w.xb, order, dims, ranks, U, 0, -1, core, &res, s, three ? w.ul : nullptr);
 }
 
 // One HOOI sweep: for each mode n, U_n = top eigenvectors of the Gram of
@@ -438,23 +532,33 @@ int tucker_tc_hooi_sweep(const float *X, int order, const long *dims, const long
         for (int m = 0; m <= n; m++) Pn *= dims[m];
         const long rest = total / Pn;
         const int first = (n + 1) % order;
-        if (rest == 1) st = unfold_bf16(X, total, 1, 1, w.xb, nullptr, s);
-        else st = unfold_bf16(X, 1, Pn, rest, w.xb, nullptr, s);
+        // three-term: the low part of X goes to ul (not otherwise used here)
+        __nv_bfloat16 *xlo = three ? w.ul : nullptr;
+        if (rest == 1) st = unfold_bf16(X, total, 1, 1, w.xb, xlo, s);
+        else st = unfold_bf16(X, 1, Pn, rest, w.xb, xlo, s);
         if (st) return st;
         const __nv_bfloat16 *Y;
-        if ((st = chain(w, w.xb, order, dims, ranks, U, first, n, nullptr, &Y, s))) return st;
+        if ((st = chain(w, w.xb, order, dims, ranks, U, first, n, three ? w.yf : nullptr, &Y, s, xlo))) return st;
         // Y: mode n fastest, then the other modes' ranks -> rows of mode n
         long R = 1;
         for (int m = 0; m < order; m++)
             if (m != n) R *= ranks[m];
-        // Y (BF16) has mode n fastest: a tiled transpose gives the Gram
-        // operand's rows; Y is already rounded, so there is no low part
+        // Y has mode n fastest: a tiled transpose gives the Gram operand's
+        // rows (single-term: Y is already BF16; three-term: Y is FP32 and
+        // is split into hi/lo on the way)
         // rows padded to a multiple of 8 (the GEMM's leading-dimension rule)
         const long Rp = (R + 7) / 8 * 8;
         const long tiles = ((dims[n] + 31) / 32) * ((Rp + 31) / 32);
-        k_transpose_bf16<<<(unsigned)std::min<long>(tiles, 16L * kNumSMs), 256, 0, s>>>(Y, dims[n], R, Rp, w.uh);
+        const unsigned tg = (unsigned)std::min<long>(tiles, 16L * kNumSMs);
+        if (three) {
+            // Y in FP32 (the chain's last step) -> hi/lo Gram operands; X's
+            // low part in ul is no longer needed
+            k_transpose_split<<<tg, 256, 0, s>>>(w.yf, dims[n], R, Rp, w.uh, w.ul);
+        } else {
+            k_transpose_bf16<<<tg, 256, 0, s>>>(Y, dims[n], R, Rp, w.uh);
+        }
         CUD_CHECK_LAUNCH("hooi transpose");
-        if ((st = gram_tc(w, dims[n], Rp, false, s))) return st;
+        if ((st = gram_tc(w, dims[n], Rp, three, s))) return st;
         st = top_vectors(w, dims[n], ranks[n], U[n], s, n > 0 || u0_set);
         if (st == CUD_ERR_NOT_CONVERGED) *worst = st;
         else if (st) return st;

@@ -454,3 +454,142 @@ def ws_mlp_grads(params, X, T):
     dH1 = round_bf16_np((dH2 @ W2h) * (H1 > 0))
     gW1, gb1 = dH1.T @ X, dH1.sum(0)
     return loss, [gW1, gb1, gW2, gb2, gW3, gb3]
+
+
+# ---------------------------------------------------------------- reference GPU MTTKRP (baseline harness)
+
+REF_GPU_PATH = os.path.join(_HERE, "_build", "libref_gpu.so")
+
+
+class RefGpuMttkrp:
+    """The reference's own GPU MTTKRP (its cuBLAS Khatri-Rao + SGEMM call
+    sequence, oracle/ref_gpu.cu) on device buffers of one 3rd- or 4th-order
+    problem.  Used as a timing baseline and checked against `mttkrp` by the
+    GPU tests.  Arguments are raw device pointers (ints) and a stream handle.
+
+    `factors` are the column-major dims[m] x R device buffers, `X` the flat
+    column-major tensor.  Owns its scratch (the permuted copies the
+    reference makes once, the Khatri-Rao matrices) through torch."""
+
+    def __init__(self, torch, X, dims, factors, R, stream=None):
+        self.torch = torch
+        self.lib = ctypes.CDLL(REF_GPU_PATH)
+        vp, l, i = ctypes.c_void_p, ctypes.c_long, ctypes.c_int
+        self.lib.rg_create.argtypes = [ctypes.POINTER(vp), vp]
+        self.lib.rg_destroy.argtypes = [vp]
+        self.lib.rg_cp3_mttkrp.argtypes = [vp, i] + [vp] * 5 + [l] * 4 + [vp, vp]
+        self.lib.rg_cp4_prepare.argtypes = [vp, vp, vp, vp, vp] + [l] * 4 + [vp]
+        self.lib.rg_cp4_mttkrp.argtypes = [vp, i] + [vp] * 7 + [l] * 5 + [vp, vp, vp]
+        self.dims, self.R = [int(d) for d in dims], int(R)
+        self.X, self.U = X, list(factors)
+        self.stream = stream
+        h = vp()
+        if self.lib.rg_create(ctypes.byref(h), stream) != 0:
+            raise RuntimeError("cublasCreate failed")
+        self.h = h
+        dev = X.device
+        n = X.numel()
+        if len(dims) == 3:
+            a, b, c = self.dims
+            # X2: the mode-2 unfolding (b x ac), made once as the reference's
+            # t2m does before its sweeps (src/cp_als.cu:28)
+            self.X2 = X.view(c, b, a).permute(0, 2, 1).contiguous().view(-1)
+            self.kr = torch.empty(max(b * c, a * c, a * b) * R, device=dev)
+        elif len(dims) == 4:
+            a, b, c, d = self.dims
+            self.X2 = torch.empty(n, device=dev)
+            self.X3 = torch.empty(n, device=dev)
+            ident = torch.empty(a * b * a * b, device=dev)
+            st = self.lib.rg_cp4_prepare(self.h, X.data_ptr(), self.X2.data_ptr(), self.X3.data_ptr(),
+                                         ident.data_ptr(), a, b, c, d, stream)
+            if st:
+                raise RuntimeError("rg_cp4_prepare failed")
+            torch.cuda.synchronize()
+            del ident
+            self.kr1 = torch.empty(max(c * d, a * b) * R, device=dev)
+            self.kr = torch.empty(max(b * c * d, a * c * d, a * b * d, a * b * c) * R, device=dev)
+        else:
+            raise ValueError("the reference's CP-ALS has orders 3 and 4")
+        self.out_t = torch.empty(max(self.dims) * R, device=dev)
+
+    def run(self, mode):
+        """Issue the mode's calls on the stream; the result (R x dims[mode],
+        transposed, as the reference keeps it) lands in self.out_t.  In 4th
+        order, modes 1 and 3 reuse the two-factor product that modes 0 and 2
+        formed, as in the reference's sweep."""
+        p = [u.data_ptr() for u in self.U]
+        if len(self.dims) == 3:
+            st = self.lib.rg_cp3_mttkrp(self.h, mode, self.X.data_ptr(), self.X2.data_ptr(), *p, *self.dims,
+                                        self.R, self.kr.data_ptr(), self.out_t.data_ptr())
+        else:
+            st = self.lib.rg_cp4_mttkrp(self.h, mode, self.X.data_ptr(), self.X2.data_ptr(), self.X3.data_ptr(),
+                                        *p, *self.dims, self.R, self.kr1.data_ptr(), self.kr.data_ptr(),
+                                        self.out_t.data_ptr())
+        if st:
+            raise RuntimeError(f"reference MTTKRP mode {mode} failed")
+
+    def result(self, mode):
+        """dims[mode] x R column-major copy of the last result (host, FP64)."""
+        q = self.dims[mode]
+        t = self.out_t[: q * self.R].double().cpu().numpy()
+        return t.reshape(self.R, q, order="F").T.reshape(-1, order="F")
+
+    def close(self):
+        if self.h:
+            self.lib.rg_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------- C++/OpenMP CPU baseline
+
+CPU_ALS_PATH = os.path.join(_HERE, "_build", "libcpu_als.so")
+_cpu = None
+
+
+def _cpu_lib():
+    global _cpu
+    if _cpu is None:
+        _cpu = ctypes.CDLL(CPU_ALS_PATH)
+        vp, l, i, d = ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_double
+        for name in ("cpu_mttkrp_f32", "cpu_mttkrp_f64"):
+            getattr(_cpu, name).argtypes = [vp, i, ctypes.POINTER(l), ctypes.POINTER(vp), i, l, vp, i]
+        for name in ("cpu_cp_als_f32", "cpu_cp_als_f64"):
+            getattr(_cpu, name).argtypes = [vp, i, ctypes.POINTER(l), l, ctypes.POINTER(vp), i, d, d, i, vp,
+                                            ctypes.POINTER(i), ctypes.POINTER(d)]
+        _cpu.cpu_max_threads.restype = i
+    return _cpu
+
+
+def cpu_threads():
+    return int(_cpu_lib().cpu_max_threads())
+
+
+def cpu_mttkrp(X, dims, factors, mode, R, threads=0):
+    """The C++/OpenMP MTTKRP (oracle/cpu_als.cpp) in X's dtype (float32 or
+    float64); returns dims[mode] x R column-major."""
+    dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
+    X = np.ascontiguousarray(X, dt).reshape(-1)
+    facs = [np.ascontiguousarray(f, dt).reshape(-1) for f in factors]
+    out = np.zeros(int(dims[mode]) * int(R), dt)
+    fn = _cpu_lib().cpu_mttkrp_f64 if dt == np.float64 else _cpu_lib().cpu_mttkrp_f32
+    fn(X.ctypes.data, len(dims), _longs(dims), (ctypes.c_void_p * len(facs))(*[f.ctypes.data for f in facs]),
+       int(mode), int(R), out.ctypes.data, int(threads))
+    return out
+
+
+def cpu_cp_als(X, dims, R, init, max_sweeps, tol=0.0, target_fit=0.0, threads=0):
+    """The ALS of decomposition/CPU/python/mycp.py:7-22 in C++/OpenMP
+    (oracle/cpu_als.cpp), in X's dtype, from `init`.  Returns (factors, fits,
+    sweeps, seconds) -- seconds measured inside the C++ code."""
+    dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
+    X = np.ascontiguousarray(X, dt).reshape(-1)
+    facs = [np.array(f, dt).reshape(-1) for f in init]
+    fits = np.zeros(max(1, max_sweeps), np.float64)
+    sw, sec = ctypes.c_int(0), ctypes.c_double(0.0)
+    fn = _cpu_lib().cpu_cp_als_f64 if dt == np.float64 else _cpu_lib().cpu_cp_als_f32
+    st = fn(X.ctypes.data, len(dims), _longs(dims), int(R), (ctypes.c_void_p * len(facs))(*[f.ctypes.data for f in facs]),
+            int(max_sweeps), float(tol), float(target_fit), int(threads), fits.ctypes.data, ctypes.byref(sw),
+            ctypes.byref(sec))
+    if st:
+        raise RuntimeError(f"cpu_cp_als failed ({st})")
+    return facs, fits[: sw.value], sw.value, sec.value

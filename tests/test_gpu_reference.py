@@ -193,3 +193,23 @@ def test_drop_in_program_runs(golden, tmp_path):
     np.testing.assert_array_equal(vals["t2m3"], oracle.t2m(X, 3, 3, 3, 3))
     np.testing.assert_array_equal(vals["gencp"], oracle.gencp((3, 3, 3), [A, B, C], 2))
     assert vals["status"][0] == 0
+
+
+@pytest.mark.parametrize("dims,R", [((40, 36, 28), 8), ((12, 10, 9, 8), 5)])
+def test_reference_gpu_mttkrp_harness(dims, R):
+    """The baseline harness that times the reference's GPU MTTKRP (its
+    Khatri-Rao + SGEMM calls) computes the MTTKRP: every mode against the
+    FP64 oracle at the FP32 bar."""
+    if not os.path.exists(oracle.REF_GPU_PATH):
+        pytest.skip("baseline harness not built (make -C oracle)")
+    rng = np.random.default_rng(sum(dims) + R)
+    X = rng.random(int(np.prod(dims))).astype(np.float32)
+    facs = [rng.random(d * R).astype(np.float32) for d in dims]
+    h = oracle.RefGpuMttkrp(torch, dev_t(X), dims, [dev_t(f) for f in facs], R)
+    try:
+        for mode in range(len(dims)):
+            h.run(mode)
+            torch.cuda.synchronize()
+            assert rel(h.result(mode), oracle.mttkrp(X, dims, facs, mode, R)) <= 1e-5, mode
+    finally:
+        h.close()

@@ -129,8 +129,17 @@ def pb_plan(dims, mode, R):
     stages = -(-S // BKS) if kind0 else S * psteps
     qtiles = -(-Q // BQ)
     rows0 = dims[1] if kind0 else dims[0]
-    assert rows0 % BKS == 0 and rows0 // BKS >= 2     # the pre-packed path
-    blk = rows0 // BKS
+    # factors folded into the packed B (gen, then outer) while a block is
+    # shorter than a segment and the packed tiles stay within 8 MiB
+    fl = [d for m, d in enumerate(dims) if m != mode and (kind0 or m < mode)]
+    fl += [] if kind0 else list(dims[mode + 1:])
+    fold, frows = 1, rows0
+    while frows // BKS < SEG and fold < len(fl) and frows * fl[fold] * rpad * 4 <= 8 << 20:
+        frows *= fl[fold]
+        fold += 1
+    if rows0 % BKS or frows // BKS < 2:
+        return None                                    # not the pre-packed path
+    blk = frows // BKS
     smem = lambda n: 1024 + PB_CTRL + n * (X_STAGE + 2 * b_tile_bytes(rpad))
     cps = nring = 0
     for n in range(PB_RING, 2, -1):
@@ -147,7 +156,7 @@ def pb_plan(dims, mode, R):
     chunk = -(-stages // splits)
     splits = -(-stages // chunk)
     return dict(stages=stages, qtiles=qtiles, blk=blk, rpad=rpad, rows0=rows0, cps=cps, nring=nring,
-                splits=splits, chunk=chunk, smem=smem(nring))
+                splits=splits, chunk=chunk, smem=smem(nring), fold=fold, frows=frows, fl=fl, P=P, psteps=psteps)
 
 
 def segments(beg, end, blk):
@@ -167,6 +176,7 @@ def segments(beg, end, blk):
 def test_mttkrp_pb_plan_partitions_stages(dims, R):
     for mode in range(len(dims)):
         p = pb_plan(dims, mode, R)
+        assert p is not None
         assert p["cps"] in (1, 2) and p["nring"] >= 3
         assert p["smem"] <= (115712 if p["cps"] == 2 else 232448)
         assert p["qtiles"] * p["splits"] <= p["cps"] * NSM          # one wave
@@ -180,6 +190,50 @@ def test_mttkrp_pb_plan_partitions_stages(dims, R):
                 assert s0 // blk == (s0 + n - 1) // blk           # never across a constant-row block
             covered += end - beg
         assert covered == p["stages"]
+
+
+@pytest.mark.parametrize("dims,R", [((96, 96, 96, 96), 32), ((128, 64, 32), 8), ((64, 40, 36), 4),
+                                    ((32, 96, 6, 5), 3), ((512, 512, 512), 64)])
+def test_mttkrp_pb_fold_reproduces_khatri_rao(dims, R):
+    """Stage g's B rows (packed row 32 (g mod blk) + i, the product of the
+    folded factors) times its constant row (the other factors at the digits
+    of 32 g / frows) equal the Khatri-Rao row of contraction position
+    l = 32 g + i, digits over gen then outer."""
+    rng = np.random.default_rng(sum(dims) + R)
+    for mode in range(len(dims)):
+        p = pb_plan(dims, mode, R)
+        if p is None:
+            continue
+        kind0 = mode == 0
+        facs = [m for m in range(len(dims)) if m != mode and (kind0 or m < mode)]
+        facs += [] if kind0 else list(range(mode + 1, len(dims)))
+        U = {m: rng.integers(1, 7, (dims[m], R)).astype(np.float64) for m in facs}
+        fold, frows, blk = p["fold"], p["frows"], p["blk"]
+        assert np.prod([dims[m] for m in facs[:fold]]) == frows
+        packed = np.ones((frows, R))
+        for rho in range(frows):
+            lin = rho
+            for m in facs[:fold]:
+                packed[rho] *= U[m][lin % dims[m]]
+                lin //= dims[m]
+        total = int(np.prod([dims[m] for m in facs]))
+        for g in rng.choice(p["stages"], min(40, p["stages"]), replace=False):
+            lin = (32 * int(g)) // frows
+            c = np.ones(R)
+            for m in facs[fold:]:
+                c *= U[m][lin % dims[m]]
+                lin //= dims[m]
+            pos = int(g) % blk
+            for i in range(32):
+                l = 32 * int(g) + i
+                if l >= total:
+                    continue
+                want = np.ones(R)
+                ll = l
+                for m in facs:
+                    want *= U[m][ll % dims[m]]
+                    ll //= dims[m]
+                np.testing.assert_array_equal(packed[32 * pos + i] * c, want)
 
 
 @pytest.mark.parametrize("rows0,R", [(512, 64), (96, 32), (64, 128), (512, 5)])
@@ -199,3 +253,141 @@ def test_mttkrp_pack_b_in_bounds(rows0, R):
     assert ((t * 2 + 1) * bbytes + off + 16).max() <= blk * 2 * bbytes   # inside the packed buffer
     # each 16-byte chunk of every tile half written exactly once
     assert len(np.unique(t * bbytes * 2 + off)) == n
+
+
+# ---- mttkrp_simt.cu k_mttkrp_ffma: the plain FP32 FFMA MTTKRP, restated on
+# the CPU with the kernel's own tile arithmetic (float4 A loads, transposing
+# swizzled stores, B = pre-packed U0 rows x the constant row, split partials)
+FQ, FK, FT = 128, 32, 128
+
+
+def _swz(q, k):
+    return q ^ (k & 28)
+
+
+def ffma_plan(dims, mode, R, sms=148):
+    order = len(dims)
+    P = int(np.prod(dims[:mode])) if mode else 1
+    Q = dims[mode]
+    S = int(np.prod(dims[mode + 1:])) if mode + 1 < order else 1
+    kind = 0 if mode == 0 else 1
+    rows0 = dims[1] if mode == 0 else dims[0]
+    if rows0 % FK or (kind == 0 and Q % 4):
+        return None
+    BR = 32 if R <= 32 else 64
+    rtiles = -(-R // BR)
+    Rp = rtiles * BR
+    qtiles = -(-Q // FQ)
+    psteps = P // FK if kind else 0
+    steps = S * psteps if kind else S // FK
+    want = -(-(2 * sms) // (qtiles * rtiles))
+    splits = max(1, min(want, steps))
+    chunk = -(-steps // splits)
+    splits = -(-steps // chunk)
+    return dict(P=P, Q=Q, S=S, kind=kind, rows0=rows0, BR=BR, rtiles=rtiles, Rp=Rp, qtiles=qtiles,
+                psteps=psteps, steps=steps, chunk=chunk, splits=splits)
+
+
+def ffma_restated(X, dims, facs, mode, R, sms=148):
+    """FP64 evaluation of the kernel's data movement; asserts every global
+    and shared access in bounds and returns the summed result (Q x R)."""
+    p = ffma_plan(dims, mode, R, sms)
+    P, Q, kind, rows0, BR, Rp = p["P"], p["Q"], p["kind"], p["rows0"], p["BR"], p["Rp"]
+    order = len(dims)
+    gen = [m for m in range(order) if m != mode and (kind == 0 or m < mode)]
+    outer = [m for m in range(order) if m != mode and kind == 1 and m > mode]
+    U = [f.reshape(dims[m], R, order="F") for m, f in enumerate(facs)]
+    U0p = np.zeros((rows0, Rp))
+    U0p[:, :R] = U[gen[0]]
+    part = np.zeros((p["splits"], R, Q))
+    t = np.arange(FT)
+    rv, kb, kstep = t % (BR // 4), t // (BR // 4), FT // (BR // 4)
+    NB = BR * FK // 4 // FT
+    blk_stages = rows0 // FK
+    nX = X.size
+    for bx in range(p["qtiles"] * p["splits"]):
+        q0, z = (bx % p["qtiles"]) * FQ, bx // p["qtiles"]
+        for by in range(p["rtiles"]):
+            r0 = by * BR
+            acc = np.zeros((FQ, BR))
+            sbeg, send = z * p["chunk"], min(p["steps"], z * p["chunk"] + p["chunk"])
+            for st in range(sbeg, send):
+                As = np.full((FK, FQ), np.nan)
+                Bs = np.full((FK, BR), np.nan)
+                if kind == 0:
+                    k0 = st * FK
+                    i0 = k0 % rows0
+                    blk, s = k0 // rows0, 0
+                    for i in range(8):
+                        e = t + FT * i
+                        k, qv = e >> 5, e & 31
+                        q = q0 + 4 * qv
+                        ok = q < Q
+                        addr = q + Q * (k0 + k)
+                        assert (addr[ok] + 3 < nX).all() and (addr[ok] % 4 == 0).all()
+                        for j in range(4):
+                            col = _swz(4 * qv, k) + j
+                            assert (col < FQ).all()
+                            As[k, col] = np.where(ok, X[np.where(ok, addr + j, 0)], 0.0)
+                else:
+                    s = st // p["psteps"]
+                    p0 = (st - s * p["psteps"]) * FK
+                    i0 = p0 % rows0
+                    blk = p0 // rows0
+                    for i in range(8):
+                        e = t + FT * i
+                        pv, q = e & 7, e >> 3
+                        ok = q0 + q < Q
+                        addr = p0 + 4 * pv + P * (q0 + q + Q * s)
+                        assert (addr[ok] + 3 < nX).all() and (addr[ok] % 4 == 0).all()
+                        for j in range(4):
+                            k = 4 * pv + j
+                            As[k, _swz(q, k)] = np.where(ok, X[np.where(ok, addr + j, 0)], 0.0)
+                # constant row: other generating factors (digits of blk), outer (digits of s)
+                c = np.ones(Rp)
+                b = blk
+                for m in gen[1:]:
+                    c[:R] *= U[m][b % dims[m]]
+                    b //= dims[m]
+                ss = s
+                for m in outer:
+                    c[:R] *= U[m][ss % dims[m]]
+                    ss //= dims[m]
+                for i in range(NB):
+                    row = i0 + kb + kstep * i
+                    assert (row < rows0).all() and (r0 + 4 * rv + 3 < Rp).all()
+                    for j in range(4):
+                        Bs[kb + kstep * i, 4 * rv + j] = U0p[row, r0 + 4 * rv + j] * c[r0 + 4 * rv + j]
+                assert not np.isnan(As).any() and not np.isnan(Bs).any()
+                # compute: thread (tq, tr) reads logical q = 8 tq + i at swz
+                A = np.empty((FK, FQ))
+                for k in range(FK):
+                    for g in range(FQ // 4):
+                        A[k, 4 * g:4 * g + 4] = As[k, _swz(4 * g, k):_swz(4 * g, k) + 4]
+                acc += A.T @ Bs
+            for r in range(BR):
+                if r0 + r < R:
+                    n = min(FQ, Q - q0)
+                    part[z, r0 + r, q0:q0 + n] = acc[:n, r]
+    return part.sum(0).T
+
+
+@pytest.mark.parametrize("dims,R,mode", [((128, 64, 32), 16, 0), ((128, 64, 32), 16, 1), ((128, 64, 32), 16, 2),
+                                         ((36, 96, 40), 40, 0), ((64, 20, 12), 70, 1), ((32, 9, 7), 5, 2),
+                                         ((32, 64, 3, 5), 12, 3), ((260, 32, 6), 8, 0)])
+def test_ffma_mttkrp_restated_matches_oracle(dims, R, mode):
+    import oracle
+    rng = np.random.default_rng(sum(dims) + R + mode)
+    X = rng.random(int(np.prod(dims))).astype(np.float32).astype(np.float64)
+    facs = [rng.random(d * R).astype(np.float32).astype(np.float64) for d in dims]
+    got = ffma_restated(X, dims, facs, mode, R, sms=3)
+    want = oracle.mttkrp(X, dims, facs, mode, R)
+    assert np.abs(got.reshape(-1, order="F") - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_ffma_plan_limits():
+    # eligible shapes and the ones that fall back to the general kernel
+    assert ffma_plan((512, 512, 512), 0, 64)["splits"] * 4 <= 2 * 148 + 4
+    assert ffma_plan((96, 96, 96, 96), 2, 32)["BR"] == 32
+    assert ffma_plan((37, 8, 8), 1, 8) is None       # rows0 not a multiple of 32
+    assert ffma_plan((38, 64, 8), 0, 8) is None       # mode 0 rows not a multiple of 4

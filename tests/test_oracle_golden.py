@@ -133,3 +133,28 @@ def test_numpy_baseline_matches_oracle_sweep():
     oracle.numpy_cp_als_sweep(X3, F)
     for f, g, d in zip(F, facs, dims):
         np.testing.assert_allclose(f.reshape(-1, order="F"), g, rtol=1e-9, atol=1e-12)
+
+
+def test_cpu_baseline_als_matches_oracle():
+    """The C++/OpenMP CPU baseline (oracle/cpu_als.cpp) computes the same ALS
+    as the FP64 oracle: in FP64 the factors and fits agree to rounding, and
+    its MTTKRP matches at orders 3 and 4."""
+    rng = np.random.default_rng(12)
+    for dims, R in (((20, 16, 12), 4), ((9, 8, 7, 6), 3)):
+        X = oracle.gencp(dims, [rng.random(d * R) for d in dims], R) + 1e-3 * rng.standard_normal(int(np.prod(dims)))
+        X = X.astype(np.float32).astype(np.float64)
+        init = [rng.random(d * R).astype(np.float32).astype(np.float64) for d in dims]
+        for mode in range(len(dims)):
+            got = oracle.cpu_mttkrp(X, dims, init, mode, R, threads=3)
+            want = oracle.mttkrp(X, dims, init, mode, R)
+            assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+        facs, fits, sweeps, _ = oracle.cpu_cp_als(X, dims, R, init, 8, threads=3)
+        wfacs, wfits, wsweeps = oracle.cp_als(X, dims, R, init, 8)
+        assert sweeps == wsweeps == 8
+        assert np.abs(fits - wfits).max() <= 1e-9
+        for f, w in zip(facs, wfacs):
+            assert np.abs(f - w).max() <= 1e-7 * np.abs(w).max()
+        # FP32 arithmetic stays close to FP64
+        f32, fits32, _, _ = oracle.cpu_cp_als(X.astype(np.float32), dims, R, [i.astype(np.float32) for i in init], 8,
+                                              threads=3)
+        assert abs(fits32[-1] - wfits[-1]) <= 1e-4
