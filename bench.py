@@ -11,9 +11,12 @@ bytes per MTTKRP) divided by the sweep time, in GB/s, summed over ranks.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the reference's CPU path (the ALS of
-decomposition/CPU/python/mycp.py, restated on NumPy/OpenBLAS because
-TensorLy is not installed) on a bounded slab of the same workload, on this
-host's cores, and reports the same metric.
+decomposition/CPU/python/mycp.py, TensorLy on NumPy in FP64, restated on
+NumPy/OpenBLAS because TensorLy is not installed) on the same workload, on
+this host's cores, and reports the same metric.  The line of our arm also
+times the reference's own GPU MTTKRP (its cuBLAS Khatri-Rao + SGEMM calls and
+its public FP16 mttkrp) beside ours on the same GPU, and a C++/OpenMP CPU
+baseline.
 """
 from __future__ import annotations
 
@@ -156,13 +159,14 @@ def cpu_sweep_gbs(X3, factors, sweeps=1):
     return sweep_bytes(dims, R) * sweeps / dt / 1e9, dt
 
 
-def cpu_sample(dims, R, seed=0, slab=64):
-    """A bounded slab (first `slab` indices of the last mode) of the same
-    synthetic workload, generated on the host."""
+def cpu_sample(dims, R, seed=0, slab=0):
+    """The same synthetic workload generated on the host (FP64 holding FP32
+    values), or a slab of it (the first `slab` indices of the last mode)."""
     import numpy as np
     rng = np.random.default_rng(seed)
     d = list(dims)
-    d[-1] = min(slab, d[-1])
+    if slab > 0:
+        d[-1] = min(slab, d[-1])
     facs = [rng.random((n, R)) for n in d]
     K = facs[1]
     for m in range(2, len(d)):
@@ -174,12 +178,59 @@ def cpu_sample(dims, R, seed=0, slab=64):
     return X, init, d
 
 
+def cpu_baseline_leg(dims, R, X, init, args, sweeps=3):
+    """C++/OpenMP (oracle/cpu_als.cpp) ALS sweeps of the bench's own tensor
+    and start in FP32 on every host core; config 0 (128^3 rank 16) time to
+    the fit of the FP32 GPU path's stopping rule (<= 50 sweeps or delta fit
+    < 1e-6) in FP32 and FP64; one sweep of 96^4 rank 32; and one NumPy FP64
+    sweep of the full tensor (the port the --impl reference arm times)."""
+    import numpy as np
+    import oracle
+    threads = oracle.cpu_threads()
+    Xh = X.cpu().numpy()
+    init_h = [u.cpu().numpy() for u in init]
+    oracle.cpu_cp_als(Xh, dims, R, [u.copy() for u in init_h], 1)  # warm the threads and pages
+    _, fits, sw, sec = oracle.cpu_cp_als(Xh, dims, R, [u.copy() for u in init_h], sweeps)
+    value = sweep_bytes(dims, R) * sw / sec / 1e9
+    out = {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+           "sample": f"{sw} ALS sweeps of the full {'x'.join(map(str, dims))} rank-{R} FP32 tensor from the "
+                     f"bench's start, {sec:.2f} s; C++/OpenMP restatement of decomposition/CPU/python/mycp.py "
+                     f"(oracle/cpu_als.cpp), FP32 arithmetic, {threads} threads",
+           "seconds_per_sweep": round(sec / sw, 4)}
+    rng = np.random.default_rng(10)
+    d0, R0 = (128, 128, 128), 16
+    f0 = [rng.random(n * R0) for n in d0]
+    X0 = oracle.gencp(d0, f0, R0)
+    X0 = (X0 + 1e-3 * np.linalg.norm(X0) / np.sqrt(X0.size) * rng.standard_normal(X0.size)).astype(np.float32)
+    i0 = [rng.random(n * R0).astype(np.float32) for n in d0]
+    ttf = {}
+    for name, dt in (("fp32", np.float32), ("fp64", np.float64)):
+        _, fits0, sw0, sec0 = oracle.cpu_cp_als(X0.astype(dt), d0, R0, [u.astype(dt) for u in i0], 50, tol=1e-6)
+        ttf[name] = {"seconds": round(sec0, 4), "sweeps": sw0, "fit": round(float(fits0[-1]), 8)}
+    out["cp_128x128x128_r16_time_to_fit"] = ttf
+    d1, R1 = (96, 96, 96, 96), 32
+    X1 = rng.random(int(np.prod(d1)), dtype=np.float32)
+    i1 = [rng.random(n * R1).astype(np.float32) for n in d1]
+    _, _, sw1, sec1 = oracle.cpu_cp_als(X1, d1, R1, i1, 1)
+    out["cp_96x96x96x96_r32_sweep"] = {"seconds": round(sec1, 4),
+                                       "gbs": round(sweep_bytes(d1, R1) / sec1 / 1e9, 3)}
+    X3 = np.asfortranarray(Xh.reshape(tuple(reversed(dims))).transpose(2, 1, 0).astype(np.float64))
+    F = [u.reshape(R, n).T.astype(np.float64).copy() for u, n in zip(init_h, dims)]
+    gbs_np, dt_np = cpu_sweep_gbs(X3, F, 1)
+    out["numpy_fp64_port"] = {"gbs": round(gbs_np, 3), "seconds_per_sweep": round(dt_np, 4),
+                              "cores": os.cpu_count()}
+    return out
+
+
 def run_reference(args):
-    """--impl reference: the reference's CPU ALS on the host cores."""
+    """--impl reference: the reference's CPU ALS (decomposition/CPU/python/
+    mycp.py, TensorLy on the NumPy backend, FP64) on the host cores, restated
+    on NumPy/OpenBLAS because TensorLy is not installed; the full workload
+    unless --cpu-slab asks for a slab."""
     import numpy as np
     dims = [int(x) for x in args.dims.split(",")]
     R = args.rank
-    X3, init, sd = cpu_sample(dims, R, slab=args.cpu_slab)
+    X3, init, sd = cpu_sample(dims, R, slab=args.cpu_slab if args.cpu_slab > 0 else dims[-1])
     cores = os.cpu_count()
     for _ in range(max(0, args.warmup)):
         cpu_sweep_gbs(X3, [f.copy() for f in init], 1)
@@ -197,8 +248,8 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
         "config": config_dict(dims, R, "fp64-numpy"),
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": cores, "kind": "port",
-                         "sample": f"one ALS sweep per step on a {sd[0]}x{sd[1]}x{sd[2]} slab "
-                                   f"(rank {R}) of the workload; NumPy/OpenBLAS restatement of "
+                         "sample": f"one ALS sweep per step of the {'x'.join(map(str, sd))} rank-{R} "
+                                   f"tensor; NumPy/OpenBLAS (FP64) restatement of "
                                    f"decomposition/CPU/python/mycp.py"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -411,6 +462,39 @@ def run_tucker_once(cd, torch, dims, ranks):
     return out
 
 
+def batched_workload(cd, torch, n, seed=30):
+    """The batched CP-ALS workload: n tensors, dims uniform in [16, 96],
+    ranks in [4, 16], each a sum of rank-1 terms with uniform [0,1) factors
+    plus 1e-3 relative Gaussian noise, uniform [0,1) initial factors."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    dims = [tuple(int(x) for x in rng.integers(16, 97, 3)) for _ in range(n)]
+    ranks = [int(x) for x in rng.integers(4, 17, n)]
+    b = cd.Batch(dims, ranks)
+    g = torch.Generator(device="cuda").manual_seed(seed + 1)
+    for t, (d, r) in enumerate(zip(dims, ranks)):
+        facs = [torch.rand(x * r, generator=g, device="cuda") for x in d]
+        xv = b.x_view(t)
+        cd.gencp(xv, facs, d, r)
+        nz = torch.randn(xv.numel(), generator=g, device="cuda")
+        xv.add_(nz * (1e-3 * torch.linalg.norm(xv) / (xv.numel() ** 0.5)))
+        for m in range(3):
+            b.u_view(t, m).copy_(torch.rand(d[m] * r, generator=g, device="cuda"))
+    torch.cuda.synchronize()
+    return b, dims, ranks, rng
+
+
+def run_batched_once(cd, torch, n):
+    """Three batched sweeps (one kernel launch each, no graph) on the first n
+    tensors of the batched workload."""
+    b, dims, ranks, _ = batched_workload(cd, torch, n)
+    t0 = time.perf_counter()
+    fits, sweeps, launches = cd.cp_als_batched(b, max_sweeps=3, tol=0.0, use_graph=False)
+    torch.cuda.synchronize()
+    return {"tensors": n, "elements": sum(np_prod(d) for d in dims), "launches": launches,
+            "seconds": round(time.perf_counter() - t0, 4), "fit_mean": float(sum(fits) / len(fits))}
+
+
 def np_prod(xs):
     p = 1
     for x in xs:
@@ -424,21 +508,7 @@ def leg_batched(cd, torch, stream, sptr, n=4096):
     replay, autotuned launch shape; <= 50 sweeps or delta fit < 1e-6 per
     tensor.  Parity sample: 16 tensors through the plain path."""
     import numpy as np
-    rng = np.random.default_rng(30)
-    dims = [tuple(int(x) for x in rng.integers(16, 97, 3)) for _ in range(n)]
-    ranks = [int(x) for x in rng.integers(4, 17, n)]
-    b = cd.Batch(dims, ranks)
-    g = torch.Generator(device="cuda").manual_seed(31)
-    with torch.cuda.stream(stream):
-        for t, (d, r) in enumerate(zip(dims, ranks)):
-            facs = [torch.rand(x * r, generator=g, device="cuda") for x in d]
-            xv = b.x_view(t)
-            cd.gencp(xv, facs, d, r, stream=sptr)
-            nz = torch.randn(xv.numel(), generator=g, device="cuda")
-            xv.add_(nz * (1e-3 * torch.linalg.norm(xv) / (xv.numel() ** 0.5)))
-            for m in range(3):
-                b.u_view(t, m).copy_(torch.rand(d[m] * r, generator=g, device="cuda"))
-    stream.synchronize()
+    b, dims, ranks, rng = batched_workload(cd, torch, n)
     U0 = b.U.clone()
     t0 = time.perf_counter()
     th, cps = cd.cp_batched_tune(b, stream=sptr)
@@ -480,9 +550,9 @@ def leg_batched(cd, torch, stream, sptr, n=4096):
 def leg_warmstart(cd, torch, n_train, n_eval):
     """Learned warm start: 64^3 rank-8 smooth-factor tensors, network trained
     on n_train ALS solutions the library generates (fresh tensors, 10 epochs
-    over them), then sweeps and time to each tensor's reference fit - 1e-4
-    from random, HOSVD, learned and judged (better of HOSVD and learned after
-    one sweep) starts on n_eval held-out tensors."""
+    over them), the judge's rule chosen on 2048 calibration tensors, then
+    sweeps and time to each tensor's reference fit - 1e-4 from random, HOSVD,
+    learned and judged starts on n_eval held-out tensors."""
     import warmstart
     w = warmstart.WarmStart(I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256)
     torch.cuda.synchronize()
@@ -491,7 +561,9 @@ def leg_warmstart(cd, torch, n_train, n_eval):
                      warmup=400)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
+    cal = w.calibrate(2048, id0=5 * 10 ** 8)
     ev = w.evaluate(n_eval, id0=10 ** 9)
+    ev["judge_calibration"] = cal
     ev["train"] = {"samples": n_train, "epochs": 10, "seconds": round(train_s, 2),
                    "loss_first": round(losses[0][1], 6) if losses else None,
                    "loss_last": round(losses[-1][1], 6) if losses else None}
@@ -718,7 +790,8 @@ def main():
     ap.add_argument("--rank", type=int, default=64)
     ap.add_argument("--precision", default="default")
     ap.add_argument("--e2e-sweeps", type=int, default=10)
-    ap.add_argument("--cpu-slab", type=int, default=64)
+    ap.add_argument("--cpu-slab", type=int, default=0,
+                    help="last-mode slices of the CPU baseline's sample (0 = the whole tensor)")
     ap.add_argument("--no-ttf", action="store_true", help="skip the time-to-fit runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-refgpu", action="store_true",
@@ -729,12 +802,15 @@ def main():
                     help="run one Tucker HOSVD and one HOOI sweep on --dims with --tucker-ranks "
                          "(profiling runs) and exit")
     ap.add_argument("--tucker-ranks", default="16,16,16,16")
+    ap.add_argument("--only-batched", type=int, default=0, metavar="N",
+                    help="run 3 batched CP-ALS sweeps (one kernel launch each, no graph) on the first N "
+                         "tensors of the batched workload (profiling runs) and exit")
     ap.add_argument("--kreps", type=int, default=10, help="timed MTTKRP launches per mode")
     ap.add_argument("--kwarm", type=int, default=3, help="untimed MTTKRP launches per mode")
     ap.add_argument("--legs", default="cp128,order4,tucker,batched,warmstart,streamed",
                     help="side workloads to add as extra keys (comma list, or 'none')")
     ap.add_argument("--ws-train", type=int, default=204800, help="warm-start training samples")
-    ap.add_argument("--ws-eval", type=int, default=4096, help="warm-start held-out tensors")
+    ap.add_argument("--ws-eval", type=int, default=10240, help="warm-start held-out tensors")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -762,6 +838,10 @@ def main():
     R = args.rank
     prec = cd.PRECISIONS[args.precision]
     prec_name = "bf16x3" if prec in (cd.PREC_DEFAULT, cd.PREC_BF16X3) else args.precision
+    if args.only_batched:
+        if rank == 0:
+            print(json.dumps(run_batched_once(cd, torch, args.only_batched)), flush=True)
+        return
     if args.only_tucker:
         if rank == 0:
             print(json.dumps(run_tucker_once(cd, torch, dims, [int(x) for x in args.tucker_ranks.split(",")])),
@@ -972,14 +1052,14 @@ def main():
             result["reference_gpu"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
         torch.cuda.synchronize()
 
-    # ---- CPU baseline (rank 0, bounded sample)
+    # ---- CPU baseline (rank 0): the C++/OpenMP restatement of mycp.py's
+    # ALS on the host cores at the full workload, plus its time to fit on the
+    # 128^3 workload and a sweep of the 96^4 one; the NumPy port beside it
     if rank == 0 and world == 1 and not args.no_cpu:
-        X3, cinit, sd = cpu_sample(dims, R, slab=args.cpu_slab)
-        gbs, dt = cpu_sweep_gbs(X3, cinit, 1)
-        result["cpu_baseline"] = {
-            "value": round(gbs, 3), "unit": "GB/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"one ALS sweep on a {sd[0]}x{sd[1]}x{sd[2]} slab (rank {R}), "
-                      f"{dt:.2f} s; NumPy/OpenBLAS restatement of decomposition/CPU/python/mycp.py"}
+        try:
+            result["cpu_baseline"] = cpu_baseline_leg(dims, R, X, init, args)
+        except Exception as exc:
+            result["cpu_baseline"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
 
     if dist:
         dist.barrier()

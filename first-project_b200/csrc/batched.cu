@@ -4,12 +4,14 @@
 //
 // Each CTA pulls tensors from a work queue (largest first) and runs one full
 // sweep of that tensor on its own, everything on-chip except X:
-//   * the three factor matrices live in shared memory (<= 96 x 16 each);
-//   * each MTTKRP streams X through shared memory one frontal slice
-//     (I x J) at a time and contracts it with register-blocked FMA (the
-//     ranks are too small for tensor cores to pay): mode 1 over j, modes 2
-//     and 3 over i, with the slice's C row as the per-slice weight (mode 3
-//     reduces the slice to one row of M);
+//   * the three factor matrices live in shared memory (<= 96 x 16 each,
+//     row-major with the ranks padded to 16 with zeros);
+//   * each MTTKRP reads X straight from global memory into registers with
+//     the lanes of a warp along the tensor's contiguous index i (one
+//     coalesced 128-byte request per load) and contracts it against factor
+//     rows broadcast from shared memory (the ranks are too small for tensor
+//     cores to pay); mode 1 keeps each lane's own row of M, modes 2 and 3
+//     sum the lanes' terms by a recursive-halving shuffle (mttkrp_lanes);
 //   * the R x R normal equations (Hadamard of the FP64 Grams) are inverted
 //     by Gauss-Jordan in shared memory (FP64), with a tiny diagonal shift
 //     retried when a pivot is not positive;
@@ -18,9 +20,8 @@
 //     converged and skipped by later sweeps.
 // The host captures `sweeps_per_graph` sweeps (queue reset + kernel) in one
 // CUDA graph and replays it until every tensor has converged or hit the
-// sweep limit.  The CTA size, the CTAs per SM and the MTTKRP register tile's
-// height come from a small autotuner
-// (batched_tune) that times one sweep per candidate on the batch itself and
+// sweep limit.  The CTA size and the CTAs per SM come from a small autotuner
+// (batched_tune) that times two sweeps per candidate on the batch itself and
 // caches the winner per batch shape class.
 #include <atomic>
 #include <map>
@@ -36,15 +37,7 @@ namespace {
 
 constexpr int BMAXD = 96;    // largest mode size handled (smem sizing)
 constexpr int BMAXR = 16;    // largest rank handled
-constexpr int B_RED3 = 2 * BMAXR * BMAXD;  // mode-3 partials: 2 RT groups x ranks x BMAXD / RT row groups
-
-__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+constexpr int RS = BMAXR;    // row stride of factors and results in shared memory (ranks padded)
 
 struct TensorMeta {
     long xoff;          // offset of X (elements) in the packed tensor buffer
@@ -72,12 +65,14 @@ struct BatchArgs {
     int *fallbacks;
 };
 
-// shared memory layout (floats / doubles), sized for BMAXD x BMAXR
+// Shared memory of a CTA of NW warps: the factors and the MTTKRP result
+// row-major (rank contiguous, ranks padded to RS with zeros), and the
+// per-warp partial results.
+template <int NW>
 struct BatchSmem {
-    float F[3][BMAXD * BMAXR];       // factors, column-major I_m x R
-    float slice[2][BMAXD * (BMAXD + 1) + 4];  // two frontal slices (double buffer), row stride I + 1
-    float M[BMAXD * BMAXR];          // MTTKRP result of the current mode
-    float red3[B_RED3];              // mode-3 per-slice partials (group x rank x row group)
+    float F[3][BMAXD * RS];
+    float M[BMAXD * RS];
+    float Mp[NW][BMAXD * RS];
     double V[BMAXR * BMAXR];         // normal matrix / its inverse
     double rowk[BMAXR], colk[BMAXR];
     double red[32];
@@ -85,189 +80,165 @@ struct BatchSmem {
     int fail;
 };
 
-template <int NT>
-__device__ void load_factors(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t) {
+template <int NT, class Smem>
+__device__ void load_factors(Smem &sm, const BatchArgs &a, const TensorMeta &t) {
     for (int m = 0; m < 3; m++) {
         const float *src = a.U + t.uoff[m];
-        const int n = t.dims[m] * t.R;
-        for (int e = threadIdx.x; e < n; e += NT) sm.F[m][e] = src[e];
+        const int I = t.dims[m];
+        for (int e = threadIdx.x; e < I * RS; e += NT) {
+            const int i = e / RS, r = e - i * RS;
+            sm.F[m][e] = (r < t.R) ? src[i + I * r] : 0.f;
+        }
     }
 }
 
-// M (I_mode x R) = MTTKRP of mode `mode` with the factors in shared memory.
-// Thread items: (RT consecutive rows, 4 ranks) with rows = i (mode 1) or j
-// (modes 2, 3) -- an RT x 4 register tile, RT x 4 FMAs per RT + 4 shared
-// loads; RT (2 or 4) is the autotuner's tile height.  The loads are not
-// guarded: rows past the mode's end read the slice's padding column or the
-// next column, ranks past R read the factor arrays' spare columns (all
-// inside the buffers since BMAXD is a multiple of RT), and those products
-// only reach accumulators that are never stored.  When the items leave
-// threads idle, S <= 2 RT groups of threads split the inner contraction
-// (over j, or over i) and their partials are added at the end (modes 1, 2)
-// or per slice (mode 3) in group order.  The frontal slices stream through
-// two shared-memory buffers with cp.async: slice k + 1 loads while slice k
-// is contracted.  (A deeper ring measured slower: the contraction's
-// instruction issue, not the load latency, sets the pace.)
-template <int NT, int RT>
-__device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
-    constexpr int GS = 2 * RT;          // most groups splitting one contraction
-    constexpr int NGM = BMAXD / RT;     // row groups at most
-    constexpr int IPB = (NGM * (BMAXR / 4) + NT - 1) / NT;
-    static_assert(BMAXD % RT == 0, "row tiles must divide BMAXD");
-    static_assert(GS * BMAXR * NGM <= B_RED3, "mode-3 partials");
-    const int I = t.dims[0], J = t.dims[1], K = t.dims[2], R = t.R;
-    const int ld = I + 1;
-    const float *X = a.X + t.xoff;
-    const int Q = t.dims[mode];
-    const int rows = (mode == 0) ? I : J;
-    const int ngrp = (rows + RT - 1) / RT;
-    const int rq = (R + 3) / 4;
-    const int items = ngrp * rq;
-    const int S = max(1, min(GS, NT / max(1, items)));
-    const int L = (mode == 0) ? J : I;  // contraction length within a slice
-    // this thread: item it = tid % items' (u = 0 when split), group g
-    const int g = (S > 1) ? (int)threadIdx.x / items : 0;
-    const int l0 = g * L / S, l1 = (g + 1) * L / S;
-    float acc[IPB][RT][4];
+// Sum of v[0..RP) over the warp's 32 lanes by recursive halving (levels
+// with shuffle offsets 16, 8, ... each keep half of the values a lane
+// holds); afterwards lane l holds the total of rank l >> (5 - L).  RP is 4,
+// 8 or 16.  Every lane of the warp must call it.
+template <int RP>
+__device__ __forceinline__ float lane_sum(float (&v)[RP], int lane) {
+    constexpr int L = (RP == 16) ? 4 : (RP == 8) ? 3 : 2;
 #pragma unroll
-    for (int u = 0; u < IPB; u++)
+    for (int l = 0; l < L; l++) {
+        const int off = 16 >> l;
+        const int n = RP >> (l + 1);
+        const bool up = (lane & off) != 0;
 #pragma unroll
-        for (int v = 0; v < RT; v++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) acc[u][v][c] = 0.f;
-    auto issue = [&](int k) {  // slice k into buffer k & 1, as one cp.async group
-        const float *src = X + (long)k * I * J;
-        float *dst = sm.slice[k & 1];
-        int i = threadIdx.x % I, j = threadIdx.x / I;
-        const int di = NT % I, dj = NT / I;
-        for (int e = threadIdx.x; e < I * J; e += NT) {
-            cp_async4(&dst[i + ld * j], src + e);
-            i += di;
-            j += dj;
-            if (i >= I) { i -= I; j++; }
+        for (int j = 0; j < n; j++) {
+            const float send = up ? v[j] : v[j + n];
+            const float keep = up ? v[j + n] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
         }
-        cp_async_commit();
-    };
-    __syncthreads();  // the previous user of the slice buffers is done
-    issue(0);
-    for (int k = 0; k < K; k++) {
-        if (k + 1 < K) {
-            issue(k + 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        const float *sl = sm.slice[k & 1];
-#pragma unroll
-        for (int u = 0; u < IPB; u++) {
-            const int it = (S > 1) ? ((u == 0 && (int)threadIdx.x < S * items) ? (int)threadIdx.x % items : items)
-                                   : (int)threadIdx.x + NT * u;
-            if (it >= items) continue;
-            const int rg = it % ngrp;
-            const int rp = rg * RT;
-            const int r0 = (it / ngrp) * 4;
-            float t2[RT][4];
-#pragma unroll
-            for (int v = 0; v < RT; v++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) t2[v][c] = 0.f;
-            if (mode == 0) {
-                // T[i, r] = sum_j X[i, j] B[j, r]
-                const float *xp = sl + rp;
-                const float *bp = sm.F[1] + J * r0;
-#pragma unroll 2
-                for (int j = l0; j < l1; j++) {
-                    float x[RT], b[4];
-#pragma unroll
-                    for (int v = 0; v < RT; v++) x[v] = xp[v + ld * j];
-#pragma unroll
-                    for (int c = 0; c < 4; c++) b[c] = bp[j + J * c];
-#pragma unroll
-                    for (int v = 0; v < RT; v++)
-#pragma unroll
-                        for (int c = 0; c < 4; c++) t2[v][c] = fmaf(x[v], b[c], t2[v][c]);
-                }
-            } else {
-                // T[j, r] = sum_i X[i, j] A[i, r]
-                const float *xp = sl + ld * rp;
-                const float *ap = sm.F[0] + I * r0;
-#pragma unroll 2
-                for (int i = l0; i < l1; i++) {
-                    float x[RT], av[4];
-#pragma unroll
-                    for (int v = 0; v < RT; v++) x[v] = xp[i + ld * v];
-#pragma unroll
-                    for (int c = 0; c < 4; c++) av[c] = ap[i + I * c];
-#pragma unroll
-                    for (int v = 0; v < RT; v++)
-#pragma unroll
-                        for (int c = 0; c < 4; c++) t2[v][c] = fmaf(x[v], av[c], t2[v][c]);
-                }
-            }
-            if (mode < 2) {
-                const float *cp = sm.F[2] + K * r0 + k;
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const float w = cp[K * c];
-#pragma unroll
-                    for (int v = 0; v < RT; v++) acc[u][v][c] = fmaf(t2[v][c], w, acc[u][v][c]);
-                }
-            } else {
-                // this row group's (and thread group's) share of M[k, r] = sum_j T[j, r] B[j, r]
-                const float *Bf = sm.F[1];
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const int r = r0 + c;
-                    float v = 0.f;
-                    if (r < R)
-#pragma unroll
-                        for (int w = 0; w < RT; w++)
-                            if (rp + w < J) v = fmaf(t2[w][c], Bf[rp + w + J * r], v);
-                    sm.red3[(g * BMAXR + r0 + c) * NGM + rg] = v;
-                }
-            }
-        }
-        if (mode == 2) {
-            // sum over groups and row groups: one warp per rank, lanes over
-            // the row groups, then a fixed shuffle tree (deterministic)
-            __syncthreads();
-            const int lane = threadIdx.x & 31;
-            for (int r = threadIdx.x >> 5; r < R; r += NT / 32) {
-                float v = 0.f;
-                for (int gg = 0; gg < S; gg++)
-                    for (int p2 = lane; p2 < ngrp; p2 += 32) v += sm.red3[(gg * BMAXR + r) * NGM + p2];
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) sm.M[k + K * r] = v;
-            }
-        }
-        __syncthreads();  // slice k's buffer is refilled by the next issue
     }
-    if (mode < 2) {
-        // groups' partials added in group order: group 0 writes, the others
-        // add in turn
-        for (int gg = 0; gg < S; gg++) {
+    float s = v[0];
 #pragma unroll
-            for (int u = 0; u < IPB; u++) {
-                const int it = (S > 1) ? ((u == 0 && (int)threadIdx.x < S * items) ? (int)threadIdx.x % items : items)
-                                       : (int)threadIdx.x + NT * u;
-                if (it >= items || g != gg) continue;
-                const int rp = (it % ngrp) * RT;
-                const int r0 = (it / ngrp) * 4;
+    for (int off = 16 >> L; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    return s;
+}
+
+// M (row-major, I_mode x RS) = MTTKRP of mode `mode`, factors in shared
+// memory.  The lanes of a warp run along i, the tensor's contiguous index
+// (32 rows per warp, ceil(I / 32) warps per row chunk), so every load of X
+// is one coalesced 128-byte request and goes straight into registers; the
+// warps of a chunk split the outer index into contiguous ranges:
+//   mode 0: M[i, :] = sum_k C[k, :] * sum_j X[i, j, k] B[j, :]
+//           (outer k, inner j; the lane's own row, no cross-lane sum)
+//   mode 1: M[j, :] = sum_i A[i, :] * sum_k X[i, j, k] C[k, :]
+//   mode 2: M[k, :] = sum_i A[i, :] * sum_j X[i, j, k] B[j, :]
+//           (outer j or k; the lanes' terms summed by lane_sum)
+// Two outer indices at a time, four inner ones unrolled: eight loads in
+// flight per lane, and each broadcast factor row (RP/4 16-byte shared
+// loads) feeds 2 RP FMAs.  Partials of the warps (mode 0: per outer range;
+// modes 1, 2: per row chunk) are combined in a fixed order.  RP = the rank
+// rounded up to 4, 8 or 16; the padding ranks are zero.
+template <int NW, int RP>
+__device__ void mttkrp_lanes(BatchSmem<NW> &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
+    const int I = t.dims[0], J = t.dims[1], K = t.dims[2];
+    const float *X = a.X + t.xoff;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int LI = (I + 31) >> 5;
+    const int NG = NW / LI;
+    const int ic = warp % LI, g = warp / LI;
+    const int i = ic * 32 + lane;
+    const bool valid = i < I;
+    const long IJ = (long)I * J;
+    const int O = (mode == 1) ? J : K;        // outer index
+    const int Nn = (mode == 1) ? K : J;       // inner index
+    const long so = (mode == 1) ? I : IJ;     // X strides of the outer and inner index
+    const long sn = (mode == 1) ? IJ : I;
+    const float *Vf = (mode == 1) ? sm.F[2] : sm.F[1];  // the inner index's factor rows
+    const int o0 = (g < NG) ? (int)((long)O * g / NG) : O;
+    const int o1 = (g < NG) ? (int)((long)O * (g + 1) / NG) : O;
+    float acc[RP];
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const int r = r0 + c;
-                    if (r < R)
+    for (int r = 0; r < RP; r++) acc[r] = 0.f;
+    const float *xi = X + (valid ? i : 0);
+    for (int o = o0; o < o1; o += 2) {
+        const bool two = o + 1 < o1;
+        float t0[RP], t1[RP];
 #pragma unroll
-                        for (int v = 0; v < RT; v++)
-                            if (rp + v < Q) {
-                                if (gg == 0) sm.M[rp + v + Q * r] = acc[u][v][c];
-                                else sm.M[rp + v + Q * r] += acc[u][v][c];
-                            }
+        for (int r = 0; r < RP; r++) { t0[r] = 0.f; t1[r] = 0.f; }
+        const float *x0 = xi + so * o;
+        const float *x1 = xi + so * (two ? o + 1 : o);
+        const bool l0 = valid, l1 = valid && two;
+        int n = 0;
+        for (; n + 4 <= Nn; n += 4) {
+            float xa[4], xb[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                xa[u] = l0 ? __ldg(x0 + sn * (n + u)) : 0.f;
+                xb[u] = l1 ? __ldg(x1 + sn * (n + u)) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float *vr = Vf + (n + u) * RS;
+#pragma unroll
+                for (int r4 = 0; r4 < RP; r4 += 4) {
+                    const float4 v = *reinterpret_cast<const float4 *>(vr + r4);
+                    t0[r4 + 0] = fmaf(xa[u], v.x, t0[r4 + 0]); t1[r4 + 0] = fmaf(xb[u], v.x, t1[r4 + 0]);
+                    t0[r4 + 1] = fmaf(xa[u], v.y, t0[r4 + 1]); t1[r4 + 1] = fmaf(xb[u], v.y, t1[r4 + 1]);
+                    t0[r4 + 2] = fmaf(xa[u], v.z, t0[r4 + 2]); t1[r4 + 2] = fmaf(xb[u], v.z, t1[r4 + 2]);
+                    t0[r4 + 3] = fmaf(xa[u], v.w, t0[r4 + 3]); t1[r4 + 3] = fmaf(xb[u], v.w, t1[r4 + 3]);
                 }
             }
-            __syncthreads();
         }
+        for (; n < Nn; n++) {
+            const float xa = l0 ? __ldg(x0 + sn * n) : 0.f;
+            const float xb = l1 ? __ldg(x1 + sn * n) : 0.f;
+            const float *vr = Vf + n * RS;
+#pragma unroll
+            for (int r4 = 0; r4 < RP; r4 += 4) {
+                const float4 v = *reinterpret_cast<const float4 *>(vr + r4);
+                t0[r4 + 0] = fmaf(xa, v.x, t0[r4 + 0]); t1[r4 + 0] = fmaf(xb, v.x, t1[r4 + 0]);
+                t0[r4 + 1] = fmaf(xa, v.y, t0[r4 + 1]); t1[r4 + 1] = fmaf(xb, v.y, t1[r4 + 1]);
+                t0[r4 + 2] = fmaf(xa, v.z, t0[r4 + 2]); t1[r4 + 2] = fmaf(xb, v.z, t1[r4 + 2]);
+                t0[r4 + 3] = fmaf(xa, v.w, t0[r4 + 3]); t1[r4 + 3] = fmaf(xb, v.w, t1[r4 + 3]);
+            }
+        }
+        if (mode == 0) {
+            const float *c0 = sm.F[2] + o * RS;
+            const float *c1 = sm.F[2] + (two ? o + 1 : o) * RS;
+#pragma unroll
+            for (int r4 = 0; r4 < RP; r4 += 4) {
+                const float4 u = *reinterpret_cast<const float4 *>(c0 + r4);
+                const float4 w = *reinterpret_cast<const float4 *>(c1 + r4);
+                acc[r4 + 0] = fmaf(t1[r4 + 0], w.x, fmaf(t0[r4 + 0], u.x, acc[r4 + 0]));
+                acc[r4 + 1] = fmaf(t1[r4 + 1], w.y, fmaf(t0[r4 + 1], u.y, acc[r4 + 1]));
+                acc[r4 + 2] = fmaf(t1[r4 + 2], w.z, fmaf(t0[r4 + 2], u.z, acc[r4 + 2]));
+                acc[r4 + 3] = fmaf(t1[r4 + 3], w.w, fmaf(t0[r4 + 3], u.w, acc[r4 + 3]));
+            }
+        } else {
+            // the lane's terms A[i, :] * t, summed over the lanes (rows i)
+            const float *ar = sm.F[0] + (valid ? i : 0) * RS;
+#pragma unroll
+            for (int r4 = 0; r4 < RP; r4 += 4) {
+                const float4 u = *reinterpret_cast<const float4 *>(ar + r4);
+                t0[r4 + 0] *= u.x; t0[r4 + 1] *= u.y; t0[r4 + 2] *= u.z; t0[r4 + 3] *= u.w;
+                t1[r4 + 0] *= u.x; t1[r4 + 1] *= u.y; t1[r4 + 2] *= u.z; t1[r4 + 3] *= u.w;
+            }
+            const float s0 = lane_sum<RP>(t0, lane);
+            const float s1 = lane_sum<RP>(t1, lane);
+            constexpr int SH = (RP == 16) ? 1 : (RP == 8) ? 2 : 3;
+            if ((lane & ((1 << SH) - 1)) == 0) {
+                const int r = lane >> SH;
+                sm.Mp[ic][o * RS + r] = s0;
+                if (two) sm.Mp[ic][(o + 1) * RS + r] = s1;
+            }
+        }
+    }
+    if (mode == 0 && g < NG && valid) {
+#pragma unroll
+        for (int r = 0; r < RP; r++) sm.Mp[g][i * RS + r] = acc[r];
+    }
+    __syncthreads();
+    const int Q = t.dims[mode];
+    const int nparts = (mode == 0) ? NG : LI;
+    for (int e = threadIdx.x; e < Q * RS; e += NW * 32) {
+        if ((e & (RS - 1)) >= RP) continue;  // padding ranks: never read
+        float v = 0.f;
+        for (int p = 0; p < nparts; p++) v += sm.Mp[p][e];
+        sm.M[e] = v;
     }
     __syncthreads();
 }
@@ -275,8 +246,8 @@ __device__ void mttkrp_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta
 // V = Hadamard of the Grams other than `mode`; V <- V^-1 (Gauss-Jordan).
 // Leaves sm.fail set when both attempts met a non-positive pivot (V is then
 // not an inverse and the caller keeps the old factor).
-template <int NT>
-__device__ void normal_inverse_small(BatchSmem &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
+template <int NT, class Smem>
+__device__ void normal_inverse_small(Smem &sm, const BatchArgs &a, const TensorMeta &t, int mode) {
     const int R = t.R;
     for (int attempt = 0; attempt < 2; attempt++) {
         for (int e = threadIdx.x; e < R * R; e += NT) {
@@ -320,10 +291,13 @@ __device__ void normal_inverse_small(BatchSmem &sm, const BatchArgs &a, const Te
     }
 }
 
-template <int NT, int RT>
-__global__ void __launch_bounds__(NT) k_batch_sweep(BatchArgs a) {
+// One ALS sweep of every tensor not yet converged: CTAs of NW warps pull
+// tensors from the queue.
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) k_batch_sweep(BatchArgs a) {
+    constexpr int NT = NW * 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BatchSmem &sm = *reinterpret_cast<BatchSmem *>(smem_raw);
+    BatchSmem<NW> &sm = *reinterpret_cast<BatchSmem<NW> *>(smem_raw);
     for (;;) {
         if (threadIdx.x == 0) {
             unsigned w = atomicAdd(a.queue, 1u);
@@ -340,31 +314,34 @@ __global__ void __launch_bounds__(NT) k_batch_sweep(BatchArgs a) {
         __syncthreads();
         double inner = 0.0;
         for (int mode = 0; mode < 3; mode++) {
-            mttkrp_small<NT, RT>(sm, a, t, mode);
+            if (R <= 4) mttkrp_lanes<NW, 4>(sm, a, t, mode);
+            else if (R <= 8) mttkrp_lanes<NW, 8>(sm, a, t, mode);
+            else mttkrp_lanes<NW, 16>(sm, a, t, mode);
             normal_inverse_small<NT>(sm, a, t, mode);
-            // U_mode = M V^-1 (FP64 accumulation), into shared and global memory
+            // U_mode = M V^-1 (FP64 accumulation), into shared (row-major)
+            // and global (column-major) memory
             const int Q = t.dims[mode];
             float *Ug = a.U + t.uoff[mode];
             const bool keep = sm.fail != 0;  // singular twice: keep the old factor
             double part = 0.0;
             for (int e = threadIdx.x; e < Q * R; e += NT) {
                 const int q = e % Q, c = e / Q;
-                float u = sm.F[mode][e];
+                float u = sm.F[mode][q * RS + c];
                 if (!keep) {
                     double s = 0.0;
-                    for (int r = 0; r < R; r++) s = fma((double)sm.M[q + Q * r], sm.V[r + R * c], s);
+                    for (int r = 0; r < R; r++) s = fma((double)sm.M[q * RS + r], sm.V[r + R * c], s);
                     u = (float)s;
-                    sm.F[mode][e] = u;
+                    sm.F[mode][q * RS + c] = u;
                     Ug[e] = u;
                 }
-                if (mode == 2) part += (double)sm.M[e] * (double)u;
+                if (mode == 2) part += (double)sm.M[q * RS + c] * (double)u;
             }
             __syncthreads();
             // Gram of the new factor
             for (int e = threadIdx.x; e < R * R; e += NT) {
                 const int p = e % R, q2 = e / R;
                 double s = 0.0;
-                for (int i = 0; i < Q; i++) s = fma((double)sm.F[mode][i + Q * p], (double)sm.F[mode][i + Q * q2], s);
+                for (int i = 0; i < Q; i++) s = fma((double)sm.F[mode][i * RS + p], (double)sm.F[mode][i * RS + q2], s);
                 t.G[mode][e] = s;
             }
             if (mode == 2) {
@@ -373,7 +350,7 @@ __global__ void __launch_bounds__(NT) k_batch_sweep(BatchArgs a) {
             }
             __syncthreads();
             if (mode == 2 && threadIdx.x == 0) {
-                for (int w = 0; w < NT / 32; w++) inner += sm.red[w];
+                for (int w = 0; w < NW; w++) inner += sm.red[w];
             }
         }
         __syncthreads();
@@ -441,32 +418,34 @@ struct BatchState {
     int *fallbacks = nullptr;
 };
 
-template <int NT, int RT>
+template <int NW>
 int launch_sweep(const BatchArgs &a, int ctas_per_sm, cudaStream_t s) {
     static std::atomic<bool> attr[64];  // per device; zero-initialised
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
-        CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NT, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(BatchSmem)));
+        CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(BatchSmem<NW>)));
         attr[dev].store(true, std::memory_order_release);
     }
     CUD_CHECK(cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s));
-    k_batch_sweep<NT, RT><<<kNumSMs * ctas_per_sm, NT, sizeof(BatchSmem), s>>>(a);
+    k_batch_sweep<NW><<<kNumSMs * ctas_per_sm, NW * 32, sizeof(BatchSmem<NW>), s>>>(a);
     CUD_CHECK_LAUNCH("batched sweep");
     return CUD_OK;
 }
 
-// Launch shape: threads per CTA, CTAs per SM, rows of the MTTKRP register
-// tile.
+// Launch shape: threads per CTA (warps x 32) and CTAs per SM.
 struct BatchCfg {
-    int threads, ctas, rt;
+    int threads, ctas;
 };
 
 int launch_cfg(const BatchArgs &a, const BatchCfg &c, cudaStream_t s) {
-    if (c.rt == 4)
-        return c.threads == 128 ? launch_sweep<128, 4>(a, c.ctas, s) : launch_sweep<256, 4>(a, c.ctas, s);
-    return c.threads == 128 ? launch_sweep<128, 2>(a, c.ctas, s) : launch_sweep<256, 2>(a, c.ctas, s);
+    switch (c.threads) {
+        case 128: return launch_sweep<4>(a, c.ctas, s);
+        case 192: return launch_sweep<6>(a, c.ctas, s);
+        case 256: return launch_sweep<8>(a, c.ctas, s);
+        default: return launch_sweep<12>(a, c.ctas, s);
+    }
 }
 
 // Autotuner cache: shape class -> launch shape
@@ -551,7 +530,7 @@ int batched_impl(int ntensors, const long *dims, const long *ranks, const float 
 
     // launch shape from the autotuner (threads per CTA, CTAs per SM, tile rows)
     long key = shape_class(ntensors, hd.data(), hr.data());
-    BatchCfg cfg{256, 2, 4};
+    BatchCfg cfg{192, 3};
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(key);
@@ -646,12 +625,11 @@ extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *r
         hr[t] = (int)ranks[t];
     }
     long key = shape_class(ntensors, hd.data(), hr.data());
-    const int shapes[][2] = {{128, 2}, {128, 3}, {128, 4}, {256, 1}, {256, 2}, {256, 3}};
-    std::vector<BatchCfg> cand;
-    for (int rt : {2, 4})
-        for (auto &sh : shapes) cand.push_back({sh[0], sh[1], rt});
+    // (threads, CTAs per SM) that fit in shared memory: BatchSmem<NW> is
+    // ~52 KB at 4 warps, ~64 KB at 6, ~77 KB at 8, ~101 KB at 12
+    const std::vector<BatchCfg> cand = {{128, 3}, {128, 4}, {192, 2}, {192, 3}, {256, 2}, {384, 2}};
     float best = 1e30f;
-    BatchCfg bestc{256, 2, 4};
+    BatchCfg bestc{192, 3};
     cudaStream_t s = as_stream(stream);
     cudaEvent_t e0, e1;
     CUD_CHECK(cudaEventCreate(&e0));

@@ -808,16 +808,22 @@ __global__ void __launch_bounds__(256) k_pack_b(KrFactors fold, long R, int Rpad
     const int rem = (int)(id - t * 4 * Rpad);
     const int kc = rem / Rpad, r = rem - kc * Rpad;
     float v[8];
+    if (fold.n == 1) {
+        // U0's own rows (no index arithmetic)
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-        long lin = 32 * t + 8 * kc + j;
-        float p = 1.f;
-        for (int f = 0; f < fold.n; f++) {
-            const long d = fold.rows[f], qd = lin / d;
-            p *= (r < R) ? __ldg(fold.U[f] + (lin - qd * d) + (long)r * d) : 0.f;
-            lin = qd;
+        for (int j = 0; j < 8; j++) v[j] = (r < R) ? __ldg(fold.U[0] + 32 * t + 8 * kc + j + (long)r * fold.rows[0]) : 0.f;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            long lin = 32 * t + 8 * kc + j;
+            float p = 1.f;
+            for (int f = 0; f < fold.n; f++) {
+                const long d = fold.rows[f], qd = lin / d;
+                p *= (r < R) ? __ldg(fold.U[f] + (lin - qd * d) + (long)r * d) : 0.f;
+                lin = qd;
+            }
+            v[j] = (r < R) ? p : 0.f;
         }
-        v[j] = (r < R) ? p : 0.f;
     }
     const bool three = (prec == CUD_PREC_BF16X3 || prec == CUD_PREC_DEFAULT);
     uint4 h, l;

@@ -14,6 +14,8 @@
 // along mode 0.  Per-CTA partials are summed in a fixed order by a second
 // kernel, so the result is deterministic.
 //
+// Shapes that allow it take an FFMA-tiled fast path (k_residual_ffma below).
+//
 // Unlike the fit the ALS sweep derives from its last MTTKRP
 // (||X||^2 - 2<M, U> + ||Xh||^2, which cancels catastrophically when the fit
 // is close to 1 and inherits the MTTKRP's rounding), this value depends only
@@ -179,6 +181,187 @@ __global__ void __launch_bounds__(256) k_sum_pairs(const double *part, long n, d
     if (threadIdx.x == 0) { out[0] = red[0][0]; out[1] = red[1][0]; }
 }
 
+// ---------------------------------------------------------------------------
+// FFMA fast path (R <= 64, mode-0 rows a multiple of 4, U_1's rows a
+// multiple of 32, X and U_1 16-byte aligned): the SGEMM-style tile of the
+// plain FP32 MTTKRP, transposed.  A CTA owns RQ = 128 rows q of mode 0 with
+// their U_0 rows staged once in shared memory (rank-major), and walks a
+// contiguous range of RK = 32-column stages of the "rest" index; a stage's
+// 32 Khatri-Rao columns are 32 consecutive rows of U_1 times one constant
+// row c (the other factors' rows, fixed for a block of rows_1 / 32 stages),
+// formed in FP32 into a double-buffered shared tile.  Each of the 128
+// threads rebuilds an 8 x 4 patch of the reconstruction in registers
+// (xh = sum_r U_0[q, r] KR[col, r], FP32, r in order), takes the difference
+// with the matching X values (16-byte loads, prefetched one stage ahead)
+// and adds (x - xh)^2 and x^2 of the stage in FP32 to FP64 totals.
+// Per-CTA totals go to the partial pairs summed by k_sum_pairs.
+constexpr int RQ = 128, RK = 32, RTH = 128, RRMAX = 64;
+
+struct ResFArgs {
+    const float *X;
+    const float *U0;
+    long I0, rest;
+    int R, rows1;
+    KrFactors f;    // U_1 .. U_{N-1}, fastest first (f.U[0] = U_1)
+    long stages, chunk;
+    double *part;   // [grid][2]
+};
+
+__global__ void __launch_bounds__(RTH, 3) k_residual_ffma(ResFArgs a) {
+    __shared__ __align__(16) float As[RRMAX][RQ];
+    __shared__ __align__(16) float Bs[2][RRMAX][RK];
+    // the end-of-kernel reduction reuses the B tiles (after the last barrier)
+    double(*red)[RTH / 32] = reinterpret_cast<double(*)[RTH / 32]>(&Bs[0][0][0]);
+    const int t = threadIdx.x, tq = t >> 3, tk = t & 7;
+    const long qtiles = (a.I0 + RQ - 1) / RQ;
+    const long q0 = (blockIdx.x % qtiles) * RQ;
+    const long z = blockIdx.x / qtiles;
+    const long sbeg = z * a.chunk, send = min(a.stages, sbeg + a.chunk);
+    const int R = a.R;
+    for (int e = t; e < RRMAX * RQ; e += RTH) {
+        const int r = e / RQ, q = e - r * RQ;
+        As[r][q] = (r < R && q0 + q < a.I0) ? a.U0[q0 + q + a.I0 * r] : 0.f;
+    }
+    const int blk_stages = a.rows1 / RK;
+    const long qa = q0 + 8 * tq;          // this thread's rows qa .. qa + 7
+    const bool ok0 = qa < a.I0, ok1 = qa + 4 < a.I0;
+    float4 rb[4], xv[4][2], xn[4][2];
+    float cr[4] = {0.f, 0.f, 0.f, 0.f};
+    // B slots of this thread: ranks tq + 16 i, columns 4 tk .. 4 tk + 3
+    auto loadB = [&](long st) {
+        const long k0 = st * RK;
+        const long i1 = k0 % a.rows1;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int r = tq + 16 * i;
+            rb[i] = (r < R) ? __ldg(reinterpret_cast<const float4 *>(a.f.U[0] + i1 + 4 * tk + (long)a.rows1 * r))
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (st == sbeg || (st % blk_stages) == 0) {
+            // the constant row: digits of the block index over U_2, U_3, ...
+            uint32_t lin = (uint32_t)(k0 / a.rows1);
+#pragma unroll
+            for (int i = 0; i < 4; i++) cr[i] = (tq + 16 * i < R) ? 1.f : 0.f;
+            for (int m = 1; m < a.f.n; m++) {
+                const uint32_t d = (uint32_t)a.f.rows[m], qd = lin / d;
+                const float *row = a.f.U[m] + (lin - qd * d);
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int r = tq + 16 * i;
+                    if (r < R) cr[i] *= __ldg(row + (long)d * r);
+                }
+                lin = qd;
+            }
+        }
+    };
+    auto loadX = [&](long st, float4 (&x)[4][2]) {
+        const long c0 = st * RK + 4 * tk;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float *p = a.X + qa + a.I0 * (c0 + c);
+            x[c][0] = ok0 ? __ldcs(reinterpret_cast<const float4 *>(p)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            x[c][1] = ok1 ? __ldcs(reinterpret_cast<const float4 *>(p + 4)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    auto storeB = [&](int buf) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            float4 v = rb[i];
+            v.x *= cr[i]; v.y *= cr[i]; v.z *= cr[i]; v.w *= cr[i];
+            *reinterpret_cast<float4 *>(&Bs[buf][tq + 16 * i][4 * tk]) = v;
+        }
+    };
+    double acc = 0.0, xx = 0.0;
+    if (sbeg < send) {
+        loadB(sbeg);
+        storeB(0);
+        loadX(sbeg, xv);
+    }
+    __syncthreads();
+    for (long st = sbeg; st < send; st++) {
+        const int cur = (int)((st - sbeg) & 1);
+        const bool more = st + 1 < send;
+        if (more) {
+            loadB(st + 1);
+            loadX(st + 1, xn);
+        }
+        float h[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) h[i][c] = 0.f;
+#pragma unroll 4
+        for (int r = 0; r < R; r++) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&As[r][8 * tq]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&As[r][8 * tq + 4]);
+            const float4 b = *reinterpret_cast<const float4 *>(&Bs[cur][r][4 * tk]);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) h[i][c] = fmaf(av[i], bv[c], h[i][c]);
+        }
+        float sr = 0.f, sx = 0.f;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float x[8] = {xv[c][0].x, xv[c][0].y, xv[c][0].z, xv[c][0].w,
+                                xv[c][1].x, xv[c][1].y, xv[c][1].z, xv[c][1].w};
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const float d = x[i] - h[i][c];
+                sr = fmaf(d, d, sr);
+                sx = fmaf(x[i], x[i], sx);
+            }
+        }
+        // rows past I0 read zeros: their h is zero too (U_0 rows zero)
+        acc += (double)sr;
+        xx += (double)sx;
+        if (more) {
+            storeB(cur ^ 1);
+#pragma unroll
+            for (int c = 0; c < 4; c++) { xv[c][0] = xn[c][0]; xv[c][1] = xn[c][1]; }
+        }
+        __syncthreads();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        xx += __shfl_xor_sync(0xffffffffu, xx, o);
+    }
+    if ((t & 31) == 0) {
+        red[0][t >> 5] = acc;
+        red[1][t >> 5] = xx;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int w = 0; w < RTH / 32; w++) { s0 += red[0][w]; s1 += red[1][w]; }
+        a.part[2 * blockIdx.x] = s0;
+        a.part[2 * blockIdx.x + 1] = s1;
+    }
+}
+
+// Launch plan of the fast path; false when the shape or R does not allow it.
+bool residual_ffma_plan(int order, const long *dims, long R, long &qtiles, long &stages, long &chunk,
+                        long &splits) {
+    if (order < 2 || R <= 0 || R > RRMAX) return false;
+    const long I0 = dims[0], rows1 = dims[1];
+    if (I0 % 4 != 0 || rows1 % RK != 0 || I0 > 0x7fffffffL) return false;
+    long rest = 1;
+    for (int m = 1; m < order; m++) {
+        if (dims[m] > 0x7fffffffL) return false;
+        rest *= dims[m];
+    }
+    qtiles = (I0 + RQ - 1) / RQ;
+    stages = rest / RK;
+    if (rest / rows1 > 0xffffffffL) return false;  // block index in 32 bits
+    const long want = (3L * kNumSMs + qtiles - 1) / qtiles;
+    splits = std::max(1L, std::min(want, stages));
+    chunk = (stages + splits - 1) / splits;
+    splits = (stages + chunk - 1) / chunk;
+    return qtiles * splits <= 0x7fffffffL;
+}
+
 void residual_grid(long I0, long rest, unsigned &gx, unsigned &gy) {
     gx = (unsigned)((I0 + TI - 1) / TI);
     const long nchunks = (rest + TJ - 1) / TJ;
@@ -193,7 +376,11 @@ size_t cp_residual_ws_bytes(int order, const long *dims) {
     for (int m = 1; m < order; m++) rest *= dims[m];
     unsigned gx, gy;
     residual_grid(dims[0], rest, gx, gy);
-    return sizeof(double) * (2 * (size_t)gx * gy + 2);
+    size_t parts = (size_t)gx * gy;
+    long qt, st, ch, sp;
+    // the fast path's grid, for any rank (the partials are all it needs)
+    if (residual_ffma_plan(order, dims, 1, qt, st, ch, sp)) parts = std::max(parts, (size_t)(qt * sp));
+    return sizeof(double) * (2 * parts + 2);
 }
 
 int cp_residual(const float *X, int order, const long *dims, const float *const *U, long R, double *out2,
@@ -213,6 +400,26 @@ int cp_residual(const float *X, int order, const long *dims, const float *const 
         a.f.n++;
     }
     a.part = static_cast<double *>(ws);
+    long qt, stg, ch, sp;
+    if (residual_ffma_plan(order, dims, R, qt, stg, ch, sp) && ((reinterpret_cast<uintptr_t>(X) |
+                                                               reinterpret_cast<uintptr_t>(U[1])) & 15) == 0) {
+        ResFArgs f;
+        f.X = X;
+        f.U0 = U[0];
+        f.I0 = dims[0];
+        f.rest = a.rest;
+        f.R = (int)R;
+        f.rows1 = (int)dims[1];
+        f.f = a.f;
+        f.stages = stg;
+        f.chunk = ch;
+        f.part = a.part;
+        k_residual_ffma<<<(unsigned)(qt * sp), RTH, 0, s>>>(f);
+        CUD_CHECK_LAUNCH("cp_residual ffma");
+        k_sum_pairs<<<1, 256, 0, s>>>(a.part, qt * sp, out2);
+        CUD_CHECK_LAUNCH("cp_residual sum");
+        return CUD_OK;
+    }
     unsigned gx, gy;
     residual_grid(a.I0, a.rest, gx, gy);
     k_cp_residual<<<dim3(gx, gy), NT, 0, s>>>(a);

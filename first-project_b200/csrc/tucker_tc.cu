@@ -166,13 +166,14 @@ __global__ void k_split_bf16(const float *__restrict__ a, __nv_bfloat16 *__restr
         put_split(hi, lo, e, a[e]);
 }
 
-// Three-term TTM finish: v = F2[e] (+ F2[e + n] when the two halves of
-// Th [Uh | Ul] were written side by side), written as FP32 (fout) or split
+// Three-term TTM finish: v = F2[e] + F2[e + n] + F3[e] (Th Uh, Th Ul and
+// Tl Uh, each GEMM's plain FP32 output), written as FP32 (fout) or split
 // into the next step's hi/lo operands.
-__global__ void k_ttm3_finish(const float *__restrict__ F2, long n, int halves, float *__restrict__ fout,
-                              __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+__global__ void k_ttm3_finish(const float *__restrict__ F2, const float *__restrict__ F3, long n,
+                              float *__restrict__ fout, __nv_bfloat16 *__restrict__ hi,
+                              __nv_bfloat16 *__restrict__ lo) {
     for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
-        const float v = halves ? F2[e] + F2[e + n] : F2[e];
+        const float v = (F2[e] + F2[e + n]) + F3[e];
         if (fout) fout[e] = v;
         else put_split(hi, lo, e, v);
     }
@@ -264,6 +265,7 @@ struct TcWork {
     __nv_bfloat16 *ub = nullptr;       // a factor in BF16 (three-term: hi then lo, 2 K r)
     __nv_bfloat16 *zl0 = nullptr, *zl1 = nullptr;  // three-term: low parts of the intermediates
     float *f2 = nullptr;               // three-term: FP32 TTM partials, 2 zmax
+    float *f3 = nullptr;               // three-term: FP32 partial Tl Uh, zmax
     float *yf = nullptr;               // three-term: the projection Y in FP32, zmax
     float *g32 = nullptr;              // Gram FP32
     double *g64 = nullptr, *W = nullptr, *V = nullptr;
@@ -304,6 +306,7 @@ int tc_alloc(int order, const long *dims, const long *ranks, bool three, TcWork 
     const size_t o_zl1 = off; off += three ? up(2 * (size_t)zmax) : 0;
     const size_t o_f2 = off; off += three ? up(4 * 2 * (size_t)zmax) : 0;
     const size_t o_yf = off; off += three ? up(4 * (size_t)zmax) : 0;
+    const size_t o_f3 = off; off += three ? up(4 * (size_t)zmax) : 0;
     const size_t o_g32 = off; off += up(4 * (size_t)maxd * maxd);
     const size_t o_g64 = off; off += up(8 * (size_t)maxd * maxd);
     const size_t o_W = off; off += up(8 * (size_t)maxd);
@@ -322,6 +325,7 @@ int tc_alloc(int order, const long *dims, const long *ranks, bool three, TcWork 
     w.zl1 = three ? (__nv_bfloat16 *)(p + o_zl1) : nullptr;
     w.f2 = three ? (float *)(p + o_f2) : nullptr;
     w.yf = three ? (float *)(p + o_yf) : nullptr;
+    w.f3 = three ? (float *)(p + o_f3) : nullptr;
     w.g32 = (float *)(p + o_g32);
     w.g64 = (double *)(p + o_g64);
     w.W = (double *)(p + o_W);
@@ -406,24 +410,25 @@ int ttm_fast(const TcWork &w, const __nv_bfloat16 *T, long K, long rest, const f
 // Three-term TTM over the fastest mode: (Th + Tl) (K x rest, K fastest) times
 // U (K x r, FP32) ~ Th Uh + Th Ul + Tl Uh -> (rest x r), r slowest, as FP32
 // into fout or as the hi/lo pair (zh, zl).  With 2 r <= 32 (the skinny GEMM's
-// width) Th is read once, against [Uh | Ul]; wider ranks take three GEMMs of
-// width r, accumulating in FP32.
+// width) Th is read once, against [Uh | Ul]; wider ranks take two GEMMs of
+// width r over Th.  Every GEMM writes its own plain FP32 output (the fast
+// epilogue) and one pass adds the three terms.
 int ttm3_fast(const TcWork &w, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl, long K, long rest, const float *U,
               long r, __nv_bfloat16 *zh, __nv_bfloat16 *zl, float *fout, cudaStream_t s) {
     if (gemm_tc_ws_bytes(rest, 2 * r, K) > w.gws_bytes) return CUD_ERR_INVALID_ARGUMENT;
     const __nv_bfloat16 *Uh = w.ub, *Ul = w.ub + K * r;
     k_split_bf16<<<gfor(K * r), 256, 0, s>>>(U, w.ub, w.ub + K * r, K * r);
     CUD_CHECK_LAUNCH("ttm3 factor split");
-    const bool halves = 2 * r <= 32;
     int st;
-    if (halves) {
+    if (2 * r <= 32) {
         if ((st = gemm_tc_bf16(Th, K, Uh, K, rest, 2 * r, K, epi_f32(w.f2, 1, rest, 0), w.gws, s))) return st;
     } else {
         if ((st = gemm_tc_bf16(Th, K, Uh, K, rest, r, K, epi_f32(w.f2, 1, rest, 0), w.gws, s))) return st;
-        if ((st = gemm_tc_bf16(Th, K, Ul, K, rest, r, K, epi_f32(w.f2, 1, rest, 1), w.gws, s))) return st;
+        if ((st = gemm_tc_bf16(Th, K, Ul, K, rest, r, K, epi_f32(w.f2 + rest * r, 1, rest, 0), w.gws, s)))
+            return st;
     }
-    if ((st = gemm_tc_bf16(Tl, K, Uh, K, rest, r, K, epi_f32(w.f2, 1, rest, 1), w.gws, s))) return st;
-    k_ttm3_finish<<<gfor(rest * r), 256, 0, s>>>(w.f2, rest * r, halves ? 1 : 0, fout, zh, zl);
+    if ((st = gemm_tc_bf16(Tl, K, Uh, K, rest, r, K, epi_f32(w.f3, 1, rest, 0), w.gws, s))) return st;
+    k_ttm3_finish<<<gfor(rest * r), 256, 0, s>>>(w.f2, w.f3, rest * r, fout, zh, zl);
     CUD_CHECK_LAUNCH("ttm3 finish");
     return CUD_OK;
 }

@@ -103,3 +103,51 @@ class CudaOps:
 
     def norm2(self, X):
         return self.cd.norm2(X, stream=self.stream)
+
+
+# ---------------------------------------------------------------- batched CP-ALS by tensor
+
+def shard_batch(dims, ranks, rank, world):
+    """The tensors of a batch that rank `rank` of `world` runs: a
+    longest-processing-time assignment by work (elements x rank, the cost of
+    an ALS sweep), largest first, ties to the lower rank; every tensor goes
+    to exactly one rank and the assignment is the same on every rank.  The
+    batch shards with no collective on the data path: the tensors are
+    independent."""
+    work = sorted(((-int(d[0]) * int(d[1]) * int(d[2]) * int(r), t) for t, (d, r) in enumerate(zip(dims, ranks))))
+    load = [0] * world
+    mine = []
+    for w, t in work:
+        k = min(range(world), key=lambda j: (load[j], j))
+        load[k] -= w
+        if k == rank:
+            mine.append(t)
+    return sorted(mine)
+
+
+class ShardedBatch:
+    """Batched CP-ALS over ranks: each rank packs its share of the tensors
+    (shard_batch) into its own cd.Batch and runs the persistent batched
+    kernel on its GPU; fits and sweeps are gathered once at the end (a
+    result collective, not a data-path one)."""
+
+    def __init__(self, cd, dims, ranks, rank, world):
+        self.cd, self.rank, self.world = cd, rank, world
+        self.all_dims, self.all_ranks = [tuple(d) for d in dims], list(ranks)
+        self.mine = shard_batch(dims, ranks, rank, world)
+        self.batch = cd.Batch([self.all_dims[t] for t in self.mine], [self.all_ranks[t] for t in self.mine])
+
+    def run(self, max_sweeps=50, tol=1e-6, stream=None):
+        fits, sweeps, launches = self.cd.cp_als_batched(self.batch, max_sweeps=max_sweeps, tol=tol, stream=stream)
+        return dict(zip(self.mine, zip(fits, sweeps))), launches
+
+    @staticmethod
+    def gather(dist, local, n):
+        """Per-tensor (fit, sweeps) of every rank's share, in tensor order."""
+        parts = [None] * dist.get_world_size()
+        dist.all_gather_object(parts, local)
+        out = [None] * n
+        for p in parts:
+            for t, v in p.items():
+                out[t] = v
+        return out

@@ -224,21 +224,77 @@ class WarmStart:
         n = b.n * 3 * self.I * self.R
         b.U[:n].copy_(torch.randn(n, device="cuda", generator=g))
 
-    def judged_init(self, b):
-        """Learned factors, judged against HOSVD: one ALS sweep from each, and
-        each tensor keeps the start with the better fit (its factors after
-        that sweep).  Never worse than the HOSVD start; costs the extra sweep
-        and the HOSVD initialisation."""
-        self.hosvd_init(b)
-        f_h, _, _ = cd.cp_als_batched(b, max_sweeps=1, tol=0.0)
-        U_h = b.U.clone()
-        self.learned_init(b)
-        f_l, _, _ = cd.cp_als_batched(b, max_sweeps=1, tol=0.0)
-        keep_h = torch.tensor([fh > fl for fh, fl in zip(f_h, f_l)], device="cuda")
+    # ---------------------------------------------------------------- the judge
+    # The judged start keeps plain HOSVD-initialised ALS as the fallback and
+    # lets the network's start in only where a rule, chosen on calibration
+    # tensors disjoint from training and evaluation, says it pays:
+    #   'hosvd'          the fallback alone (no network call);
+    #   race(k, delta)   k ALS sweeps from both starts, then per tensor the
+    #                    learned chain continues only if its fit leads the
+    #                    HOSVD chain's by more than delta.
+    # A rule's cost is the ALS sweeps it runs per tensor (race: the kept
+    # chain's sweeps to the target plus the discarded chain's, at most k);
+    # the cheapest rule wins and ties go to 'hosvd', so on the calibration
+    # set the judged start never costs more sweeps than HOSVD.
+    POLICIES = [("hosvd", 0, 0.0)] + [("race", k, d) for k in (1, 3, 5) for d in (0.0, 1e-4, 1e-3, 1e-2)]
+
+    def _runs(self, b, init, targets, max_sweeps, ks):
+        """Per tensor: the fit after each k in ks, and the sweeps to its
+        target (ALS trajectories are deterministic from a start)."""
+        fk = {}
+        for k in ks:
+            init(b)
+            f, _, _ = cd.cp_als_batched(b, max_sweeps=k, tol=0.0)
+            fk[k] = np.asarray(f)
+        init(b)
+        _, sweeps, _ = cd.cp_als_batched_target(b, targets, max_sweeps=max_sweeps)
+        return fk, np.asarray(sweeps, dtype=np.float64)
+
+    def calibrate(self, n_cal, id0, margin=1e-4, max_sweeps=200, ref_sweeps=200):
+        """Chooses the judge's rule on n_cal calibration tensors (ids id0..);
+        returns every rule's mean cost in sweeps and the chosen one."""
+        b, _ = self.batch(n_cal, id0)
+        ref, _, _ = cd.cp_als_batched(b, max_sweeps=ref_sweeps, tol=1e-9)
+        targets = [f - margin for f in ref]
+        ks = sorted({k for _, k, _ in self.POLICIES if k > 0})
+        fh, sh = self._runs(b, self.hosvd_init, targets, max_sweeps, ks)
+        fl, sl = self._runs(b, self.learned_init, targets, max_sweeps, ks)
+        costs = {}
+        for kind, k, d in self.POLICIES:
+            if kind == "hosvd":
+                costs[(kind, k, d)] = float(np.mean(sh))
+            else:
+                pick = fl[k] > fh[k] + d
+                kept = np.where(pick, sl, sh)
+                other = np.where(pick, sh, sl)
+                costs[(kind, k, d)] = float(np.mean(kept + np.minimum(k, other)))
+        self.policy = min(self.POLICIES, key=lambda c: (costs[c], c[0] != "hosvd"))
+        return {"n": n_cal, "chosen": list(self.policy),
+                "costs": {f"{c[0]}_{c[1]}_{c[2]:g}": round(v, 3) for c, v in costs.items()},
+                "learned_alone_sweeps": round(float(np.mean(sl)), 3), "hosvd_sweeps": round(float(np.mean(sh)), 3)}
+
+    def judged_run(self, b, targets, max_sweeps):
+        """ALS from the judged start under the calibrated rule.  Returns
+        (fits, sweeps run per tensor, sweep kernels)."""
+        kind, k, d = getattr(self, "policy", ("hosvd", 0, 0.0))
+        if kind == "hosvd":
+            self.hosvd_init(b)
+            return cd.cp_als_batched_target(b, targets, max_sweeps=max_sweeps)
         per = 3 * self.I * self.R
+        self.hosvd_init(b)
+        fh, swh, lh = cd.cp_als_batched_target(b, targets, max_sweeps=k)
+        U_h = b.U[: b.n * per].clone()
+        self.learned_init(b)
+        fl, swl, ll = cd.cp_als_batched_target(b, targets, max_sweeps=k)
+        pick = np.asarray(fl) > np.asarray(fh) + d
         Ub = b.U[: b.n * per].view(b.n, per)
-        Ub[keep_h] = U_h[: b.n * per].view(b.n, per)[keep_h]
-        return float(keep_h.float().mean().item())
+        keep_h = torch.tensor(~pick, device="cuda")
+        Ub[keep_h] = U_h.view(b.n, per)[keep_h]
+        raced = np.asarray(swl) + np.asarray(swh)
+        # every chain continues from its kept factors (one that reached its
+        # target in the race stops after one more sweep); all sweeps count
+        fits, sw, lc = cd.cp_als_batched_target(b, targets, max_sweeps=max(1, max_sweeps - k))
+        return list(fits), list(raced + np.asarray(sw)), lh + ll + lc
 
     def evaluate(self, n_eval, id0, margin=1e-4, max_sweeps=200, ref_sweeps=200):
         """Sweeps and time for random-, HOSVD-, learned- and judged-init ALS
@@ -251,13 +307,20 @@ class WarmStart:
         targets = [f - margin for f in ref_fits]
         out = {"n": n_eval, "margin": margin, "reference_fit_mean": float(np.mean(ref_fits))}
         for name, init in (("random", self.random_init), ("hosvd", self.hosvd_init), ("learned", self.learned_init),
-                           ("judged", self.judged_init)):
+                           ("judged", None)):
+            if name == "judged" and getattr(self, "policy", ("hosvd",))[0] == "hosvd":
+                # the judged start is the HOSVD start: the same run
+                out[name] = dict(out["hosvd"], policy="hosvd")
+                continue
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t0 = time.perf_counter()
             e0.record()
-            init(b)
-            fits, sweeps, launches = cd.cp_als_batched_target(b, targets, max_sweeps=max_sweeps)
+            if init is None:
+                fits, sweeps, launches = self.judged_run(b, targets, max_sweeps)
+            else:
+                init(b)
+                fits, sweeps, launches = cd.cp_als_batched_target(b, targets, max_sweeps=max_sweeps)
             e1.record()
             torch.cuda.synchronize()
             wall = time.perf_counter() - t0

@@ -105,3 +105,43 @@ def test_sharded_cp_matches_single_process(tmp_path, world):
     # the sharded last factor, reassembled
     C = np.concatenate([p[f"arr_{len(DIMS) - 1}"].reshape(-1, R, order="F") for p in parts])
     np.testing.assert_allclose(C.reshape(-1, order="F"), facs[-1], rtol=1e-8, atol=1e-10)
+
+
+def _shard_worker(rank, world, port, outdir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import json
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                    "first-project_b200"))
+    from distributed import shard_batch
+    rng = np.random.default_rng(30)
+    n = 300
+    dims = [tuple(int(x) for x in rng.integers(16, 97, 3)) for _ in range(n)]
+    ranks = [int(x) for x in rng.integers(4, 17, n)]
+    mine = shard_batch(dims, ranks, rank, world)
+    parts = [None] * world
+    dist.all_gather_object(parts, mine)
+    if rank == 0:
+        with open(os.path.join(outdir, "shards.json"), "w") as f:
+            json.dump({"parts": parts, "work": [int(np.prod(d)) * r for d, r in zip(dims, ranks)]}, f)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_batched_shards_by_tensor(tmp_path, world):
+    """Batched CP-ALS shards by tensor: every tensor on exactly one rank, the
+    ranks' work within one tensor's work of each other (greedy largest
+    first), each rank computing its share on its own (no data-path
+    collective)."""
+    import json
+    mp.start_processes(_shard_worker, args=(world, free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    d = json.loads((tmp_path / "shards.json").read_text())
+    parts, work = d["parts"], d["work"]
+    allt = sorted(t for p in parts for t in p)
+    assert allt == list(range(len(work)))
+    loads = [sum(work[t] for t in p) for p in parts]
+    assert max(loads) - min(loads) <= max(work)

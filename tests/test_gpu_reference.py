@@ -213,3 +213,28 @@ def test_reference_gpu_mttkrp_harness(dims, R):
             assert rel(h.result(mode), oracle.mttkrp(X, dims, facs, mode, R)) <= 1e-5, mode
     finally:
         h.close()
+
+
+def test_print_tensor_same_text_as_reference(tmp_path):
+    """printTensor (src/kr.cu:13-30): the same program linked against the
+    drop-in archive and against the reference library prints the same
+    bytes."""
+    if not os.path.exists(oracle.REF_LIB_PATH):
+        pytest.skip("reference library not built (oracle/Makefile ref)")
+    src = os.path.join(ROOT, "tests", "drivers", "print_tensor.cpp")
+    inc = os.path.join(ROOT, "include")
+    ours, theirs = tmp_path / "print_ours", tmp_path / "print_ref"
+    arc = os.path.join(ROOT, "first-project_b200", "libcutensordecomposition.a")
+    r = subprocess.run(["nvcc", "-o", str(ours), src, "-I", inc, arc, "-lcublas", "-lcusolver", "-lcurand"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    refdir = os.path.dirname(oracle.REF_LIB_PATH)
+    r = subprocess.run(["nvcc", "-o", str(theirs), src, "-I", inc, oracle.REF_LIB_PATH,
+                        f"-Xlinker=-rpath,{refdir}", "-lcublas", "-lcusolver", "-lcurand"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    a = subprocess.run([str(ours)], capture_output=True, text=True, timeout=120)
+    b = subprocess.run([str(theirs)], capture_output=True, text=True, timeout=120)
+    assert a.returncode == 0 and b.returncode == 0, (a.stderr, b.stderr)
+    assert a.stdout == b.stdout
+    assert a.stdout.count("-----------------------------------") == 2

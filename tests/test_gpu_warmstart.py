@@ -165,3 +165,26 @@ def test_trained_network_beats_random_start(cd, ws):
     w.model.close()
     assert res["learned"][0] < res["random"][0] - 5, res
     assert res["learned"][1] > res["random"][1], res
+
+
+def test_judged_start_never_costs_more_than_hosvd(cd, ws):
+    """The judged start: its rule is chosen on calibration tensors disjoint
+    from training and evaluation, among 'HOSVD alone' and races of k sweeps
+    from both starts; by construction its calibration cost in ALS sweeps is
+    at most HOSVD's.  On held-out tensors it must then stay at HOSVD's mean
+    sweeps (exactly, when the rule is HOSVD alone; within 2 sweeps
+    otherwise), and reach the target at least as often, less 2 %."""
+    w = ws.WarmStart(I=64, R=8, S=32, hidden=512, noise=1e-3, seed=1, max_batch=256)
+    w.train(51200, batch=256, lr=3e-4, chunk=4096, label_sweeps=3, epochs=10, warmup=200)
+    cal = w.calibrate(512, id0=5 * 10 ** 8)
+    costs = cal["costs"]
+    chosen = "_".join(str(x) if not isinstance(x, float) else f"{x:g}" for x in cal["chosen"])
+    assert costs[chosen] <= costs["hosvd_0_0"], cal
+    ev = w.evaluate(1024, id0=10 ** 9)
+    w.model.close()
+    h, j = ev["hosvd"], ev["judged"]
+    if cal["chosen"][0] == "hosvd":
+        assert j["sweeps_mean"] == h["sweeps_mean"] and j["seconds"] == h["seconds"]
+    else:
+        assert j["sweeps_mean"] <= h["sweeps_mean"] + 2, (cal, ev)
+    assert j["reached"] >= h["reached"] - 0.02, (cal, ev)

@@ -71,35 +71,124 @@ def test_cluster_rows_partition_and_fit(n):
             assert ntiles * ng <= CL_T and 4 * nt <= 32
 
 
-# ---- batched.cu mttkrp_small: RT x 4 register tiles with unguarded loads
-BMAXD, BMAXR = 96, 16
-SLICE = BMAXD * (BMAXD + 1) + 4
-RED3 = 2 * BMAXR * BMAXD
+# ---- batched.cu mttkrp_lanes: lanes along i, warps split the outer index,
+# recursive-halving lane sums, partials combined in a fixed order
+BMAXD, BMAXR, RS = 96, 16, 16
 
 
-@pytest.mark.parametrize("RT", [2, 4])
-def test_batched_tile_reads_stay_in_buffers(RT):
-    NGM = BMAXD // RT
-    worst_slice = worst_fac = worst_red = -1
-    for I in (16, 37, 94, 95, 96):
-        for J in (16, 53, 95, 96):
-            ld = I + 1
-            for mode in (0, 1):
-                rows = I if mode == 0 else J
-                ngrp = -(-rows // RT)
-                rp_max = (ngrp - 1) * RT
-                L = J if mode == 0 else I
-                if mode == 0:   # sl[rp + v + ld j], F[1][j + J (r0 + c)]
-                    worst_slice = max(worst_slice, rp_max + RT - 1 + ld * (L - 1))
-                    worst_fac = max(worst_fac, (L - 1) + J * (BMAXR - 1))
-                else:           # sl[i + ld (rp + v)], F[0][i + I (r0 + c)]
-                    worst_slice = max(worst_slice, (L - 1) + ld * (rp_max + RT - 1))
-                    worst_fac = max(worst_fac, (L - 1) + I * (BMAXR - 1))
-            ngrp = -(-J // RT)
-            worst_red = max(worst_red, (2 * RT * BMAXR - 1) * NGM + ngrp - 1)
-    assert worst_slice < SLICE
-    assert worst_fac < BMAXD * BMAXR
-    assert worst_red < RED3
+def lane_sum_restated(v):
+    """lane_sum<RP>: v is 32 lanes x RP values; returns the per-lane result
+    and checks lane l holds the total of rank l >> (5 - L)."""
+    RP = v.shape[1]
+    L = {16: 4, 8: 3, 4: 2}[RP]
+    v = v.copy()
+    lanes = np.arange(32)
+    for l in range(L):
+        off, n = 16 >> l, RP >> (l + 1)
+        up = (lanes & off) != 0
+        send = np.where(up[:, None], v[:, :n], v[:, n:2 * n])
+        keep = np.where(up[:, None], v[:, n:2 * n], v[:, :n])
+        v = keep + send[lanes ^ off]
+    s = v[:, 0].copy()
+    off = 16 >> L
+    while off >= 1:
+        s = s + s[lanes ^ off]
+        off >>= 1
+    return s, lanes >> (5 - L)
+
+
+@pytest.mark.parametrize("RP", [4, 8, 16])
+def test_lane_sum_totals_each_rank(RP):
+    rng = np.random.default_rng(RP)
+    v = rng.integers(-50, 50, (32, RP)).astype(np.float64)
+    s, rank = lane_sum_restated(v)
+    np.testing.assert_array_equal(s, v.sum(0)[rank])
+
+
+def batched_mttkrp_restated(X, dims, F, mode, R, NW):
+    """mttkrp_lanes<NW, RP> on the CPU: returns M (Q x R) and checks every
+    load in bounds, every output row written by one warp group."""
+    I, J, K = dims
+    RP = 4 if R <= 4 else 8 if R <= 8 else 16
+    Fp = [np.zeros((BMAXD, RS)) for _ in range(3)]
+    for m in range(3):
+        Fp[m][:dims[m], :R] = F[m]
+    LI = -(-I // 32)
+    NG = NW // LI
+    O = J if mode == 1 else K
+    Nn = K if mode == 1 else J
+    so, sn = (I, I * J) if mode == 1 else (I * J, I)
+    Vf = Fp[2] if mode == 1 else Fp[1]
+    Q = dims[mode]
+    Mp = np.full((NW, BMAXD * RS), np.nan)
+    lanes = np.arange(32)
+    written = np.zeros(O, int)
+    for warp in range(NW):
+        ic, g = warp % LI, warp // LI
+        i = ic * 32 + lanes
+        valid = i < I
+        o0 = O * g // NG if g < NG else O
+        o1 = O * (g + 1) // NG if g < NG else O
+        acc = np.zeros((32, RP))
+        for o in range(o0, o1, 2):
+            two = o + 1 < o1
+            t = [np.zeros((32, RP)), np.zeros((32, RP))]
+            for k, oo in enumerate((o, o + 1 if two else o)):
+                ok = valid & (two or k == 0)
+                for n in range(Nn):
+                    addr = np.where(valid, i, 0) + so * oo + sn * n
+                    assert (addr[ok] < X.size).all()
+                    x = np.where(ok, X[np.where(ok, addr, 0)], 0.0)
+                    assert n < BMAXD
+                    t[k] += x[:, None] * Vf[n, :RP][None, :]
+            if mode == 0:
+                acc += t[0] * Fp[2][o, :RP] + t[1] * Fp[2][o + 1 if two else o, :RP]
+            else:
+                a = Fp[0][np.where(valid, i, 0), :RP]
+                for k, oo in enumerate((o, o + 1)):
+                    if k == 1 and not two:
+                        break
+                    s, rank = lane_sum_restated(t[k] * a)
+                    SH = {16: 1, 8: 2, 4: 3}[RP]
+                    w = (lanes & ((1 << SH) - 1)) == 0
+                    Mp[ic, oo * RS + rank[w]] = s[w]
+                    if ic == 0:
+                        written[oo] += 1
+        if mode == 0 and g < NG:
+            for l in np.nonzero(valid)[0]:
+                Mp[g, i[l] * RS:i[l] * RS + RP] = acc[l]
+    nparts = NG if mode == 0 else LI
+    M = np.zeros((Q, R))
+    for q in range(Q):
+        for r in range(R):
+            M[q, r] = sum(Mp[p, q * RS + r] for p in range(nparts))
+    assert not np.isnan(M).any()
+    if mode != 0:
+        assert (written == 1).all()
+    return M
+
+
+@pytest.mark.parametrize("dims,R,NW", [((16, 20, 17), 4, 6), ((37, 16, 24), 7, 4), ((64, 19, 33), 12, 6),
+                                       ((96, 50, 18), 16, 12), ((70, 33, 41), 5, 8), ((33, 96, 16), 9, 6)])
+def test_batched_mttkrp_lanes_restated_matches_oracle(dims, R, NW):
+    import oracle
+    rng = np.random.default_rng(sum(dims) + R + NW)
+    X = rng.random(int(np.prod(dims))).astype(np.float32).astype(np.float64)
+    F = [rng.random((d, R)).astype(np.float32).astype(np.float64) for d in dims]
+    for mode in range(3):
+        M = batched_mttkrp_restated(X, dims, F, mode, R, NW)
+        want = oracle.mttkrp(X, dims, [f.reshape(-1, order="F") for f in F], mode, R).reshape(dims[mode], R, order="F")
+        assert np.abs(M - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_batched_shared_memory_fits():
+    # BatchSmem<NW>: F[3], M, Mp[NW] (floats, BMAXD x RS each), V and the
+    # pivot rows (doubles); the CTAs per SM of every tuning candidate fit
+    # in 228 KB (1 KB reserved per CTA)
+    for NW, ctas in ((4, 3), (4, 4), (6, 2), (6, 3), (8, 2), (12, 2)):
+        smem = 4 * BMAXD * RS * (4 + NW) + 8 * (BMAXR * BMAXR + 2 * BMAXR + 32) + 16
+        assert ctas * (smem + 1024) <= 228 * 1024, (NW, ctas, smem)
+        assert smem <= 232448
 
 
 # ---- gemm_tc.cu skinny GEMM: B resident for K <= 1024 plus an 8-deep A ring
@@ -391,3 +480,71 @@ def test_ffma_plan_limits():
     assert ffma_plan((96, 96, 96, 96), 2, 32)["BR"] == 32
     assert ffma_plan((37, 8, 8), 1, 8) is None       # rows0 not a multiple of 32
     assert ffma_plan((38, 64, 8), 0, 8) is None       # mode 0 rows not a multiple of 4
+
+
+# ---- residual.cu k_residual_ffma: 128 rows x 32-column stages, B = U_1 rows
+# x the constant row, 8 x 4 patches per thread, X float4 loads
+def residual_ffma_restated(X, dims, facs, R, sms=148):
+    I0, rows1 = dims[0], dims[1]
+    assert I0 % 4 == 0 and rows1 % 32 == 0 and R <= 64
+    rest = int(np.prod(dims[1:]))
+    qtiles = -(-I0 // 128)
+    stages = rest // 32
+    want = -(-(3 * sms) // qtiles)
+    splits = max(1, min(want, stages))
+    chunk = -(-stages // splits)
+    splits = -(-stages // chunk)
+    U = [f.reshape(d, R, order="F") for f, d in zip(facs, dims)]
+    As = np.zeros((64, 128))
+    t = np.arange(128)
+    tq, tk = t >> 3, t & 7
+    res = xx = 0.0
+    parts = 0
+    for bx in range(qtiles * splits):
+        q0, z = (bx % qtiles) * 128, bx // qtiles
+        As[:] = 0
+        n = min(128, I0 - q0)
+        As[:R, :n] = U[0][q0:q0 + n].T
+        for st in range(z * chunk, min(stages, z * chunk + chunk)):
+            k0 = st * 32
+            i1 = k0 % rows1
+            lin = k0 // rows1
+            c = np.ones(R)
+            for m in range(2, len(dims)):
+                c *= U[m][lin % dims[m]]
+                lin //= dims[m]
+            Bs = np.zeros((64, 32))
+            for i in range(4):
+                r = tq + 16 * i
+                ok = r < R
+                addr = i1 + 4 * tk + rows1 * r
+                assert (addr[ok] + 3 < rows1 * R).all()
+                for j in range(4):
+                    Bs[r[ok], 4 * tk[ok] + j] = facs[1][addr[ok] + j] * c[r[ok]]
+            H = As.T @ Bs                                 # 128 x 32
+            for c4 in range(4):
+                col = k0 + 4 * tk + c4
+                qa = q0 + 8 * tq
+                for half in range(2):
+                    ok = qa + 4 * half < I0
+                    addr = qa + 4 * half + I0 * col
+                    assert (addr[ok] + 3 < X.size).all() and (addr[ok] % 4 == 0).all()
+                    for j in range(4):
+                        x = np.where(ok, X[np.where(ok, addr + j, 0)], 0.0)
+                        h = H[8 * tq + 4 * half + j, 4 * tk + c4]
+                        res += float(np.sum(np.where(ok, (x - h) ** 2, 0.0)))
+                        xx += float(np.sum(x ** 2))
+        parts += 1
+    return res, xx, parts
+
+
+@pytest.mark.parametrize("dims,R", [((128, 64, 32), 16), ((260, 32, 6, 5), 7), ((36, 96, 40), 64), ((4, 32, 3), 3)])
+def test_residual_ffma_restated_matches_fp64(dims, R):
+    import oracle
+    rng = np.random.default_rng(sum(dims) + R)
+    facs = [rng.random(d * R) for d in dims]
+    X = oracle.gencp(dims, facs, R) + 0.01 * rng.standard_normal(int(np.prod(dims)))
+    res, xx, parts = residual_ffma_restated(X, dims, facs, R, sms=2)
+    want = float(np.sum((X - oracle.gencp(dims, facs, R)) ** 2))
+    assert abs(res - want) <= 1e-9 * want
+    assert abs(xx - float(np.sum(X ** 2))) <= 1e-12 * xx
