@@ -66,6 +66,11 @@ enum ScratchSlot {
 // Pinned host scalar buffer (for device->host reads of norms and fits).
 double *pinned_scalars();
 
+// Measurement hooks (runtime.cu): a CUDA event pair around a main kernel
+// when timing is enabled (cud_prof_enable); prof_begin returns -1 when off.
+int prof_begin(cudaStream_t s);
+void prof_end(int k, cudaStream_t s);
+
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

@@ -557,8 +557,10 @@ int mttkrp_simt_impl(const T *X, int order, const long *dims, const T *const *U,
             k_pack_rows<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(a.gen.U[0], f.rows0, (int)R, f.Rp, packed);
             CUD_CHECK_LAUNCH("mttkrp_ffma pack");
             dim3 grid((unsigned)(f.qtiles * f.splits), (unsigned)f.rtiles);
+            const int pk = prof_begin(s);
             if (f.BR == 32) k_mttkrp_ffma<32><<<grid, FT, 0, s>>>(fa);
             else k_mttkrp_ffma<64><<<grid, FT, 0, s>>>(fa);
+            prof_end(pk, s);
             CUD_CHECK_LAUNCH("mttkrp_ffma");
             k_sum_partials<float><<<blocks_for(R * v.Q, 256), 256, 0, s>>>(fa.part, (int)f.splits, R * v.Q, out);
             CUD_CHECK_LAUNCH("mttkrp_ffma reduce");
@@ -567,9 +569,11 @@ int mttkrp_simt_impl(const T *X, int order, const long *dims, const T *const *U,
     }
     if (rtiles > 65535 || qtiles * splits > 0x7fffffffL) return CUD_ERR_UNSUPPORTED;
     dim3 grid((unsigned)(qtiles * splits), (unsigned)rtiles);
+    const int pk = prof_begin(s);
     if (kind == 0) k_mttkrp_simt<0, T><<<grid, NT, 0, s>>>(a);
     else if (kind == 1) k_mttkrp_simt<1, T><<<grid, NT, 0, s>>>(a);
     else k_mttkrp_simt<2, T><<<grid, NT, 0, s>>>(a);
+    prof_end(pk, s);
     CUD_CHECK_LAUNCH("mttkrp_simt");
     k_sum_partials<T><<<blocks_for(R * v.Q, 256), 256, 0, s>>>(a.part, (int)splits, R * v.Q, out);
     CUD_CHECK_LAUNCH("mttkrp_simt reduce");

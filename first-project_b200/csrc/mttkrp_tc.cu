@@ -741,15 +741,16 @@ constexpr int PB_THREADS = 352;
 // at the digits of l / frows.
 template <class Ctrl>
 __device__ __forceinline__ float pb_const_row(const TcArgs &a, const Ctrl &sm, long g, int r) {
-    long lin = ((long)g * BKS) / a.frows;
+    // the block index fits 32 bits: stages < 2^31, so 32 g / frows < 2^31
+    uint32_t lin = (uint32_t)(((long)g * BKS) / a.frows);
     float c = 1.f;
     for (int f = a.fold; f < a.gen.n; f++) {
-        const long d = sm.grows[f], qd = lin / d;
+        const uint32_t d = (uint32_t)sm.grows[f], qd = lin / d;
         c *= __ldg(sm.gU[f] + (lin - qd * d) + (long)r * d);
         lin = qd;
     }
     for (int f = (a.fold > a.gen.n ? a.fold - a.gen.n : 0); f < a.outer.n; f++) {
-        const long d = sm.orows[f], qd = lin / d;
+        const uint32_t d = (uint32_t)sm.orows[f], qd = lin / d;
         c *= __ldg(sm.oU[f] + (lin - qd * d) + (long)r * d);
         lin = qd;
     }
@@ -802,6 +803,9 @@ __global__ void __launch_bounds__(256) k_pack_b(KrFactors fold, long R, int Rpad
                                                 uint8_t *__restrict__ pb, int *error) {
     const long n = blk * 4 * Rpad;
     const long id = blockIdx.x * 256L + threadIdx.x;
+    // the MTTKRP kernel may start now: it waits for this grid only before it
+    // reads the packed tiles
+    ptx::griddep_launch();
     if (id == 0) *error = 0;
     if (id >= n) return;
     const long t = id / (4 * Rpad);
@@ -815,10 +819,10 @@ __global__ void __launch_bounds__(256) k_pack_b(KrFactors fold, long R, int Rpad
     } else {
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            long lin = 32 * t + 8 * kc + j;
+            uint32_t lin = (uint32_t)(32 * t + 8 * kc + j);  // < frows < 2^31 (the plan's bound)
             float p = 1.f;
             for (int f = 0; f < fold.n; f++) {
-                const long d = fold.rows[f], qd = lin / d;
+                const uint32_t d = (uint32_t)fold.rows[f], qd = lin / d;
                 p *= (r < R) ? __ldg(fold.U[f] + (lin - qd * d) + (long)r * d) : 0.f;
                 lin = qd;
             }
@@ -899,6 +903,7 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
             long ks = (a.kind == 0) ? 0 : st_beg / a.psteps;
             long kp = (a.kind == 0) ? st_beg : st_beg % a.psteps;
             long pos = st_beg % a.blk;  // stage position in its block = B tile
+            bool packed = false;        // the pack kernel's tiles are visible
             for (long i = 0; i < nst && !*abort; i++) {
                 if (xr.use > 0 && !ptx::mbar_wait(&sm.empty_x[xr.slot], xr.prev_parity(), abort)) break;
                 uint8_t *dst = xring + (size_t)xr.slot * X_STAGE_BYTES;
@@ -908,6 +913,10 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
                 issued_x = i + 1;
                 // the slot's B tile is free once the MMA of stage i - nb is done
                 if (br.use > 0 && !ptx::mbar_wait(&sm.empty_a[br.slot], br.prev_parity(), abort)) break;
+                if (!packed) {
+                    ptx::griddep_wait();
+                    packed = true;
+                }
                 ptx::mbar_arrive_expect_tx(&sm.full_a[br.slot], bstage);
                 ptx::bulk_load(bring + (size_t)br.slot * bstage, a.pb + (size_t)pos * bstage, bstage,
                                &sm.full_a[br.slot]);
@@ -1104,13 +1113,45 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
             for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.full_a[i % nb], par, 100000u); it++) {
             }
         }
+        ptx::griddep_wait();  // after the pack kernel's clearing of the flag
         atomicExch(a.error, 1);
     }
     ptx::tc_fence_before();
     __syncthreads();
     ptx::tc_fence_after();
     if (warp == 0) ptx::tmem_dealloc(tbase, a.tmem_cols);
+    // the split reduce may launch once every CTA got here (it waits for the
+    // whole grid before reading the partials)
+    ptx::griddep_launch();
 }
+
+// The same sum with one warp per output (lane l takes z = l, l + 32, ...,
+// then a fixed shuffle tree), for outputs too few to fill the GPU with the
+// 8-lane layout below (96 x 32 outputs at 96^4 rank 32: 96 CTAs of 37
+// sequential loads each).
+__global__ void __launch_bounds__(256) k_sum_tc_partials_w(const float *__restrict__ part, int splits, long Q,
+                                                           long R, long Rp, const int *__restrict__ error,
+                                                           float *__restrict__ out) {
+    ptx::griddep_wait();  // the MTTKRP grid's partials
+    const int lane = threadIdx.x & 31;
+    const long e = blockIdx.x * 8L + (threadIdx.x >> 5);  // q * Rp + r
+    const long n = Q * Rp;
+    if (e >= n) return;  // warp-uniform
+    double sum = 0.0;
+#pragma unroll 4
+    for (int z = lane; z < splits; z += 32) sum += (double)__ldcs(part + (long)z * n + e);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) {
+        const long q = e / Rp, r = e - q * Rp;
+        if (*error) sum = __longlong_as_double(0x7ff8000000000000LL);
+        if (r < R) out[q + Q * r] = (float)sum;
+    }
+}
+
+// Launches the split reduce in the layout that fills the GPU.
+void sum_tc_partials(const float *part, int splits, long Q, long R, long Rp, const int *error, float *out,
+                     cudaStream_t s);
 
 // out[q + Q r] = sum_z part[z][q][r] in FP64, fixed order.  A CTA owns 32
 // consecutive (q, r) slots of the padded partial rows (coalesced reads), each
@@ -1120,6 +1161,7 @@ __global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict
                                                          long R, long Rp, const int *__restrict__ error,
                                                          float *__restrict__ out) {
     __shared__ double red[8][32];
+    ptx::griddep_wait();  // the MTTKRP grid's partials
     const int o = threadIdx.x & 31, zl = threadIdx.x >> 5;
     const long e = blockIdx.x * 32L + o;  // q * Rp + r
     const long n = Q * Rp;
@@ -1138,6 +1180,36 @@ __global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict
         // output becomes NaN so the failure cannot pass for a result
         if (*error) t = __longlong_as_double(0x7ff8000000000000LL);
         if (r < R) out[q + Q * r] = (float)t;
+    }
+}
+
+// A launch configuration with programmatic stream serialization (the
+// kernel may start while the previous one on the stream finishes).
+struct PdlLaunch {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg;
+    PdlLaunch(unsigned grid, unsigned block, size_t smem, cudaStream_t s) {
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg = cudaLaunchConfig_t{};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+};
+
+void sum_tc_partials(const float *part, int splits, long Q, long R, long Rp, const int *error, float *out,
+                     cudaStream_t s) {
+    const long n = Q * Rp;
+    if ((n + 31) / 32 < 2L * kNumSMs && splits > 32) {
+        PdlLaunch l((unsigned)((n + 7) / 8), 256, 0, s);
+        cudaLaunchKernelEx(&l.cfg, k_sum_tc_partials_w, part, splits, Q, R, Rp, error, out);
+    } else {
+        PdlLaunch l((unsigned)((n + 31) / 32), 256, 0, s);
+        cudaLaunchKernelEx(&l.cfg, k_sum_tc_partials, part, splits, Q, R, Rp, error, out);
     }
 }
 
@@ -1304,7 +1376,8 @@ int launch_pb(const CUtensorMap &tmap, const TcArgs &a, size_t smem, unsigned gr
         CUD_CHECK(cudaFuncSetAttribute(k_mttkrp_pb<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
         attr[dev].store(true, std::memory_order_release);
     }
-    k_mttkrp_pb<MINB><<<grid, PB_THREADS, smem, s>>>(tmap, a);
+    PdlLaunch l(grid, PB_THREADS, smem, s);  // overlaps the B pack (see griddep_wait)
+    CUD_CHECK(cudaLaunchKernelEx(&l.cfg, k_mttkrp_pb<MINB>, tmap, a));
     CUD_CHECK_LAUNCH("mttkrp_pb");
     return CUD_OK;
 }
@@ -1422,10 +1495,11 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
         a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;
         const unsigned grid = (unsigned)(p.qtiles * p.splits);
         const size_t smem = pb_smem_bytes((int)p.Rpad, p.nb);
+        const int pk = prof_begin(s);
         int st = (p.ctas_per_sm == 2) ? launch_pb<2>(tmap, a, smem, grid, s) : launch_pb<1>(tmap, a, smem, grid, s);
+        prof_end(pk, s);
         if (st) return st;
-        k_sum_tc_partials<<<(unsigned)((p.Q * a.Rp + 31) / 32), 256, 0, s>>>(a.part, (int)p.splits, p.Q, R,
-                                                                             a.Rp, a.error, out);
+        sum_tc_partials(a.part, (int)p.splits, p.Q, R, a.Rp, a.error, out, s);
         CUD_CHECK_LAUNCH("mttkrp_tc reduce");
         return CUD_OK;
     }
@@ -1435,6 +1509,7 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     unsigned grid = (unsigned)(p.qtiles * p.splits);
     const size_t smem = tc_smem_bytes((int)p.Rpad, p.fast, p.nx, p.nb);
     int st;
+    const int pk = prof_begin(s);
     if (p.ctas_per_sm == 2) {
         if (kipt_need <= 2 && cipt_need <= 0) st = launch_tc<2, 0, 2>(tmap, umap, a, smem, grid, s);
         else if (kipt_need <= 2 && cipt_need <= 1) st = launch_tc<2, 1, 2>(tmap, umap, a, smem, grid, s);
@@ -1444,9 +1519,9 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
         if (kipt_need <= 4 && cipt_need <= 3) st = launch_tc<4, 3, 1>(tmap, umap, a, smem, grid, s);
         else return CUD_ERR_UNSUPPORTED;  // Rpad <= 128 needs at most 4 / 3
     }
+    prof_end(pk, s);
     if (st) return st;
-    k_sum_tc_partials<<<(unsigned)((p.Q * a.Rp + 31) / 32), 256, 0, s>>>(a.part, (int)p.splits, p.Q, R, a.Rp,
-                                                                         a.error, out);
+    sum_tc_partials(a.part, (int)p.splits, p.Q, R, a.Rp, a.error, out, s);
     CUD_CHECK_LAUNCH("mttkrp_tc reduce");
     return CUD_OK;
 }

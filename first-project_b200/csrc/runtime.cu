@@ -76,7 +76,63 @@ double *pinned_scalars() {
     return p;
 }
 
+// Kernel timing for measurement (off unless cud_prof_enable turned it on):
+// the MTTKRP entry points bracket their main kernel with a pair of CUDA
+// events recorded on the call's stream (not while the stream is being
+// captured into a graph).  Up to kProfPairs pairs are kept until read.
+constexpr int kProfPairs = 256;
+static std::mutex g_prof_mu;
+static bool g_prof_on = false;
+static int g_prof_n = 0;
+static cudaEvent_t g_prof_ev[2 * kProfPairs];
+static bool g_prof_made = false;
+
+int prof_begin(cudaStream_t s) {
+    if (!g_prof_on) return -1;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return -1;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!g_prof_made || g_prof_n >= kProfPairs) return -1;
+    const int k = g_prof_n++;
+    if (cudaEventRecord(g_prof_ev[2 * k], s) != cudaSuccess) return -1;
+    return k;
+}
+
+void prof_end(int k, cudaStream_t s) {
+    if (k >= 0) cudaEventRecord(g_prof_ev[2 * k + 1], s);
+}
+
 }  // namespace cud
+
+extern "C" int cud_prof_enable(int on) {
+    using namespace cud;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (on && !g_prof_made) {
+        for (int i = 0; i < 2 * kProfPairs; i++)
+            if (cudaEventCreate(&g_prof_ev[i]) != cudaSuccess) return set_status(CUD_ERR_CUDA);
+        g_prof_made = true;
+    }
+    g_prof_on = on != 0;
+    g_prof_n = 0;
+    return set_status(CUD_OK);
+}
+
+extern "C" int cud_prof_kernel_times(float *ms, int max_n, int *count) {
+    using namespace cud;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    int n = 0;
+    for (int k = 0; k < g_prof_n; k++) {
+        if (cudaEventSynchronize(g_prof_ev[2 * k + 1]) != cudaSuccess) return set_status(CUD_ERR_CUDA);
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, g_prof_ev[2 * k], g_prof_ev[2 * k + 1]) != cudaSuccess)
+            return set_status(CUD_ERR_CUDA);
+        if (ms && n < max_n) ms[n] = t;
+        n++;
+    }
+    g_prof_n = 0;
+    if (count) *count = n;
+    return set_status(CUD_OK);
+}
 
 extern "C" int cud_get_last_error(void) { return cud::t_last_status; }
 

@@ -282,5 +282,14 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                  : "memory");
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic
+// stream serialization may start before the previous kernel on its stream
+// has finished; griddep_wait blocks the calling thread until that kernel
+// has completed and its memory operations are visible (a no-op when the
+// launch did not use the attribute), and griddep_launch lets the next such
+// kernel start once every CTA of this one has called it or exited.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 }  // namespace ptx
 }  // namespace cud

@@ -430,6 +430,10 @@ __global__ void __launch_bounds__(256) k_ws_jacobi_top(const float *G, float *F,
     __syncthreads();
     float norm = 0.f;
     for (int e = 0; e < n; e++) norm = fmaxf(norm, fabsf(A[e][e]));
+    // the cyclic sweeps converge quadratically down to FP32's rounding floor
+    // and then stall: stop at the tolerance, or once a sweep no longer
+    // halves the off-diagonal mass
+    float prev_off = 3.4e38f;
     for (int sweep = 0; sweep < max_sweeps; sweep++) {
         // off-diagonal mass
         float s = 0.f;
@@ -446,6 +450,8 @@ __global__ void __launch_bounds__(256) k_ws_jacobi_top(const float *G, float *F,
         const float off = off_red[0];
         __syncthreads();
         if (!(off > 1e-12f * norm * norm)) break;
+        if (sweep >= 2 && off > 0.5f * prev_off) break;
+        prev_off = off;
         for (int round = 0; round < n - 1; round++) {
             if (threadIdx.x < n / 2) {
                 // round-robin: index n-1 fixed, the others rotate

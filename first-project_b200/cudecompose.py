@@ -105,6 +105,8 @@ _sig("cud_mttkrp_legacy", [_vp, _vp, _vp, _vp, _l, _l, _l, _l, _l, _i, _vp])
 _sig("cud_mttkrp", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _vp, _i, _vp])
 _sig("cud_unfold_gram", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _i, _vp])
 _sig("cud_mttkrp_path", [_i, ctypes.POINTER(_l), _i, _l, _i])
+_sig("cud_prof_enable", [_i])
+_sig("cud_prof_kernel_times", [ctypes.POINTER(ctypes.c_float), _i, ctypes.POINTER(_i)])
 _sig("cud_syev_jacobi", [_vp, _l, _vp, _vp, _i, _vp])
 _sig("cud_cross_gram", [_vp, _vp, _l, _l, _l, _vp, _l, _vp])
 _sig("cud_syev_top", [_vp, _l, _l, _vp, _vp, _i, _vp])
@@ -309,6 +311,19 @@ def mttkrp(X, dims, factors, mode, R, out, precision=PREC_DEFAULT, stream=None):
 def mttkrp_path(dims, mode, R, precision=PREC_DEFAULT) -> str:
     """'tensor-core' or 'cuda-core': the kernel mttkrp() runs for this shape."""
     return "tensor-core" if _lib.cud_mttkrp_path(len(dims), _longs(dims), mode, R, precision) else "cuda-core"
+
+
+def prof_enable(on=True):
+    """Turns the MTTKRP entry points' kernel timing on or off (measurement)."""
+    _check(_lib.cud_prof_enable(1 if on else 0), "prof_enable")
+
+
+def prof_kernel_times(max_n=256):
+    """Durations (ms) of the MTTKRP main kernels recorded since the last read."""
+    buf = (ctypes.c_float * max_n)()
+    n = _i(0)
+    _check(_lib.cud_prof_kernel_times(buf, max_n, ctypes.byref(n)), "prof_kernel_times")
+    return [buf[i] for i in range(min(n.value, max_n))]
 
 
 def unfold_gram(X, dims, mode, G, stream=None):

@@ -151,6 +151,17 @@ int cud_mttkrp(const float *X, int order, const long *dims, const float *const *
 int cud_mttkrp_noalloc(const float *X, int order, const long *dims, const float *const *U,
                        int mode, long R, float *out, int precision, void *stream);
 
+/* Extension (measurement; no counterpart in the reference): kernel timing
+ * of the MTTKRP entry points.  With cud_prof_enable(1), every cud_mttkrp /
+ * cud_mttkrp_legacy call records a pair of CUDA events on its stream around
+ * its main kernel (the MTTKRP itself, not the B pack or the split reduce),
+ * except while the stream is being captured into a graph; up to 256 pairs
+ * are kept.  cud_prof_kernel_times synchronises on them, writes up to max_n
+ * durations (ms) into ms, the number recorded into count, and clears them.
+ * cud_prof_enable(0) turns it off. */
+int cud_prof_enable(int on);
+int cud_prof_kernel_times(float *ms, int max_n, int *count);
+
 /* Extension: the kernel cud_mttkrp runs for these arguments (given a
  * 16-byte-aligned X): 1 = tcgen05 tensor cores, 0 = CUDA cores. */
 int cud_mttkrp_path(int order, const long *dims, int mode, long R, int precision);
