@@ -67,12 +67,14 @@ struct BatchArgs {
 
 // Shared memory of a CTA of NW warps: the factors and the MTTKRP result
 // row-major (rank contiguous, ranks padded to RS with zeros), and the
-// per-warp partial results.
+// partial results of the (at most three) 32-row chunks of modes 2 and 3.
+constexpr int MAXCHUNK = (BMAXD + 31) / 32;
+
 template <int NW>
 struct BatchSmem {
     float F[3][BMAXD * RS];
     float M[BMAXD * RS];
-    float Mp[NW][BMAXD * RS];
+    float Mp[MAXCHUNK][BMAXD * RS];
     double V[BMAXR * BMAXR];         // normal matrix / its inverse
     double rowk[BMAXR], colk[BMAXR];
     double red[32];
@@ -129,7 +131,12 @@ __device__ __forceinline__ float lane_sum(float (&v)[RP], int lane) {
 //           (outer j or k; the lanes' terms summed by lane_sum)
 // Two outer indices at a time, four inner ones unrolled: eight loads in
 // flight per lane, and each broadcast factor row (RP/4 16-byte shared
-// loads) feeds 2 RP FMAs.  Partials of the warps (mode 0: per outer range;
+// loads) feeds 2 RP FMAs.  (Issuing the next group's loads ahead of the
+// current group's FMAs raised the registers to 166 and measured slower:
+// 0.314 s against 0.255 s for the bench batch; L2 prefetches of the
+// outer pair after next -- bulk for the contiguous slices of modes 1 and 3,
+// per line for mode 2 -- cut the long-scoreboard stalls but measured slower
+// too: 1.58 against 1.38 ms for one sweep of 512 tensors.)  Partials of the warps (mode 0: per outer range;
 // modes 1, 2: per row chunk) are combined in a fixed order.  RP = the rank
 // rounded up to 4, 8 or 16; the padding ranks are zero.
 template <int NW, int RP>
@@ -227,17 +234,27 @@ __device__ void mttkrp_lanes(BatchSmem<NW> &sm, const BatchArgs &a, const Tensor
             }
         }
     }
-    if (mode == 0 && g < NG && valid) {
+    if (mode == 0) {
+        // the groups' rows added into M in group order, one group per
+        // barrier (deterministic, one buffer)
+        for (int gg = 0; gg < NG; gg++) {
+            if (g == gg && valid) {
 #pragma unroll
-        for (int r = 0; r < RP; r++) sm.Mp[g][i * RS + r] = acc[r];
+                for (int r = 0; r < RP; r++) {
+                    float *m = &sm.M[i * RS + r];
+                    *m = (gg == 0) ? acc[r] : *m + acc[r];
+                }
+            }
+            __syncthreads();
+        }
+        return;
     }
     __syncthreads();
     const int Q = t.dims[mode];
-    const int nparts = (mode == 0) ? NG : LI;
     for (int e = threadIdx.x; e < Q * RS; e += NW * 32) {
         if ((e & (RS - 1)) >= RP) continue;  // padding ranks: never read
         float v = 0.f;
-        for (int p = 0; p < nparts; p++) v += sm.Mp[p][e];
+        for (int p = 0; p < LI; p++) v += sm.Mp[p][e];
         sm.M[e] = v;
     }
     __syncthreads();
@@ -293,8 +310,13 @@ __device__ void normal_inverse_small(Smem &sm, const BatchArgs &a, const TensorM
 
 // One ALS sweep of every tensor not yet converged: CTAs of NW warps pull
 // tensors from the queue.
+// Resident CTAs per SM the launch bounds ask for, per CTA width: 20, 18, 16
+// and 24 warps per SM (shared memory, ~45 KB a CTA, allows each); the
+// autotuner picks among the widths.
+constexpr int min_ctas(int nw) { return nw == 4 ? 5 : nw == 6 ? 3 : nw == 8 ? 2 : 2; }
+
 template <int NW>
-__global__ void __launch_bounds__(NW * 32) k_batch_sweep(BatchArgs a) {
+__global__ void __launch_bounds__(NW * 32, min_ctas(NW)) k_batch_sweep(BatchArgs a) {
     constexpr int NT = NW * 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BatchSmem<NW> &sm = *reinterpret_cast<BatchSmem<NW> *>(smem_raw);
@@ -426,6 +448,10 @@ int launch_sweep(const BatchArgs &a, int ctas_per_sm, cudaStream_t s) {
     if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
         CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(BatchSmem<NW>)));
+        // the whole unified L1 as shared memory: the CTAs per SM the tuner
+        // asks for are then limited by shared memory, not by the carveout
+        CUD_CHECK(cudaFuncSetAttribute(k_batch_sweep<NW>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
         attr[dev].store(true, std::memory_order_release);
     }
     CUD_CHECK(cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s));
@@ -625,9 +651,9 @@ extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *r
         hr[t] = (int)ranks[t];
     }
     long key = shape_class(ntensors, hd.data(), hr.data());
-    // (threads, CTAs per SM) that fit in shared memory: BatchSmem<NW> is
-    // ~52 KB at 4 warps, ~64 KB at 6, ~77 KB at 8, ~101 KB at 12
-    const std::vector<BatchCfg> cand = {{128, 3}, {128, 4}, {192, 2}, {192, 3}, {256, 2}, {384, 2}};
+    // (threads, CTAs per SM) within the launch bounds' register budgets and
+    // shared memory (~45 KB a CTA)
+    const std::vector<BatchCfg> cand = {{128, 4}, {128, 5}, {192, 3}, {256, 2}, {384, 2}};
     float best = 1e30f;
     BatchCfg bestc{192, 3};
     cudaStream_t s = as_stream(stream);

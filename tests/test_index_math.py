@@ -182,13 +182,19 @@ def test_batched_mttkrp_lanes_restated_matches_oracle(dims, R, NW):
 
 
 def test_batched_shared_memory_fits():
-    # BatchSmem<NW>: F[3], M, Mp[NW] (floats, BMAXD x RS each), V and the
-    # pivot rows (doubles); the CTAs per SM of every tuning candidate fit
-    # in 228 KB (1 KB reserved per CTA)
-    for NW, ctas in ((4, 3), (4, 4), (6, 2), (6, 3), (8, 2), (12, 2)):
-        smem = 4 * BMAXD * RS * (4 + NW) + 8 * (BMAXR * BMAXR + 2 * BMAXR + 32) + 16
+    # BatchSmem: F[3], M, Mp[3] (floats, BMAXD x RS each; Mp holds the row
+    # chunks' partials of modes 2 and 3, mode 1 adds its groups into M in
+    # turn), V and the pivot rows (doubles); the CTAs per SM of every tuning
+    # candidate fit in 228 KB (1 KB reserved per CTA), and their warps
+    # within the launch bounds' budgets
+    min_ctas = {4: 5, 6: 3, 8: 2, 12: 2}
+    for threads, ctas in ((128, 4), (128, 5), (192, 3), (256, 2), (384, 2)):
+        NW = threads // 32
+        smem = 4 * BMAXD * RS * (4 + 3) + 8 * (BMAXR * BMAXR + 2 * BMAXR + 32) + 16
         assert ctas * (smem + 1024) <= 228 * 1024, (NW, ctas, smem)
-        assert smem <= 232448
+        assert ctas <= min_ctas[NW] or NW * ctas <= 24
+        # partial buffers: at most ceil(96 / 32) = 3 row chunks
+        assert -(-BMAXD // 32) == 3
 
 
 # ---- gemm_tc.cu skinny GEMM: B resident for K <= 1024 plus an 8-deep A ring
