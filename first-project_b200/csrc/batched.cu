@@ -35,6 +35,13 @@ namespace cud {
 
 namespace {
 
+// Inner indices whose X loads are issued together (x2 outer indices): 8
+// took the 4096-tensor batch from 0.241 s to 0.217 s against 4; 16 spilled
+// and was slower.
+#ifndef CUD_BATCH_UNROLL
+#define CUD_BATCH_UNROLL 8
+#endif
+
 constexpr int BMAXD = 96;    // largest mode size handled (smem sizing)
 constexpr int BMAXR = 16;    // largest rank handled
 constexpr int RS = BMAXR;    // row stride of factors and results in shared memory (ranks padded)
@@ -170,15 +177,15 @@ __device__ void mttkrp_lanes(BatchSmem<NW> &sm, const BatchArgs &a, const Tensor
         const float *x1 = xi + so * (two ? o + 1 : o);
         const bool l0 = valid, l1 = valid && two;
         int n = 0;
-        for (; n + 4 <= Nn; n += 4) {
-            float xa[4], xb[4];
+        for (; n + CUD_BATCH_UNROLL <= Nn; n += CUD_BATCH_UNROLL) {
+            float xa[CUD_BATCH_UNROLL], xb[CUD_BATCH_UNROLL];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < CUD_BATCH_UNROLL; u++) {
                 xa[u] = l0 ? __ldg(x0 + sn * (n + u)) : 0.f;
                 xb[u] = l1 ? __ldg(x1 + sn * (n + u)) : 0.f;
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < CUD_BATCH_UNROLL; u++) {
                 const float *vr = Vf + (n + u) * RS;
 #pragma unroll
                 for (int r4 = 0; r4 < RP; r4 += 4) {
@@ -315,6 +322,8 @@ __device__ void normal_inverse_small(Smem &sm, const BatchArgs &a, const TensorM
 // autotuner picks among the widths.
 constexpr int min_ctas(int nw) { return nw == 4 ? 5 : nw == 6 ? 3 : nw == 8 ? 2 : 2; }
 
+// (A register cap per width through __maxnreg__, 112 for six warps, cut
+// the spills but measured 2-7 % slower on the 4096-tensor batch.)
 template <int NW>
 __global__ void __launch_bounds__(NW * 32, min_ctas(NW)) k_batch_sweep(BatchArgs a) {
     constexpr int NT = NW * 32;

@@ -9,6 +9,7 @@
 // the graph touches.  Mirrors the update order and equations of
 // src/cp_als.cu:44-119 and src/cp4_als.cu:64-164, without their per-sweep
 // allocations and device synchronisations.
+#include <mutex>
 #include <vector>
 #include <curand.h>
 
@@ -42,6 +43,7 @@ struct cud_cp_plan_s {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int kernels_per_sweep = -1;
+    size_t reset_bytes = 0;  // fit scalars, fallback count and update ticket (zeroed by a refresh)
 };
 
 namespace {
@@ -248,6 +250,22 @@ extern "C" int cud_cp_plan_destroy(cud_cp_plan p) {
     return set_status(CUD_OK);
 }
 
+// The data-dependent state of a plan, from X and the current factors:
+// ||X||^2, the factor Grams, and zeroed fit scalars, fallback count and
+// update ticket.  Synchronises the stream (the norm is read on the host).
+static int plan_refresh(cud_cp_plan_s *p, cudaStream_t s) {
+    long total = 1;
+    for (int m = 0; m < p->order; m++) total *= p->dims[m];
+    double o[2];
+    int st = residual_norms(p->X, nullptr, total, 0, o, s);
+    if (st) return st;
+    p->normx2 = o[1];
+    if (cudaMemsetAsync(p->fit, 0, p->reset_bytes, s) != cudaSuccess) return CUD_ERR_CUDA;
+    for (int m = 0; m < p->order && st == CUD_OK; m++)
+        st = factor_gram(p->U[m], p->dims[m], p->R, p->G + (size_t)m * p->R * p->R, s);
+    return st;
+}
+
 extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, long R,
                                   float *const *U, const cud_cp_options *opt_in, void *stream,
                                   cud_cp_plan *out) {
@@ -319,16 +337,8 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
 
     SideStream ss;
     int st = ss.open(as_stream(stream));
-    if (st == CUD_OK) {
-        double o[2];
-        st = residual_norms(X, nullptr, total, 0, o, ss.s);
-        p->normx2 = o[1];
-    }
-    // fit scalars, fallback count and the update ticket start at zero
-    if (st == CUD_OK && cudaMemsetAsync(p->fit, 0, off_P - off_F, ss.s) != cudaSuccess)
-        st = CUD_ERR_CUDA;
-    for (int m = 0; m < order && st == CUD_OK; m++)
-        st = factor_gram(U[m], dims[m], R, p->G + (size_t)m * R * R, ss.s);
+    p->reset_bytes = off_P - off_F;
+    if (st == CUD_OK) st = plan_refresh(p, ss.s);
     if (st == CUD_OK) st = normal_inverse_prepare();
     if (st == CUD_OK && opt.use_graph) {
         if (cudaStreamBeginCapture(ss.s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
@@ -401,14 +411,68 @@ extern "C" int cud_cp_plan_info(cud_cp_plan p, int *kernels_per_sweep, int *fall
     return set_status(CUD_OK);
 }
 
+// The one-shot cud_cp_als keeps its last plan for the next call with the
+// same device, tensor and factor pointers, shape, rank, precision and graph
+// setting: the buffers and the captured sweep graph carry over (the graph
+// holds pointers, not data), and plan_refresh recomputes ||X||^2 and the
+// Grams from the data.  One plan is kept (its memory stays allocated until
+// a call with other arguments replaces it, or cud_cp_als_release frees it);
+// concurrent calls each take or build their own.
+namespace {
+std::mutex g_cache_mu;
+cud_cp_plan g_cache = nullptr;
+
+bool plan_matches(const cud_cp_plan_s *p, const float *X, int order, const long *dims, long R, float *const *U,
+                  const cud_cp_options &opt) {
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (!p || p->device != dev || p->X != X || p->order != order || p->R != R ||
+        p->opt.precision != opt.precision || (p->opt.use_graph != 0) != (opt.use_graph != 0))
+        return false;
+    for (int m = 0; m < order; m++)
+        if (p->dims[m] != dims[m] || p->U[m] != U[m]) return false;
+    return true;
+}
+}  // namespace
+
+extern "C" int cud_cp_als_release(void) {
+    cud_cp_plan old = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        old = g_cache;
+        g_cache = nullptr;
+    }
+    return cud_cp_plan_destroy(old);
+}
+
 extern "C" int cud_cp_als(const float *X, int order, const long *dims, long R, float *const *U,
                           const cud_cp_options *opt_in, cud_cp_result *res, void *stream) {
     cud_cp_options opt;
     cud_cp_default_options(&opt);
     if (opt_in) opt = *opt_in;
     cud_cp_plan p = nullptr;
-    int st = cud_cp_plan_create(X, order, dims, R, U, &opt, stream, &p);
-    if (st) return set_status(st);
+    int st = CUD_OK;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        if (plan_matches(g_cache, X, order, dims, R, U, opt)) {
+            p = g_cache;
+            g_cache = nullptr;
+        }
+    }
+    if (p) {
+        p->opt = opt;
+        SideStream rs;
+        st = rs.open(as_stream(stream));
+        if (st == CUD_OK) st = plan_refresh(p, rs.s);
+        rs.close();
+        if (st) {
+            cud_cp_plan_destroy(p);
+            return set_status(st);
+        }
+    } else {
+        st = cud_cp_plan_create(X, order, dims, R, U, &opt, stream, &p);
+        if (st) return set_status(st);
+    }
     SideStream ss;
     st = ss.open(as_stream(stream));
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -452,7 +516,18 @@ extern "C" int cud_cp_als(const float *X, int order, const long *dims, long R, f
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
     ss.close();
-    cud_cp_plan_destroy(p);
+    if (st == CUD_OK) {
+        // keep this plan for the next call; release the one it replaces
+        cud_cp_plan old = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(g_cache_mu);
+            old = g_cache;
+            g_cache = p;
+        }
+        cud_cp_plan_destroy(old);
+    } else {
+        cud_cp_plan_destroy(p);
+    }
     if (st == CUD_OK) {
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = cuda_status(e, "cud_cp_als");

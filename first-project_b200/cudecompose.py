@@ -106,6 +106,7 @@ _sig("cud_mttkrp", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_vp), _i, _l, _v
 _sig("cud_unfold_gram", [_vp, _i, ctypes.POINTER(_l), _i, _vp, _i, _vp])
 _sig("cud_mttkrp_path", [_i, ctypes.POINTER(_l), _i, _l, _i])
 _sig("cud_prof_enable", [_i])
+_sig("cud_cp_als_release", [])
 _sig("cud_prof_kernel_times", [ctypes.POINTER(ctypes.c_float), _i, ctypes.POINTER(_i)])
 _sig("cud_syev_jacobi", [_vp, _l, _vp, _vp, _i, _vp])
 _sig("cud_cross_gram", [_vp, _vp, _l, _l, _l, _vp, _l, _vp])
@@ -367,6 +368,11 @@ def cp_als(X, dims, R, factors, max_sweeps=500, tol=0.0, precision=PREC_DEFAULT,
     _check(_lib.cud_cp_als(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
                            ctypes.byref(opt), ctypes.byref(res), _stream(stream)), "cp_als")
     return res
+
+
+def cp_als_release():
+    """Frees the plan cud_cp_als keeps for its next call with the same arguments."""
+    _check(_lib.cud_cp_als_release(), "cp_als_release")
 
 
 def cp_als_f64(X, dims, R, factors, max_sweeps=500, tol=0.0, target_fit=0.0, stream=None) -> CpResult:

@@ -12,7 +12,9 @@
  * Differences from the reference, by design: cp_tensorcore does not free the
  * caller's buffers (src/tensorcore_cp.cu:136-139), cp_als4 does not reset
  * the device (src/cp4_als.cu:184), tucker_tensorcore writes U1..U3
- * (src/tucker_tensorcore.cu:84-108 leaves them unwritten), and the
+ * (src/tucker_tensorcore.cu:84-108 leaves them unwritten) and computes in
+ * three-term BF16 on the tensor cores where the reference rounds to FP16
+ * (closer to the exact result), and the
  * normal-equation solve is an FP64 Gauss-Jordan inverse with SPD pivots (a
  * Jacobi pseudo-inverse when a pivot is not positive) rather than FP32 LU.
  */

@@ -233,6 +233,12 @@ void cud_cp_default_options(cud_cp_options *opt);
  * fallback.  res may be NULL. */
 int cud_cp_als(const float *X, int order, const long *dims, long R, float *const *U,
                const cud_cp_options *opt, cud_cp_result *res, void *stream);
+/* Extension: cud_cp_als keeps its last plan (workspace and captured sweep
+ * graph) for the next call on the same device with the same X and factor
+ * pointers, dims, rank, precision and graph setting -- the data-dependent
+ * state (||X||^2, the Grams, the fit history) is recomputed each call.  One
+ * plan is kept; cud_cp_als_release frees it. */
+int cud_cp_als_release(void);
 
 /* The reference's FP64 variants decomposition/GPU/normal/dprice/cp_als.cu:3-212
  * (order 3) and dprice/4_cp_als.cu:3-229 (order 4), as one general-order

@@ -137,3 +137,63 @@ def test_plan_true_fit_matches_direct(cd):
     direct = 1.0 - torch.linalg.norm((Xd - rec).double()) / torch.linalg.norm(Xd.double())
     assert abs(tf - float(direct)) <= 1e-6
     plan.close()
+
+
+def test_repeated_call_reuses_plan_and_matches_a_fresh_one(cd):
+    """cud_cp_als keeps its plan for a call with the same buffers: after the
+    tensor's and the factors' contents change, the cached plan must give
+    exactly what a freshly built plan gives (||X||^2 and the Grams come from
+    the data on every call)."""
+    rng = np.random.default_rng(21)
+    dims, R = (64, 48, 40), 8
+    n = int(np.prod(dims))
+    X = torch.from_numpy(rng.random(n).astype(np.float32)).cuda()
+    U = [torch.from_numpy(rng.random(d * R).astype(np.float32)).cuda() for d in dims]
+    cd.cp_als(X, dims, R, U, max_sweeps=6)          # builds and keeps the plan
+    X2 = rng.random(n).astype(np.float32)
+    init2 = [rng.random(d * R).astype(np.float32) for d in dims]
+    X.copy_(torch.from_numpy(X2))
+    for u, i in zip(U, init2):
+        u.copy_(torch.from_numpy(i))
+    a = cd.cp_als(X, dims, R, U, max_sweeps=6)      # the kept plan
+    got = [u.cpu().numpy().copy() for u in U]
+    cd.cp_als_release()
+    for u, i in zip(U, init2):
+        u.copy_(torch.from_numpy(i))
+    b = cd.cp_als(X, dims, R, U, max_sweeps=6)      # a fresh plan
+    for g, u in zip(got, U):
+        np.testing.assert_array_equal(g, u.cpu().numpy())
+    assert a.fit == b.fit and a.sweeps == b.sweeps
+
+
+def test_cp_tensorcore_drop_in_fp16(cd, capfd):
+    """cp_tensorcore (src/tensorcore_cp.cu:3-150): cuRAND's default generator
+    seeded 1234 for B then C, 500 ALS sweeps with FP16 MTTKRP operands, the
+    relative error printed.  Our drop-in (C++ symbol, through the library)
+    against the FP64 oracle's ALS from the same start: the FP16 operand
+    rounding (11-bit mantissas) moves the fit by at most 2e-3."""
+    import ctypes
+    rng = np.random.default_rng(22)
+    dims, R = (40, 32, 24), 4
+    true = [rng.random(d * R) for d in dims]
+    X = oracle.gencp(dims, true, R)
+    X = (X + 1e-3 * np.linalg.norm(X) / np.sqrt(X.size) * rng.standard_normal(X.size)).astype(np.float32)
+    dX = torch.from_numpy(X).cuda()
+    U = [torch.zeros(d * R, device="cuda") for d in dims]
+    # the start the drop-in draws (A is not drawn: the first update overwrites it)
+    ref_init = [torch.zeros(d * R, device="cuda") for d in dims]
+    cd.cp_init_curand(dims, R, ref_init, seed=1234)
+    init = [u.cpu().numpy() for u in ref_init]
+    lib = cd.library()
+    f = getattr(lib, "_Z13cp_tensorcorePfS_S_S_llll")
+    f.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_long] * 4
+    f.restype = None
+    capfd.readouterr()
+    f(dX.data_ptr(), *[u.data_ptr() for u in U], *dims, R)
+    torch.cuda.synchronize()
+    printed = float(capfd.readouterr().out.strip().splitlines()[-1])
+    got = [u.cpu().numpy() for u in U]
+    fit_ours = oracle.cp_fit(X, dims, got, R)
+    _, fits, _ = oracle.cp_als(X, dims, R, init, 500)
+    assert abs(fit_ours - fits[-1]) <= 2e-3, (fit_ours, fits[-1])
+    assert abs((1.0 - printed) - fit_ours) <= 1e-5, (printed, fit_ours)

@@ -238,3 +238,88 @@ def test_print_tensor_same_text_as_reference(tmp_path):
     assert a.returncode == 0 and b.returncode == 0, (a.stderr, b.stderr)
     assert a.stdout == b.stdout
     assert a.stdout.count("-----------------------------------") == 2
+
+
+def test_tucker_tensorcore_vs_reference_and_fp64(cd, capfd):
+    """tucker_tensorcore (src/tucker_tensorcore.cu:3-139) as a drop-in: the
+    reference rounds X, the factors and the TTM chain to FP16 and leaves
+    U1..U3 unwritten; ours runs three-term BF16 and writes them.  The core
+    (sign-invariant norm) of both against the FP64 HOSVD's: ours at the
+    FP32-level bar, the reference's at FP16's; our factors' subspaces against
+    FP64 eigh.  The printed errors of both are close."""
+    if not os.path.exists(oracle.REF_LIB_PATH):
+        pytest.skip("reference library not built (oracle/Makefile ref)")
+    rng = np.random.default_rng(31)
+    dims, ranks = (64, 48, 40), (6, 5, 4)
+    core0 = rng.standard_normal(int(np.prod(ranks)))
+    facs = [np.linalg.qr(rng.standard_normal((d, r)))[0].reshape(-1, order="F") for d, r in zip(dims, ranks)]
+    X = oracle.gentucker(core0, ranks, facs, dims)
+    X = (X + 1e-3 * np.linalg.norm(X) / np.sqrt(X.size) * rng.standard_normal(X.size)).astype(np.float32)
+    c64, f64 = oracle.tucker_hosvd(X, dims, ranks)
+    n64 = np.linalg.norm(c64)
+    vp, l = ctypes.c_void_p, ctypes.c_long
+    out = {}
+    for name, path in (("ours", cd.LIB_PATH), ("ref", oracle.REF_LIB_PATH)):
+        lib = ctypes.CDLL(path)
+        f = getattr(lib, "_Z17tucker_tensorcorePfS_S_S_S_llllll")
+        f.argtypes = [vp] * 5 + [l] * 6
+        f.restype = None
+        dX = dev_t(X)
+        core = torch.zeros(int(np.prod(ranks)), device="cuda")
+        U = [torch.zeros(d * r, device="cuda") for d, r in zip(dims, ranks)]
+        capfd.readouterr()
+        f(dX.data_ptr(), core.data_ptr(), *[u.data_ptr() for u in U], *dims, *ranks)
+        torch.cuda.synchronize()
+        printed = float(capfd.readouterr().out.strip().splitlines()[-1])
+        out[name] = (host(core).astype(np.float64), [host(u) for u in U], printed)
+    core_o, U_o, err_o = out["ours"]
+    core_r, _, err_r = out["ref"]
+    assert abs(np.linalg.norm(core_o) - n64) <= 1e-5 * n64
+    assert abs(np.linalg.norm(core_r) - n64) <= 2e-3 * n64
+    for u, w, d, r in zip(U_o, f64, dims, ranks):
+        a1 = u.reshape(d, r, order="F").astype(np.float64)
+        a2 = w.reshape(d, r, order="F")
+        assert np.linalg.norm(a1 @ a1.T - a2 @ a2.T) <= 1e-4
+    # the printed relative error ||X - Xhat|| / ||X||: ours is the FP64
+    # model's to 2 %; the reference's (FP16 core) is of the same magnitude
+    rec = oracle.gentucker(c64, ranks, f64, dims)
+    e64 = np.linalg.norm(X.astype(np.float64) - rec) / np.linalg.norm(X.astype(np.float64))
+    assert abs(err_o - e64) <= 0.02 * e64, (err_o, e64)
+    assert abs(err_o - err_r) <= 0.5 * max(err_o, err_r), (err_o, err_r)
+
+
+def test_tucker_hosvd4_printed_error_vs_reference_and_fp64(cd, capfd):
+    """tucker_hosvd4 (src/tucker4_hosvd.cu:3-141) prints the relative
+    reconstruction error of its model (:123-129, gentucker4 + rse).  Ours and
+    the reference's printed values against the FP64 HOSVD model's, and the
+    cores' norms against each other."""
+    if not os.path.exists(oracle.REF_LIB_PATH):
+        pytest.skip("reference library not built (oracle/Makefile ref)")
+    rng = np.random.default_rng(41)
+    dims, ranks = (24, 20, 18, 16), (4, 3, 3, 2)
+    core0 = rng.standard_normal(int(np.prod(ranks)))
+    facs = [np.linalg.qr(rng.standard_normal((d, r)))[0].reshape(-1, order="F") for d, r in zip(dims, ranks)]
+    X = oracle.gentucker(core0, ranks, facs, dims)
+    X = (X + 1e-2 * np.linalg.norm(X) / np.sqrt(X.size) * rng.standard_normal(X.size)).astype(np.float32)
+    c64, f64 = oracle.tucker_hosvd(X, dims, ranks)
+    rec = oracle.gentucker(c64, ranks, f64, dims)
+    e64 = np.linalg.norm(X.astype(np.float64) - rec) / np.linalg.norm(X.astype(np.float64))
+    vp, l = ctypes.c_void_p, ctypes.c_long
+    out = {}
+    for name, path in (("ours", cd.LIB_PATH), ("ref", oracle.REF_LIB_PATH)):
+        lib = ctypes.CDLL(path)
+        f = getattr(lib, "_Z13tucker_hosvd4PfS_S_S_S_S_llllllll")
+        f.argtypes = [vp] * 6 + [l] * 8
+        f.restype = None
+        dX = dev_t(X)
+        core = torch.zeros(int(np.prod(ranks)), device="cuda")
+        U = [torch.zeros(d * r, device="cuda") for d, r in zip(dims, ranks)]
+        capfd.readouterr()
+        f(dX.data_ptr(), core.data_ptr(), *[u.data_ptr() for u in U], *dims, *ranks)
+        torch.cuda.synchronize()
+        printed = float(capfd.readouterr().out.strip().splitlines()[-1])
+        out[name] = (np.linalg.norm(host(core).astype(np.float64)), printed)
+    (n_o, err_o), (n_r, err_r) = out["ours"], out["ref"]
+    assert abs(n_o - n_r) <= 1e-4 * n_r
+    assert abs(err_o - e64) <= 0.02 * e64, (err_o, e64)
+    assert abs(err_r - e64) <= 0.02 * e64, (err_r, e64)
