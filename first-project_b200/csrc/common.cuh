@@ -71,6 +71,25 @@ double *pinned_scalars();
 int prof_begin(cudaStream_t s);
 void prof_end(int k, cudaStream_t s);
 
+// A launch configuration with programmatic stream serialization: the kernel
+// may start while the previous kernel on the stream finishes; it must call
+// griddepcontrol.wait before it reads that kernel's output.
+struct PdlLaunch {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg;
+    PdlLaunch(unsigned grid, unsigned block, size_t smem, cudaStream_t s) {
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg = cudaLaunchConfig_t{};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+};
+
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

@@ -44,6 +44,7 @@ struct cud_cp_plan_s {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int kernels_per_sweep = -1;
     size_t reset_bytes = 0;  // fit scalars, fallback count and update ticket (zeroed by a refresh)
+    bool fused = false;      // sweep layout (fused_sweep_pays)
 };
 
 namespace {
@@ -68,9 +69,82 @@ int count_kernel_nodes(cudaGraph_t g) {
     return k;
 }
 
+NormalArgs normal_args(const cud_cp_plan_s *p, int mode) {
+    NormalArgs na;
+    for (int m = 0; m < p->order; m++) na.G[m] = p->G + (size_t)m * p->R * p->R;
+    na.nG = p->order;
+    na.mode = mode;
+    na.R = (int)p->R;
+    na.Vinv = p->Vinv;
+    na.work = p->work;
+    na.fallbacks = p->fallbacks;
+    return na;
+}
+
+// The sweep for R <= FU_RMAX.  Per mode n, on the main stream: MTTKRP_n
+// (split partials left unsummed), then one kernel that sums them and forms
+// U_n = M V_n^-1.  On the side stream, beside the next MTTKRP: the Gram of
+// U_n, then V_{n+1}^-1 (it needs G_n); after the last mode, its Gram and the
+// fit instead, joined at the end of the sweep.  V_0^-1 runs beside MTTKRP_0.
+// The main stream waits for the side stream only before each update.
+int enqueue_sweep_fused(cud_cp_plan_s *p, cudaStream_t s) {
+    int st;
+    const long R = p->R;
+    const int N = p->order;
+    CUD_CHECK(cudaEventRecord(p->ev_fork, s));
+    CUD_CHECK(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    if ((st = normal_inverse(normal_args(p, 0), p->side))) return st;
+    CUD_CHECK(cudaEventRecord(p->ev_join, p->side));
+    for (int n = 0; n < N; n++) {
+        MttkrpParts parts;
+        st = mttkrp_run_parts(p->X, N, p->dims, (const float *const *)p->U, n, R, p->M, p->opt.precision, p->ws, s,
+                              &parts);
+        if (st) return st;
+        CUD_CHECK(cudaStreamWaitEvent(s, p->ev_join, 0));
+        if ((st = update_from_parts(parts, p->Vinv, p->dims[n], (int)R, p->M, p->U[n], s))) return st;
+        CUD_CHECK(cudaEventRecord(p->ev_fork, s));
+        CUD_CHECK(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+        UpdateArgs ua;
+        ua.M = p->U[n];  // Gram of U_n
+        ua.I = p->dims[n];
+        ua.R = (int)R;
+        // beside the next MTTKRP, whose grid leaves four CTA slots free
+        ua.max_blocks = (n + 1 < N) ? 4 : 0;
+        ua.G_out = p->G + (size_t)n * R * R;
+        ua.gpart = p->gpart;
+        ua.counter = p->counter;
+        if (n == N - 1) {
+            for (int m = 0; m < N; m++) ua.Gall[m] = p->G + (size_t)m * R * R;
+            ua.nG = N;
+            ua.mode = n;
+            ua.normx2 = p->normx2;
+            ua.fit_out = p->fit;
+            ua.Mfit = p->M;
+        }
+        if ((st = factor_update(ua, p->side))) return st;
+        if (n + 1 < N && (st = normal_inverse(normal_args(p, n + 1), p->side))) return st;
+        CUD_CHECK(cudaEventRecord(p->ev_join, p->side));
+    }
+    CUD_CHECK(cudaStreamWaitEvent(s, p->ev_join, 0));
+    return CUD_OK;
+}
+
+// The fused sweep lengthens the side stream (the Gram of U_n, then
+// V_{n+1}^-1) to take the split reduce and the Gram off the main one; it
+// pays when each MTTKRP is long enough to hide that side stream.  Estimates:
+// an MTTKRP streams X at about 6 TB/s; the side stream takes about 25 us
+// plus 0.8 us per pivot of the R x R inverse (B200, measured at R = 16-64).
+bool fused_sweep_pays(const cud_cp_plan_s *p) {
+    if (p->R > FU_RMAX) return false;
+    double xbytes = 4.0;
+    for (int m = 0; m < p->order; m++) xbytes *= (double)p->dims[m];
+    return xbytes / 6.0e6 >= 25.0 + 0.8 * (double)p->R;
+}
+
 int enqueue_sweep(cud_cp_plan_s *p, cudaStream_t s) {
     int st;
     const long R = p->R;
+    if (p->fused) return enqueue_sweep_fused(p, s);
     for (int n = 0; n < p->order; n++) {
         // fork: V^-1 of mode n on the side stream, concurrent with the MTTKRP
         CUD_CHECK(cudaEventRecord(p->ev_fork, s));
@@ -338,6 +412,7 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     SideStream ss;
     int st = ss.open(as_stream(stream));
     p->reset_bytes = off_P - off_F;
+    p->fused = fused_sweep_pays(p);
     if (st == CUD_OK) st = plan_refresh(p, ss.s);
     if (st == CUD_OK) st = normal_inverse_prepare();
     if (st == CUD_OK && opt.use_graph) {

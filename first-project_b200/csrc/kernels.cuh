@@ -95,12 +95,28 @@ int mttkrp_simt_f64(const double *X, int order, const long *dims, const double *
 // Tensor-core path (mttkrp_tc.cu): CUD_OK and the workspace size when it
 // applies to this shape/precision, CUD_ERR_UNSUPPORTED otherwise.
 int mttkrp_tc_query(int order, const long *dims, int mode, long R, int precision, size_t *ws_bytes);
+// Where an MTTKRP left its result: M(q, r) = the sum over z < splits of
+// part[z zs + q qs + r rs], taken in FP64 in z order, or NaN everywhere when
+// *error is set (a CTA whose bounded wait expired).
+struct MttkrpParts {
+    const float *part;
+    long zs, qs, rs;
+    int splits;
+    const int *error;  // null: no flag
+};
+// With `parts` set, the split reduce is left to the caller: the partials'
+// layout is returned there and `out` is not written.
 int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U, int mode,
-              long R, float *out, int precision, void *ws, cudaStream_t s);
+              long R, float *out, int precision, void *ws, cudaStream_t s, MttkrpParts *parts = nullptr);
 // Dispatcher (mttkrp.cu): tensor cores when they apply, else CUDA cores.
 size_t mttkrp_ws_bytes(int order, const long *dims, int mode, long R, int precision);
 int mttkrp_run(const float *X, int order, const long *dims, const float *const *U, int mode,
                long R, float *out, int precision, void *ws, cudaStream_t s);
+// As mttkrp_run, for a consumer that sums the split partials itself: a
+// tensor-core MTTKRP returns its partials in *parts (out not written); any
+// other path writes out and describes it as one column-major split.
+int mttkrp_run_parts(const float *X, int order, const long *dims, const float *const *U, int mode,
+                     long R, float *out, int precision, void *ws, cudaStream_t s, MttkrpParts *parts);
 
 // Mode product Y = X x_mode W (contract.cu); W is J x dims[mode], or its
 // transpose when w_trans is set.

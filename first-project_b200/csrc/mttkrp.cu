@@ -36,6 +36,20 @@ int mttkrp_run(const float *X, int order, const long *dims, const float *const *
     return mttkrp_simt_rounded(X, order, dims, U, mode, R, out, round_mode(precision), ws, s);
 }
 
+int mttkrp_run_parts(const float *X, int order, const long *dims, const float *const *U, int mode, long R,
+                     float *out, int precision, void *ws, cudaStream_t s, MttkrpParts *parts) {
+    if (precision != CUD_PREC_FP32) {
+        size_t b = 0;
+        if (mttkrp_tc_query(order, dims, mode, R, precision, &b) == CUD_OK) {
+            int st = mttkrp_tc(X, order, dims, U, mode, R, out, precision, ws, s, parts);
+            if (st != CUD_ERR_UNSUPPORTED) return st;
+        }
+    }
+    int st = mttkrp_simt_rounded(X, order, dims, U, mode, R, out, round_mode(precision), ws, s);
+    if (st == CUD_OK) *parts = MttkrpParts{out, 0, 1, dims[mode], 1, nullptr};
+    return st;
+}
+
 }  // namespace cud
 
 using namespace cud;

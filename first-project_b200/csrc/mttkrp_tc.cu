@@ -1183,24 +1183,6 @@ __global__ void __launch_bounds__(256) k_sum_tc_partials(const float *__restrict
     }
 }
 
-// A launch configuration with programmatic stream serialization (the
-// kernel may start while the previous one on the stream finishes).
-struct PdlLaunch {
-    cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg;
-    PdlLaunch(unsigned grid, unsigned block, size_t smem, cudaStream_t s) {
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg = cudaLaunchConfig_t{};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3(block);
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = s;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-    }
-};
-
 void sum_tc_partials(const float *part, int splits, long Q, long R, long Rp, const int *error, float *out,
                      cudaStream_t s) {
     const long n = Q * Rp;
@@ -1393,7 +1375,7 @@ int mttkrp_tc_query(int order, const long *dims, int mode, long R, int precision
 }
 
 int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U, int mode, long R,
-              float *out, int precision, void *ws, cudaStream_t s) {
+              float *out, int precision, void *ws, cudaStream_t s, MttkrpParts *parts) {
     TcPlan p;
     if (!tc_plan(order, dims, mode, R, precision, p)) return CUD_ERR_UNSUPPORTED;
     if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return CUD_ERR_UNSUPPORTED;
@@ -1499,6 +1481,10 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
         int st = (p.ctas_per_sm == 2) ? launch_pb<2>(tmap, a, smem, grid, s) : launch_pb<1>(tmap, a, smem, grid, s);
         prof_end(pk, s);
         if (st) return st;
+        if (parts) {
+            *parts = MttkrpParts{a.part, p.Q * a.Rp, a.Rp, 1, (int)p.splits, a.error};
+            return CUD_OK;
+        }
         sum_tc_partials(a.part, (int)p.splits, p.Q, R, a.Rp, a.error, out, s);
         CUD_CHECK_LAUNCH("mttkrp_tc reduce");
         return CUD_OK;
@@ -1521,6 +1507,10 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
     }
     prof_end(pk, s);
     if (st) return st;
+    if (parts) {
+        *parts = MttkrpParts{a.part, p.Q * a.Rp, a.Rp, 1, (int)p.splits, a.error};
+        return CUD_OK;
+    }
     sum_tc_partials(a.part, (int)p.splits, p.Q, R, a.Rp, a.error, out, s);
     CUD_CHECK_LAUNCH("mttkrp_tc reduce");
     return CUD_OK;

@@ -40,9 +40,20 @@ struct UpdateArgs {
     int nG = 0, mode = 0;
     double normx2 = 0.0;
     double *fit_out = nullptr;     // [fit, fit_prev, inner, ||Xhat||^2]
+    // with Vinv null and fit_out set: the MTTKRP result paired with U = M in
+    // <M, U> (null: M itself)
+    const float *Mfit = nullptr;
+    // at most this many row-pass CTAs (0: as many as fill the GPU); a small
+    // cap keeps a Gram beside a full-GPU kernel from taking its CTA slots
+    int max_blocks = 0;
 };
 // Fused U = M Vinv, G = U^T U (+ fit), deterministic multi-CTA reduction.
 int factor_update(const UpdateArgs &a, cudaStream_t s);
+// U = M V^-1 from an MTTKRP's split partials in one kernel (M, rounded to
+// FP32, is written too); CUD_ERR_UNSUPPORTED above FU_RMAX.
+constexpr int FU_RMAX = 64;
+int update_from_parts(const MttkrpParts &pp, const double *Vinv, long I, int R, float *M, float *U,
+                      cudaStream_t s);
 size_t update_ws_doubles(long I, long R);
 
 int factor_gram(const float *U, long I, long R, double *G, cudaStream_t s);

@@ -554,3 +554,148 @@ def test_residual_ffma_restated_matches_fp64(dims, R):
     want = float(np.sum((X - oracle.gencp(dims, facs, R)) ** 2))
     assert abs(res - want) <= 1e-9 * want
     assert abs(xx - float(np.sum(X ** 2))) <= 1e-12 * xx
+
+
+# ---- solve.cu k_normal_inverse_small: 16 x 16 threads own (ty + 16a, tx + 16b)
+def normal_inverse_small_restated(V):
+    """Gauss-Jordan as k_normal_inverse_small runs it: the owners of row k
+    and column k publish them (buffer k & 1), then every thread updates its
+    16 entries from the published copies only.  Returns (Vinv, failed)."""
+    R = V.shape[0]
+    v = np.zeros((64, 64))
+    v[:R, :R] = V
+    owner_rows = np.arange(64)          # i = ty + 16 a  <->  (ty, a) = (i % 16, i // 16)
+    maxdiag = np.max(np.abs(np.diag(V)))
+    rowb = np.zeros((2, 64)); colb = np.zeros((2, 64))
+    written = np.zeros((2, 64), bool)
+    for k in range(R):
+        kb, kk, buf = k >> 4, k & 15, k & 1
+        # row k: threads ty == kk with a == kb write columns tx + 16 b
+        ty, a = owner_rows % 16, owner_rows // 16
+        assert ((ty == kk) & (a == kb)).sum() == 1
+        rowb[buf] = v[k]; colb[buf] = v[:, k]
+        written[buf] = True
+        piv = rowb[buf][k]
+        if not (piv > 1e-13 * maxdiag) or not np.isfinite(piv):
+            return None, True
+        inv = 1.0 / piv
+        j = np.arange(64)
+        rj = np.where(j == k, 1.0, rowb[buf]) * inv
+        old = np.where(j[None, :] == k, 0.0, v)
+        v = np.where(np.arange(64)[:, None] == k, rj[None, :], old - colb[buf][:, None] * rj[None, :])
+    out = 0.5 * (v[:R, :R] + v[:R, :R].T)
+    # the padding stays zero
+    assert np.all(v[R:, :] == 0) and np.all(v[:, R:] == 0)
+    return out, False
+
+
+@pytest.mark.parametrize("R", [1, 5, 16, 33, 64])
+def test_normal_inverse_small_restated_inverts(R):
+    rng = np.random.default_rng(R)
+    A = rng.standard_normal((3 * R + 2, R))
+    B = rng.standard_normal((2 * R + 3, R))
+    V = (A.T @ A) * (B.T @ B)          # Hadamard of two Grams: SPD
+    Vi, failed = normal_inverse_small_restated(V)
+    assert not failed
+    assert np.linalg.norm(Vi @ V - np.eye(R)) <= 1e-8 * np.linalg.cond(V)
+
+
+def test_normal_inverse_small_restated_flags_singular():
+    A = np.random.default_rng(0).standard_normal((3, 8))
+    V = A.T @ A                          # rank 3 of 8
+    _, failed = normal_inverse_small_restated(V)
+    assert failed
+
+
+# ---- solve.cu k_update_fused: rb rows per CTA, split z of an entry by thread z mod T
+def update_fused_restated(parts, splits, I, R, zs, qs, rs, NT=256, RBMAX=8):
+    rb = min(RBMAX, max(1, -(-I // 256)))
+    grid = -(-I // rb)
+    vec = rs == 1 and qs % 4 == 0 and zs % 4 == 0 and qs >= -(-R // 4) * 4
+    M = np.full(I * R, np.nan)
+    count = np.zeros(parts.size, np.int64)
+    W = 4 if vec else 1                      # entries per load
+    RW = -(-R // W)                          # loads per row
+    for b in range(grid):
+        q0 = b * rb
+        nr = min(rb, I - q0)
+        items = nr * RW
+        T = 1 if items >= NT else NT // items
+        sums = {}
+        for t in range(NT):
+            if T == 1:
+                its, z0 = range(t, items, NT), 0
+            else:
+                it, z0 = t % items, t // items
+                if z0 >= T:
+                    continue
+                its = [it]
+            for it in its:
+                row, cw = divmod(it, RW)
+                base = (q0 + row) * qs + cw * W * rs
+                for z in range(z0, splits, T):
+                    for k in range(W):
+                        idx = base + k * rs + z * zs
+                        assert 0 <= idx < parts.size
+                        count[idx] += 1
+                        c = cw * W + k
+                        if c < R:
+                            sums[(row, c)] = sums.get((row, c), 0.0) + parts[idx]
+        for (row, c), v in sums.items():
+            q = q0 + row
+            assert np.isnan(M[q + I * c])
+            M[q + I * c] = v
+    return M, count
+
+
+@pytest.mark.parametrize("I,R,splits", [(512, 64, 73), (96, 32, 37), (128, 16, 36), (5, 3, 1), (700, 64, 3),
+                                        (4100, 8, 2), (300, 7, 5)])
+def test_update_fused_sums_every_split_once(I, R, splits):
+    Rp = -(-R // 4) * 4
+    rng = np.random.default_rng(I + R)
+    parts = rng.standard_normal(splits * I * Rp)
+    M, count = update_fused_restated(parts, splits, I, R, I * Rp, Rp, 1)
+    want = parts.reshape(splits, I, Rp).sum(0)[:, :R]
+    assert np.allclose(M.reshape(R, I).T, want)
+    used = count.reshape(splits, I, Rp)
+    # every entry of every split once; the float4 loads also touch the padding
+    assert np.all(used[:, :, :R] == 1) and np.all(used[:, :, R:] <= 1)
+    # the column-major single-split form (an MTTKRP that wrote M itself)
+    Mc = rng.standard_normal(I * R)
+    M2, count2 = update_fused_restated(Mc, 1, I, R, 0, 1, I)
+    assert np.array_equal(M2, Mc) and np.all(count2 == 1)
+
+
+def test_update_fused_shared_memory_fits():
+    # V^-1 (R^2) + M rows (FU_RB R) + 4 NT split sums, FP64, at R = 64
+    assert 8 * (64 * 64 + 8 * 64 + 4 * 256) <= 48 * 1024
+
+
+# ---- solve.cu k_gram_rows: thread t owns the 4 x 4 block tri(t) of the upper triangle
+def tri_pq(e):
+    q = int((np.sqrt(8.0 * e + 1.0) - 1.0) * 0.5)
+    while (q + 1) * (q + 2) // 2 <= e:
+        q += 1
+    while q * (q + 1) // 2 > e:
+        q -= 1
+    return e - q * (q + 1) // 2, q
+
+
+@pytest.mark.parametrize("R", [1, 3, 4, 16, 31, 32, 63, 64])
+def test_gram_rows_blocks_cover_triangle_once(R):
+    R4 = -(-R // 4)
+    nblk = R4 * (R4 + 1) // 2
+    assert nblk <= 256
+    T = R * (R + 1) // 2
+    hits = np.zeros(T, np.int32)
+    for t in range(nblk):
+        bp, bq = tri_pq(t)
+        assert bp <= bq < R4
+        for u in range(4):
+            for v in range(4):
+                p, q = 4 * bp + u, 4 * bq + v
+                if p <= q < R:
+                    hits[q * (q + 1) // 2 + p] += 1
+    assert np.all(hits == 1)
+    # the staged rows: 128 x (4 R4 + 4) floats
+    assert 4 * 128 * (4 * R4 + 4) <= 48 * 1024
