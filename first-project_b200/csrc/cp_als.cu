@@ -30,6 +30,7 @@ struct cud_cp_plan_s {
     // device memory owned by the plan
     char *mem = nullptr;
     float *M = nullptr;
+    float *Mraw = nullptr;  // fused layout: where a CUDA-core MTTKRP writes (the update writes M)
     double *G = nullptr, *Vinv = nullptr, *work = nullptr, *fit = nullptr;
     int *fallbacks = nullptr;
     unsigned *counter = nullptr;  // ticket of the fused update's last-CTA reduction
@@ -38,6 +39,10 @@ struct cud_cp_plan_s {
     double *hbuf = nullptr;  // pinned
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // fused layout: kMultiSweeps sweeps in one graph, so each sweep's last
+    // Gram and fit (side stream) run beside the next sweep's first MTTKRP
+    cudaGraph_t graph_multi = nullptr;
+    cudaGraphExec_t exec_multi = nullptr;
     // the R x R inverse of mode n depends only on the other modes' Grams, so
     // it runs on a second stream beside the mode-n MTTKRP
     cudaStream_t side = nullptr;
@@ -81,13 +86,18 @@ NormalArgs normal_args(const cud_cp_plan_s *p, int mode) {
     return na;
 }
 
-// The sweep for R <= FU_RMAX.  Per mode n, on the main stream: MTTKRP_n
+constexpr int kMultiSweeps = 4;
+
+// The fused sweep (R <= FU_RMAX).  Per mode n, on the main stream: MTTKRP_n
 // (split partials left unsummed), then one kernel that sums them and forms
 // U_n = M V_n^-1.  On the side stream, beside the next MTTKRP: the Gram of
 // U_n, then V_{n+1}^-1 (it needs G_n); after the last mode, its Gram and the
 // fit instead, joined at the end of the sweep.  V_0^-1 runs beside MTTKRP_0.
-// The main stream waits for the side stream only before each update.
-int enqueue_sweep_fused(cud_cp_plan_s *p, cudaStream_t s) {
+// The main stream waits for the side stream only before each update, and,
+// with join_end, at the end of the sweep (a sweep followed by another in the
+// same graph leaves the last Gram and fit running beside the next MTTKRP:
+// the next update waits for them through the side stream's order).
+int enqueue_sweep_fused(cud_cp_plan_s *p, cudaStream_t s, bool join_end) {
     int st;
     const long R = p->R;
     const int N = p->order;
@@ -97,8 +107,8 @@ int enqueue_sweep_fused(cud_cp_plan_s *p, cudaStream_t s) {
     CUD_CHECK(cudaEventRecord(p->ev_join, p->side));
     for (int n = 0; n < N; n++) {
         MttkrpParts parts;
-        st = mttkrp_run_parts(p->X, N, p->dims, (const float *const *)p->U, n, R, p->M, p->opt.precision, p->ws, s,
-                              &parts);
+        st = mttkrp_run_parts(p->X, N, p->dims, (const float *const *)p->U, n, R, p->Mraw, p->opt.precision, p->ws,
+                              s, &parts);
         if (st) return st;
         CUD_CHECK(cudaStreamWaitEvent(s, p->ev_join, 0));
         if ((st = update_from_parts(parts, p->Vinv, p->dims[n], (int)R, p->M, p->U[n], s))) return st;
@@ -125,26 +135,29 @@ int enqueue_sweep_fused(cud_cp_plan_s *p, cudaStream_t s) {
         if (n + 1 < N && (st = normal_inverse(normal_args(p, n + 1), p->side))) return st;
         CUD_CHECK(cudaEventRecord(p->ev_join, p->side));
     }
-    CUD_CHECK(cudaStreamWaitEvent(s, p->ev_join, 0));
+    if (join_end) CUD_CHECK(cudaStreamWaitEvent(s, p->ev_join, 0));
     return CUD_OK;
 }
 
 // The fused sweep lengthens the side stream (the Gram of U_n, then
-// V_{n+1}^-1) to take the split reduce and the Gram off the main one; it
-// pays when each MTTKRP is long enough to hide that side stream.  Estimates:
-// an MTTKRP streams X at about 6 TB/s; the side stream takes about 25 us
-// plus 0.8 us per pivot of the R x R inverse (B200, measured at R = 16-64).
+// V_{n+1}^-1) to take the split reduce and the Gram off the main one.  On
+// B200 (BF16x3, ms a sweep, layout 1 / layout 2) it paid from 64 MiB of X
+// up: 256^3 R16 0.107 / 0.098, 64^4 R32 0.182 / 0.175, 384^3 R64 0.243 /
+// 0.236, 96^4 R16 0.390 / 0.366, 512^3 R64 0.406 / 0.349; below, the side
+// stream outlasts the MTTKRP: 128^3 R16 0.076 / 0.083, 192^3 R32 0.129 /
+// 0.135.  (Between, the two stay within 5 %: 128^3 R64 0.219 / 0.207,
+// 256^3 R64 0.204 / 0.211.)
 bool fused_sweep_pays(const cud_cp_plan_s *p) {
     if (p->R > FU_RMAX) return false;
     double xbytes = 4.0;
     for (int m = 0; m < p->order; m++) xbytes *= (double)p->dims[m];
-    return xbytes / 6.0e6 >= 25.0 + 0.8 * (double)p->R;
+    return xbytes >= 64.0 * 1024 * 1024;
 }
 
 int enqueue_sweep(cud_cp_plan_s *p, cudaStream_t s) {
     int st;
     const long R = p->R;
-    if (p->fused) return enqueue_sweep_fused(p, s);
+    if (p->fused) return enqueue_sweep_fused(p, s, true);
     for (int n = 0; n < p->order; n++) {
         // fork: V^-1 of mode n on the side stream, concurrent with the MTTKRP
         CUD_CHECK(cudaEventRecord(p->ev_fork, s));
@@ -229,6 +242,7 @@ extern "C" void cud_cp_default_options(cud_cp_options *opt) {
     opt->use_graph = 1;
     opt->check_every = 1;
     opt->target_fit = 0.0;
+    opt->sweep_layout = 0;
 }
 
 extern "C" int cud_cp_init_curand(int order, const long *dims, long R, float *const *U,
@@ -311,6 +325,8 @@ extern "C" int cud_cp_plan_destroy(cud_cp_plan p) {
     cudaSetDevice(p->device);
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->exec_multi) cudaGraphExecDestroy(p->exec_multi);
+    if (p->graph_multi) cudaGraphDestroy(p->graph_multi);
     if (p->side) {
         cudaStreamSynchronize(p->side);
         cudaStreamDestroy(p->side);
@@ -352,7 +368,8 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     cud_cp_options opt;
     cud_cp_default_options(&opt);
     if (opt_in) opt = *opt_in;
-    if (opt.max_sweeps < 0 || opt.check_every < 0 || opt.precision < 0 || opt.precision > CUD_PREC_DEFAULT)
+    if (opt.max_sweeps < 0 || opt.check_every < 0 || opt.precision < 0 || opt.precision > CUD_PREC_DEFAULT ||
+        opt.sweep_layout < 0 || opt.sweep_layout > 2)
         return set_status(CUD_ERR_INVALID_ARGUMENT);
     if (opt.check_every == 0) opt.check_every = 1;
 
@@ -373,7 +390,8 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     for (int m = 0; m < order; m++) wsb = std::max(wsb, mttkrp_ws_bytes(order, dims, m, R, opt.precision));
     auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
     size_t off_M = 0;
-    size_t off_G = off_M + up(sizeof(float) * maxd * R);
+    size_t off_Mr = off_M + up(sizeof(float) * maxd * R);
+    size_t off_G = off_Mr + up(sizeof(float) * maxd * R);
     size_t off_V = off_G + up(sizeof(double) * order * R * R);
     size_t off_W = off_V + up(sizeof(double) * R * R);
     size_t off_F = off_W + up(sizeof(double) * 2 * R * R);
@@ -393,6 +411,7 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
         return set_status(CUD_ERR_NO_MEMORY);
     }
     p->M = (float *)(p->mem + off_M);
+    p->Mraw = (float *)(p->mem + off_Mr);
     p->G = (double *)(p->mem + off_G);
     p->Vinv = (double *)(p->mem + off_V);
     p->work = (double *)(p->mem + off_W);
@@ -412,7 +431,7 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     SideStream ss;
     int st = ss.open(as_stream(stream));
     p->reset_bytes = off_P - off_F;
-    p->fused = fused_sweep_pays(p);
+    p->fused = (opt.sweep_layout == 2 && R <= FU_RMAX) || (opt.sweep_layout == 0 && fused_sweep_pays(p));
     if (st == CUD_OK) st = plan_refresh(p, ss.s);
     if (st == CUD_OK) st = normal_inverse_prepare();
     if (st == CUD_OK && opt.use_graph) {
@@ -429,6 +448,20 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
                 else p->kernels_per_sweep = count_kernel_nodes(p->graph);
             }
         }
+        if (st == CUD_OK && p->fused) {
+            if (cudaStreamBeginCapture(ss.s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                st = CUD_ERR_CUDA;
+            } else {
+                int cst = CUD_OK;
+                for (int k = 0; k < kMultiSweeps && cst == CUD_OK; k++)
+                    cst = enqueue_sweep_fused(p, ss.s, k == kMultiSweeps - 1);
+                e = cudaStreamEndCapture(ss.s, &p->graph_multi);
+                if (cst) st = cst;
+                else if (e != cudaSuccess) st = cuda_status(e, "cp plan capture (multi)");
+                else if ((e = cudaGraphInstantiate(&p->exec_multi, p->graph_multi, 0)) != cudaSuccess)
+                    st = cuda_status(e, "cp plan instantiate (multi)");
+            }
+        }
     }
     if (st == CUD_OK && cudaStreamSynchronize(ss.s) != cudaSuccess) st = CUD_ERR_CUDA;
     ss.close();
@@ -443,12 +476,17 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
 extern "C" int cud_cp_plan_run(cud_cp_plan p, int sweeps, void *stream) {
     if (!p || sweeps < 0) return set_status(CUD_ERR_INVALID_ARGUMENT);
     cudaStream_t s = as_stream(stream);
-    for (int i = 0; i < sweeps; i++) {
-        if (p->exec) {
+    for (int i = 0; i < sweeps;) {
+        if (p->exec_multi && sweeps - i >= kMultiSweeps) {
+            CUD_CHECK(cudaGraphLaunch(p->exec_multi, s));
+            i += kMultiSweeps;
+        } else if (p->exec) {
             CUD_CHECK(cudaGraphLaunch(p->exec, s));
+            i++;
         } else {
             int st = enqueue_sweep(p, s);
             if (st) return set_status(st);
+            i++;
         }
     }
     return set_status(CUD_OK);
@@ -502,7 +540,8 @@ bool plan_matches(const cud_cp_plan_s *p, const float *X, int order, const long 
     int dev = -1;
     cudaGetDevice(&dev);
     if (!p || p->device != dev || p->X != X || p->order != order || p->R != R ||
-        p->opt.precision != opt.precision || (p->opt.use_graph != 0) != (opt.use_graph != 0))
+        p->opt.precision != opt.precision || (p->opt.use_graph != 0) != (opt.use_graph != 0) ||
+        p->opt.sweep_layout != opt.sweep_layout)
         return false;
     for (int m = 0; m < order; m++)
         if (p->dims[m] != dims[m] || p->U[m] != U[m]) return false;

@@ -57,7 +57,7 @@ _d = ctypes.c_double
 
 class CpOptions(ctypes.Structure):
     _fields_ = [("max_sweeps", _i), ("tol", _d), ("precision", _i),
-                ("use_graph", _i), ("check_every", _i), ("target_fit", _d)]
+                ("use_graph", _i), ("check_every", _i), ("target_fit", _d), ("sweep_layout", _i)]
 
 
 class GemmEpilogue(ctypes.Structure):
@@ -359,11 +359,12 @@ def cp_default_options() -> CpOptions:
 
 
 def cp_als(X, dims, R, factors, max_sweeps=500, tol=0.0, precision=PREC_DEFAULT,
-           use_graph=True, check_every=1, target_fit=0.0, stream=None) -> CpResult:
+           use_graph=True, check_every=1, target_fit=0.0, stream=None, layout=0) -> CpResult:
     """CP-ALS from the given initial factors (updated in place).  Stops after
     max_sweeps, when |fit - fit_prev| < tol (tol > 0), or when fit >=
-    target_fit (target_fit > 0)."""
-    opt = CpOptions(max_sweeps, tol, precision, 1 if use_graph else 0, check_every, target_fit)
+    target_fit (target_fit > 0).  layout: the sweep layout (0 by size, 1, 2;
+    cud_cp_options.sweep_layout)."""
+    opt = CpOptions(max_sweeps, tol, precision, 1 if use_graph else 0, check_every, target_fit, layout)
     res = CpResult()
     _check(_lib.cud_cp_als(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
                            ctypes.byref(opt), ctypes.byref(res), _stream(stream)), "cp_als")
@@ -398,9 +399,9 @@ class CpPlan:
     """Reusable CP-ALS plan (cud_cp_plan_*): workspace plus the captured
     per-sweep CUDA graph; `run(n)` enqueues n sweeps without synchronising."""
 
-    def __init__(self, X, dims, R, factors, precision=PREC_DEFAULT, use_graph=True, stream=None):
+    def __init__(self, X, dims, R, factors, precision=PREC_DEFAULT, use_graph=True, stream=None, layout=0):
         self._keep = (X, list(factors))
-        opt = CpOptions(0, 0.0, precision, 1 if use_graph else 0, 1, 0.0)
+        opt = CpOptions(0, 0.0, precision, 1 if use_graph else 0, 1, 0.0, layout)
         h = _vp()
         _check(_lib.cud_cp_plan_create(_ptr(X), len(dims), _longs(dims), R, _ptrs(factors),
                                        ctypes.byref(opt), _stream(stream), ctypes.byref(h)),

@@ -207,6 +207,11 @@ typedef struct cud_cp_options {
     int check_every;  /* read the fit back every this many sweeps (>= 1)       */
     double target_fit; /* also stop once the exact fit >= target_fit, checked */
                        /* every check_every sweeps (<= 0 disables)            */
+    int sweep_layout;  /* 0: by size; 1: per mode, split reduce then update  */
+                       /* with its Gram, V^-1 beside the MTTKRP; 2 (R <= 64):*/
+                       /* the update sums the MTTKRP partials itself, the Gram*/
+                       /* and the next V^-1 run beside the next MTTKRP, four  */
+                       /* sweeps a graph.  Results agree to rounding.         */
 } cud_cp_options;
 
 typedef struct cud_cp_result {
