@@ -714,6 +714,18 @@ def run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_n
         for _ in range(args.warmup):
             cp.sweep()
     torch.cuda.synchronize()
+    # one sweep (kernels and all-reduces) captured in a CUDA graph; every
+    # rank takes the same decision (all-reduced), eager sweeps otherwise
+    with torch.cuda.stream(stream):
+        ok = cp.capture(torch, stream)
+    flag = torch.tensor([0.0 if ok else 1.0], device="cuda")
+    dist.all_reduce(flag)
+    if float(flag.item()) > 0:
+        cp.release()
+    graphed = cp.graph is not None
+    with torch.cuda.stream(stream):
+        cp.sweep()
+    torch.cuda.synchronize()
     dist.barrier()
     with ClockSampler(local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -765,6 +777,7 @@ def run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_n
                        workload=f"cp_als_sweep_{'x'.join(map(str, dims[:-1]))}x{dims[-1]}N_r{R}",
                        parallelism=f"sharded along the last mode over {world} ranks, NCCL all-reduce"),
         "gpu_launches": per_sweep_launches * args.steps * world,
+        "sweep_graph": graphed,
         "fit_after_timed_sweeps": round(fit, 8),
         "clocks": clk.summary(),
         "e2e": {"value": round(world * sweep_bytes(dims, R) * args.e2e_sweeps / e2e_s / 1e9, 3),
@@ -774,6 +787,8 @@ def run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_n
         "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                      "traffic": None, "note": "kernel roofline reported by the 1-GPU run"},
     }
+    cp.release()  # the graph holds NCCL calls: released before the group goes
+    torch.cuda.synchronize()
     dist.barrier()
     dist.destroy_process_group()
     if rank == 0:

@@ -24,27 +24,55 @@ import math
 class ShardedCP:
     def __init__(self, ops, comm, X, local_dims, R, factors):
         """factors[m] for m < N-1 are the full I_m x R factors (identical on
-        every rank); factors[N-1] holds this rank's rows of the last factor."""
+        every rank); factors[N-1] holds this rank's rows of the last factor.
+        The factors are updated in place; every buffer a sweep touches is
+        allocated here, so a sweep can be captured (see capture)."""
         self.ops, self.comm = ops, comm
         self.X, self.dims, self.R = X, list(local_dims), R
         self.U = list(factors)
         self.N = len(local_dims)
+        self.M = [ops.alloc(d * R) for d in self.dims]
         self.G = [ops.gram(u, d) for u, d in zip(self.U, self.dims)]
         self.G[-1] = comm.all_reduce(self.G[-1])
         self.normx2 = comm.all_reduce_scalar(ops.norm2(X))
         self.M_last = None
+        self.graph = None
 
     def sweep(self):
+        if self.graph is not None:
+            self.graph.replay()
+            return
         N = self.N
         for n in range(N):
-            M = self.ops.mttkrp(self.X, self.dims, self.U, n, self.R)
+            M = self.ops.mttkrp(self.X, self.dims, self.U, n, self.R, out=self.M[n])
             if n < N - 1:
                 M = self.comm.all_reduce(M)
-            self.U[n] = self.ops.solve(M, self.dims[n], self.R, self.G, n)
-            G = self.ops.gram(self.U[n], self.dims[n])
+            self.U[n] = self.ops.solve(M, self.dims[n], self.R, self.G, n, out=self.U[n])
+            G = self.ops.gram(self.U[n], self.dims[n], out=self.G[n])
             self.G[n] = self.comm.all_reduce(G) if n == N - 1 else G
             if n == N - 1:
                 self.M_last = M
+
+    def capture(self, torch, stream):
+        """Captures one sweep (the per-rank kernels and the NCCL all-reduces)
+        in a CUDA graph that sweep() replays; returns False, leaving eager
+        sweeps, when the capture is refused.  Call after a warm-up sweep (the
+        library's workspaces and the communicator exist) and release() before
+        the process group is destroyed."""
+        g = torch.cuda.CUDAGraph()
+        try:
+            # thread-local capture: the communicator's own threads keep
+            # making CUDA calls while this thread captures
+            with torch.cuda.graph(g, stream=stream, capture_error_mode="thread_local"):
+                self.sweep()
+        except Exception:
+            self.graph = None
+            return False
+        self.graph = g
+        return True
+
+    def release(self):
+        self.graph = None
 
     def fit(self):
         inner, nh = self.ops.fit_terms(self.M_last, self.U[-1], self.G, self.R)
@@ -72,7 +100,8 @@ class TorchComm:
 
 
 class CudaOps:
-    """Per-rank compute on the GPU through the library's C ABI."""
+    """Per-rank compute on the GPU through the library's C ABI; with `out`
+    the result goes into the given buffer (no allocation)."""
 
     def __init__(self, cd, precision, stream=None):
         import torch
@@ -80,23 +109,29 @@ class CudaOps:
         self.torch = torch
         self._work = None
 
-    def mttkrp(self, X, dims, U, mode, R):
-        out = self.torch.empty(dims[mode] * R, device="cuda")
+    def alloc(self, n):
+        return self.torch.empty(n, device="cuda")
+
+    def mttkrp(self, X, dims, U, mode, R, out=None):
+        if out is None:
+            out = self.torch.empty(dims[mode] * R, device="cuda")
         self.cd.mttkrp(X, dims, U, mode, R, out, self.precision, stream=self.stream)
         return out
 
-    def solve(self, M, I, R, G, mode):
+    def solve(self, M, I, R, G, mode, out=None):
         if self._work is None or self._work.numel() < 3 * R * R + 2:
             self._work = self.torch.zeros(3 * R * R + 2, dtype=self.torch.float64, device="cuda")
-        U = self.torch.empty(I * R, device="cuda")
-        self.cd.cp_solve(M, I, R, G, mode, U, self._work, stream=self.stream)
-        return U
+        if out is None:
+            out = self.torch.empty(I * R, device="cuda")
+        self.cd.cp_solve(M, I, R, G, mode, out, self._work, stream=self.stream)
+        return out
 
-    def gram(self, U, I):
+    def gram(self, U, I, out=None):
         R = U.numel() // I
-        G = self.torch.empty(R * R, dtype=self.torch.float64, device="cuda")
-        self.cd.factor_gram(U, I, R, G, stream=self.stream)
-        return G
+        if out is None:
+            out = self.torch.empty(R * R, dtype=self.torch.float64, device="cuda")
+        self.cd.factor_gram(U, I, R, out, stream=self.stream)
+        return out
 
     def fit_terms(self, M, U, G, R):
         return self.cd.cp_fit_terms(M, U, G, R, stream=self.stream)

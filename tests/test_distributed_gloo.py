@@ -20,21 +20,32 @@ R = 3
 SWEEPS = 6
 
 
-class OracleOps:
-    def mttkrp(self, X, dims, U, mode, R):
-        return torch.from_numpy(oracle.mttkrp(X, dims, [u.numpy() for u in U], mode, R))
+def _into(out, t):
+    """The ops' `out` convention: write into the given buffer and return it."""
+    if out is None:
+        return t
+    out.copy_(t)
+    return out
 
-    def solve(self, M, I, R, G, mode):
+
+class OracleOps:
+    def alloc(self, n):
+        return torch.empty(n, dtype=torch.float64)
+
+    def mttkrp(self, X, dims, U, mode, R, out=None):
+        return _into(out, torch.from_numpy(oracle.mttkrp(X, dims, [u.numpy() for u in U], mode, R)))
+
+    def solve(self, M, I, R, G, mode, out=None):
         V = np.ones((R, R))
         for m, g in enumerate(G):
             if m != mode:
                 V = V * g.numpy().reshape(R, R, order="F")
         Mm = M.numpy().reshape(I, R, order="F")
-        return torch.from_numpy(np.linalg.solve(V.T, Mm.T).T.reshape(-1, order="F").copy())
+        return _into(out, torch.from_numpy(np.linalg.solve(V.T, Mm.T).T.reshape(-1, order="F").copy()))
 
-    def gram(self, U, I):
+    def gram(self, U, I, out=None):
         Um = U.numpy().reshape(I, -1, order="F")
-        return torch.from_numpy((Um.T @ Um).reshape(-1, order="F").copy())
+        return _into(out, torch.from_numpy((Um.T @ Um).reshape(-1, order="F").copy()))
 
     def fit_terms(self, M, U, G, R):
         nh = np.ones((R, R))
