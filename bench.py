@@ -742,10 +742,15 @@ def run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_n
     with torch.cuda.stream(stream):
         fit = cp.fit()
     value = world * sweep_bytes(dims, R) * args.steps / (ms_total * 1e-3) / 1e9
-    # e2e: H2D of each rank's slab and factors, 10 sweeps, D2H of the factors
+    # e2e: H2D of each rank's slab and factors (into device buffers allocated
+    # once, as the 1-GPU e2e does), a new ShardedCP, 10 sweeps, D2H of the
+    # factors into pinned buffers
     hX = torch.empty(X.numel(), dtype=torch.float32, pin_memory=True)
     hX.copy_(X)
     hU = [u.cpu().pin_memory() for u in init]
+    dX = torch.empty_like(X)
+    dU = [torch.empty_like(u) for u in init]
+    oU = [torch.empty(u.numel(), dtype=torch.float32, pin_memory=True) for u in init]
     times = []
     for it in range(3):
         torch.cuda.synchronize()
@@ -753,12 +758,14 @@ def run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_n
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             e0.record(stream)
-            dX = hX.to("cuda", non_blocking=True)
-            dU = [u.to("cuda", non_blocking=True) for u in hU]
+            dX.copy_(hX, non_blocking=True)
+            for a, b in zip(dU, hU):
+                a.copy_(b, non_blocking=True)
             c2 = ShardedCP(CudaOps(cd, prec, stream=sptr), comm, dX, dims, R, dU)
             for _ in range(args.e2e_sweeps):
                 c2.sweep()
-            outs = [u.to("cpu", non_blocking=True) for u in c2.U]
+            for a, b in zip(oU, c2.U):
+                a.copy_(b, non_blocking=True)
             e1.record(stream)
         e1.synchronize()
         tt = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
@@ -826,6 +833,9 @@ def main():
                     help="side workloads to add as extra keys (comma list, or 'none')")
     ap.add_argument("--ws-train", type=int, default=204800, help="warm-start training samples")
     ap.add_argument("--ws-eval", type=int, default=10240, help="warm-start held-out tensors")
+    ap.add_argument("--sharded", action="store_true",
+                    help="run the sharded (multi-GPU) sweep path even with one rank (NCCL over one GPU; "
+                         "launch under torchrun) -- a check of that path, not the 1-GPU benchmark")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -843,7 +853,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dist = None
-    if world > 1:
+    if world > 1 or args.sharded:
         import torch.distributed as dist_mod
         from datetime import timedelta
         dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
@@ -862,7 +872,7 @@ def main():
             print(json.dumps(run_tucker_once(cd, torch, dims, [int(x) for x in args.tucker_ranks.split(",")])),
                   flush=True)
         return
-    if world > 1 and not args.only_mttkrp:
+    if (world > 1 or args.sharded) and not args.only_mttkrp:
         run_sharded(args, cd, torch, dist, rank, world, local, dims, R, prec, prec_name)
         return
     stream = torch.cuda.Stream()

@@ -291,6 +291,29 @@ extern "C" int cud_cp_solve(const float *M, long I, long R, int order, const dou
     return set_status(st);
 }
 
+extern "C" int cud_cp_normal_inverse(long R, int order, const double *const *G, int mode, double *work,
+                                     void *stream) {
+    if (R <= 0 || R > 160 || order < 2 || order > kMaxOrder || mode < 0 || mode >= order || !G || !work)
+        return set_status(CUD_ERR_INVALID_ARGUMENT);
+    NormalArgs na;
+    for (int m = 0; m < order; m++) {
+        if (m != mode && !G[m]) return set_status(CUD_ERR_INVALID_ARGUMENT);
+        na.G[m] = (m == mode) ? G[(mode + 1) % order] : G[m];
+    }
+    na.nG = order;
+    na.mode = mode;
+    na.R = (int)R;
+    na.Vinv = work;
+    na.work = work + R * R;
+    na.fallbacks = reinterpret_cast<int *>(work + 3 * R * R);
+    return set_status(normal_inverse(na, as_stream(stream)));
+}
+
+extern "C" int cud_cp_apply_inverse(const float *M, long I, long R, const double *work, float *U, void *stream) {
+    if (I <= 0 || R <= 0 || R > 160 || !M || !work || !U) return set_status(CUD_ERR_INVALID_ARGUMENT);
+    return set_status(apply_inverse(M, work, I, R, U, as_stream(stream)));
+}
+
 extern "C" int cud_cp_fit_terms(const float *M, const float *U, long IR, int order,
                                 const double *const *G, long R, double *inner, double *norm_hat2,
                                 void *stream) {

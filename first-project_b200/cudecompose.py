@@ -155,6 +155,8 @@ _sig("cud_cp_batched_tune", [_i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp, ct
                              ctypes.POINTER(_l), ctypes.POINTER(_i), ctypes.POINTER(_i), _vp])
 _sig("cud_factor_gram", [_vp, _l, _l, _vp, _vp])
 _sig("cud_cp_solve", [_vp, _l, _l, _i, ctypes.POINTER(_vp), _i, _vp, _vp, _vp])
+_sig("cud_cp_normal_inverse", [_l, _i, ctypes.POINTER(_vp), _i, _vp, _vp])
+_sig("cud_cp_apply_inverse", [_vp, _l, _l, _vp, _vp, _vp])
 _sig("cud_cp_fit_terms", [_vp, _vp, _l, _i, ctypes.POINTER(_vp), _l, ctypes.POINTER(_d),
                           ctypes.POINTER(_d), _vp])
 _sig("cud_tucker_hosvd", [_vp, _i, ctypes.POINTER(_l), ctypes.POINTER(_l), _vp,
@@ -504,6 +506,18 @@ def cp_solve(M, I, R, grams, mode, U, work, stream=None):
     device tensor of at least 3 R^2 + 2 elements."""
     _check(_lib.cud_cp_solve(_ptr(M), I, R, len(grams), _ptrs(grams), mode, _ptr(U), _ptr(work),
                              _stream(stream)), "cp_solve")
+
+
+def cp_normal_inverse(R, grams, mode, work, stream=None):
+    """V^-1 (V = Hadamard of the Grams other than `mode`) into the first R^2
+    doubles of work (float64 device tensor of at least 3 R^2 + 2)."""
+    _check(_lib.cud_cp_normal_inverse(R, len(grams), _ptrs(grams), mode, _ptr(work), _stream(stream)),
+           "cp_normal_inverse")
+
+
+def cp_apply_inverse(M, I, R, work, U, stream=None):
+    """U = M * V^-1 with V^-1 from cp_normal_inverse (in work)."""
+    _check(_lib.cud_cp_apply_inverse(_ptr(M), I, R, _ptr(work), _ptr(U), _stream(stream)), "cp_apply_inverse")
 
 
 def cp_fit_terms(M, U, grams, R, stream=None):

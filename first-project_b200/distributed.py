@@ -42,6 +42,9 @@ class ShardedCP:
         if self.graph is not None:
             self.graph.replay()
             return
+        if hasattr(self.ops, "inverse_begin"):
+            self._sweep_overlapped()
+            return
         N = self.N
         for n in range(N):
             M = self.ops.mttkrp(self.X, self.dims, self.U, n, self.R, out=self.M[n])
@@ -51,6 +54,28 @@ class ShardedCP:
             G = self.ops.gram(self.U[n], self.dims[n], out=self.G[n])
             self.G[n] = self.comm.all_reduce(G) if n == N - 1 else G
             if n == N - 1:
+                self.M_last = M
+
+    def _sweep_overlapped(self):
+        """The same sweep with a second stream (ops providing inverse_begin /
+        apply / side_gram): V_n^-1 needs only the other modes' Grams, so it
+        runs beside MTTKRP_n and its all-reduce; the Gram of U_n (n < N-1)
+        and V_{n+1}^-1 follow on the side stream while MTTKRP_{n+1} runs.
+        The last mode's Gram is all-reduced on the main stream, and every
+        side-stream step is waited for within the sweep (apply)."""
+        N, ops = self.N, self.ops
+        tok = ops.inverse_begin(self.G, self.R, 0)
+        for n in range(N):
+            M = ops.mttkrp(self.X, self.dims, self.U, n, self.R, out=self.M[n])
+            if n < N - 1:
+                M = self.comm.all_reduce(M)
+            self.U[n] = ops.apply(M, self.dims[n], self.R, tok, out=self.U[n])
+            if n < N - 1:
+                self.G[n] = ops.side_gram(self.U[n], self.dims[n], out=self.G[n])
+                tok = ops.inverse_begin(self.G, self.R, n + 1)
+            else:
+                G = ops.gram(self.U[n], self.dims[n], out=self.G[n])
+                self.G[n] = self.comm.all_reduce(G)
                 self.M_last = M
 
     def capture(self, torch, stream):
@@ -124,6 +149,37 @@ class CudaOps:
         if out is None:
             out = self.torch.empty(I * R, device="cuda")
         self.cd.cp_solve(M, I, R, G, mode, out, self._work, stream=self.stream)
+        return out
+
+    # The side stream: work enqueued there waits for everything queued so far
+    # on the current (main) stream; the main stream waits for it through the
+    # token apply() takes.  (self.stream must be the current torch stream.)
+    def _fork(self):
+        torch = self.torch
+        if getattr(self, "_side", None) is None:
+            self._side = torch.cuda.Stream()
+        ev = torch.cuda.Event()
+        ev.record()
+        self._side.wait_event(ev)
+        return self._side
+
+    def inverse_begin(self, G, R, mode):
+        if self._work is None or self._work.numel() < 3 * R * R + 2:
+            self._work = self.torch.zeros(3 * R * R + 2, dtype=self.torch.float64, device="cuda")
+        side = self._fork()
+        self.cd.cp_normal_inverse(R, G, mode, self._work, stream=side.cuda_stream)
+        done = self.torch.cuda.Event()
+        done.record(side)
+        return done
+
+    def apply(self, M, I, R, token, out):
+        self.torch.cuda.current_stream().wait_event(token)
+        self.cd.cp_apply_inverse(M, I, R, self._work, out, stream=self.stream)
+        return out
+
+    def side_gram(self, U, I, out):
+        side = self._fork()
+        self.cd.factor_gram(U, I, U.numel() // I, out, stream=side.cuda_stream)
         return out
 
     def gram(self, U, I, out=None):

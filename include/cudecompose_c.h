@@ -300,6 +300,12 @@ int cud_factor_gram(const float *U, long I, long R, double *G, void *stream);
  * pointers (R x R each); work holds 3 R^2 doubles + 16 bytes. */
 int cud_cp_solve(const float *M, long I, long R, int order, const double *const *G, int mode,
                  float *U, double *work, void *stream);
+/* cud_cp_solve in two halves, so the R x R inverse can run on another
+ * stream beside the mode's MTTKRP (it needs only the other modes' Grams):
+ * work (3 R^2 doubles + 16 bytes) receives V^-1 in its first R^2 doubles;
+ * then U = M * V^-1 (FP64 accumulation) reads it. */
+int cud_cp_normal_inverse(long R, int order, const double *const *G, int mode, double *work, void *stream);
+int cud_cp_apply_inverse(const float *M, long I, long R, const double *work, float *U, void *stream);
 /* Host results of the fit terms: inner = <M, U> (FP64) and
  * norm_hat2 = sum_{r,s} prod_m G[m][r,s]. */
 int cud_cp_fit_terms(const float *M, const float *U, long IR, int order, const double *const *G,
