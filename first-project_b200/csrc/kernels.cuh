@@ -118,6 +118,14 @@ int mttkrp_run(const float *X, int order, const long *dims, const float *const *
 int mttkrp_run_parts(const float *X, int order, const long *dims, const float *const *U, int mode,
                      long R, float *out, int precision, void *ws, cudaStream_t s, MttkrpParts *parts);
 
+// Exact CP residual pieces (residual.cu, residual_tc.cu): per-CTA partial
+// pairs summed in a fixed order into out[0..1]; the tensor-core residual
+// (order >= 3, R <= 64; the grid it launches, for sizing the partials).
+int sum_pairs(const double *part, long n, double *out, cudaStream_t s);
+bool residual_tc_plan(int order, const long *dims, long R, int *grid);
+int residual_tc(const float *X, int order, const long *dims, const float *const *U, long R, double *part,
+                double *out2, cudaStream_t s);
+
 // Mode product Y = X x_mode W (contract.cu); W is J x dims[mode], or its
 // transpose when w_trans is set.
 int mode_product(const float *X, int order, const long *dims, int mode, const float *W, long J,

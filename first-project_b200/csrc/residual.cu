@@ -181,6 +181,16 @@ __global__ void __launch_bounds__(256) k_sum_pairs(const double *part, long n, d
     if (threadIdx.x == 0) { out[0] = red[0][0]; out[1] = red[1][0]; }
 }
 
+}  // namespace
+
+int sum_pairs(const double *part, long n, double *out, cudaStream_t s) {
+    k_sum_pairs<<<1, 256, 0, s>>>(part, n, out);
+    CUD_CHECK_LAUNCH("cp_residual sum");
+    return CUD_OK;
+}
+
+namespace {
+
 // ---------------------------------------------------------------------------
 // FFMA fast path (R <= 64, mode-0 rows a multiple of 4, U_1's rows a
 // multiple of 32, X and U_1 16-byte aligned): the SGEMM-style tile of the
@@ -380,6 +390,8 @@ size_t cp_residual_ws_bytes(int order, const long *dims) {
     long qt, st, ch, sp;
     // the fast path's grid, for any rank (the partials are all it needs)
     if (residual_ffma_plan(order, dims, 1, qt, st, ch, sp)) parts = std::max(parts, (size_t)(qt * sp));
+    int tcg = 0;  // the tensor-core path's grid, for any rank it takes
+    if (residual_tc_plan(order, dims, 1, &tcg)) parts = std::max(parts, (size_t)tcg);
     return sizeof(double) * (2 * parts + 2);
 }
 
@@ -400,6 +412,10 @@ int cp_residual(const float *X, int order, const long *dims, const float *const 
         a.f.n++;
     }
     a.part = static_cast<double *>(ws);
+    {
+        const int st = residual_tc(X, order, dims, U, R, a.part, out2, s);
+        if (st != CUD_ERR_UNSUPPORTED) return st;
+    }
     long qt, stg, ch, sp;
     if (residual_ffma_plan(order, dims, R, qt, stg, ch, sp) && ((reinterpret_cast<uintptr_t>(X) |
                                                                reinterpret_cast<uintptr_t>(U[1])) & 15) == 0) {

@@ -168,6 +168,27 @@ def test_cp_residual_matches_reconstruction(cd, dims, R):
     assert abs(r2 - want_r2) <= 1e-5 * want_r2
 
 
+@pytest.mark.parametrize("dims,R", [((256, 200, 64), 16), ((96, 96, 40, 12), 32), ((512, 512, 32), 64),
+                                    ((132, 260, 9), 40)])
+def test_cp_residual_tensor_core_near_its_data(cd, dims, R):
+    """The tensor-core residual (order >= 3, R <= 64: BF16x3 reconstruction
+    in TMEM) on a model at fit ~0.999 of its tensor, where the residual is a
+    small difference: the residual within 1e-3 (relative) and the fit within
+    1e-6 of FP64 (ragged row tiles and U_1 chunks included)."""
+    rng = np.random.default_rng(sum(dims) + R)
+    facs = [rng.standard_normal(d * R).astype(np.float32) for d in dims]
+    rec = oracle.gencp(dims, [f.astype(np.float64) for f in facs], R)
+    X = (rec + 1e-3 * np.linalg.norm(rec) / np.sqrt(rec.size) * rng.standard_normal(rec.size)).astype(np.float32)
+    Xd = X.astype(np.float64)
+    want_r2 = float(np.sum((Xd - rec) ** 2))
+    want_x2 = float(np.sum(Xd ** 2))
+    r2, x2 = cd.cp_residual(dev_t(X), dims, [dev_t(f) for f in facs], R)
+    assert abs(x2 - want_x2) <= 1e-12 * want_x2
+    assert abs(r2 - want_r2) <= 1e-3 * want_r2, (r2, want_r2)
+    fit, want_fit = 1 - np.sqrt(r2 / x2), 1 - np.sqrt(want_r2 / want_x2)
+    assert abs(fit - want_fit) <= 1e-6, (fit, want_fit)
+
+
 def test_plan_true_fit_matches_direct(cd):
     dims, R = (40, 32, 24), 5
     X, init = low_rank(dims, R, seed=41, noise=1e-2)

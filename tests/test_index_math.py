@@ -699,3 +699,68 @@ def test_gram_rows_blocks_cover_triangle_once(R):
     assert np.all(hits == 1)
     # the staged rows: 128 x (4 R4 + 4) floats
     assert 4 * 128 * (4 * R4 + 4) <= 48 * 1024
+
+
+# ---- residual_tc.cu k_residual_tc: tiles, k split, B layout, TMEM and smem budget
+def residual_tc_plan(dims, R, sms=148):
+    if len(dims) < 3 or R > 64 or dims[0] % 4:
+        return None
+    Rpad = -(-R // 16) * 16
+    nq = -(-dims[1] // 128)
+    if 2 * nq * 128 * Rpad * 2 > 128 * 1024:
+        return None
+    K = int(np.prod(dims[2:]))
+    tiles = -(-dims[0] // 128)
+    cpt = max(1, min(K, sms // tiles))
+    return Rpad, nq, K, tiles, cpt
+
+
+@pytest.mark.parametrize("dims,R", [((512, 512, 512), 64), ((96, 96, 96, 96), 32), ((20, 16, 12), 3),
+                                    ((128, 128, 128), 16), ((4, 1000, 3), 9), ((1000, 200, 7, 3), 64)])
+def test_residual_tc_index_math(dims, R):
+    p = residual_tc_plan(dims, R)
+    assert p is not None
+    Rpad, nq, K, tiles, cpt = p
+    ctrl, xs, xbytes = 2048, 5, 128 * 32 * 4
+    bbytes = nq * 128 * Rpad * 2
+    assert bbytes % 4096 == 0                                   # the X ring stays 1024-aligned
+    assert 1024 + ctrl + 2 * bbytes + xs * xbytes <= 232448     # shared memory
+    assert 2 * 128 + 2 * 64 <= 512                              # TMEM: accumulators + A' buffers
+    # B words: every (chunk, row, k-chunk) once, inside one operand
+    kcs = Rpad // 8
+    offs = set()
+    for q in range(nq):
+        for jr in range(0, 128, 37):
+            for kc in range(kcs):
+                off = q * 128 * Rpad * 2 + jr * 16 + kc * 128 * 16
+                assert 0 <= off and off + 16 <= bbytes
+                offs.add(off)
+    # MMA descriptors: K step kk reads two 2048-byte K chunks of its chunk
+    for kk in range(Rpad // 16):
+        assert (2 * kk + 2) * 2048 <= 128 * Rpad * 2
+    # k ranges of a tile's CTAs partition [0, K)
+    covered = []
+    for zc in range(cpt):
+        kb, ke = K * zc // cpt, K * (zc + 1) // cpt
+        assert ke > kb
+        covered.extend(range(kb, ke))
+    assert covered == list(range(K))
+    # TMA coordinates: x (rows) 128-aligned inside the tensor, y and z in int32
+    assert (tiles - 1) * 128 < dims[0] and (tiles - 1) * 128 * 4 % 16 == 0
+    assert nq * 128 < 2 ** 31 and K < 2 ** 31
+    assert tiles * cpt <= 148
+
+
+def test_residual_tc_slices_reconstruct():
+    """The slice identity the kernel uses: Xh[:, :, k] = (U_0 diag(c_k)) U_1^T
+    with c_k the product of the slower factors' rows of k's digits."""
+    rng = np.random.default_rng(2)
+    dims, R = (6, 5, 4, 3), 3
+    U = [rng.standard_normal((d, R)) for d in dims]
+    full = np.einsum("ir,jr,kr,lr->ijkl", *U)
+    K = dims[2] * dims[3]
+    for k in range(K):
+        d2, d3 = k % dims[2], k // dims[2]
+        c = U[2][d2] * U[3][d3]
+        sl = (U[0] * c) @ U[1].T
+        assert np.allclose(sl, full[:, :, d2, d3])
