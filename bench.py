@@ -439,6 +439,28 @@ def leg_streamed(cd, torch, dims=(512, 512, 512), R=64, slab=64, sweeps=2):
             "link_bound_fraction": round((h2d / (copy_gbs * 1e9)) / sec, 3), "fit": round(fit, 6)}
 
 
+def run_residual_once(cd, torch, dims, R, reps=5):
+    """The exact CP residual (cud_cp_residual) of a synthetic rank-R model on
+    its tensor: `reps` calls after one warm-up, mean wall time per call (the
+    call reads its two scalars back) and the fit."""
+    X, _ = cd.make_cp_tensor(dims, R, seed=1)
+    U = cd.make_init(dims, R, seed=2)
+    cd.cp_residual(X, dims, U, R)
+    torch.cuda.synchronize()
+    cd.prof_enable(True)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        r2, x2 = cd.cp_residual(X, dims, U, R)
+    dt = (time.perf_counter() - t0) / reps
+    kms = cd.prof_kernel_times()
+    cd.prof_enable(False)
+    k_ms = sum(kms) / len(kms) if kms else None
+    return {"dims": list(dims), "rank": R, "ms_per_call": round(dt * 1e3, 4),
+            "kernel_ms": round(k_ms, 4) if k_ms else None,
+            "kernel_gbs": round(4 * X.numel() / (k_ms * 1e-3) / 1e9, 1) if k_ms else None,
+            "fit": 1 - (r2 / x2) ** 0.5}
+
+
 def run_tucker_once(cd, torch, dims, ranks):
     """One tensor-core HOSVD and one HOOI sweep (BF16x3) on a synthetic
     Tucker tensor of the given shape; wall times and reconstruction errors."""
@@ -824,6 +846,8 @@ def main():
                     help="run one Tucker HOSVD and one HOOI sweep on --dims with --tucker-ranks "
                          "(profiling runs) and exit")
     ap.add_argument("--tucker-ranks", default="16,16,16,16")
+    ap.add_argument("--only-residual", action="store_true",
+                    help="time the exact CP residual on --dims / --rank (profiling runs) and exit")
     ap.add_argument("--only-batched", type=int, default=0, metavar="N",
                     help="run 3 batched CP-ALS sweeps (one kernel launch each, no graph) on the first N "
                          "tensors of the batched workload (profiling runs) and exit")
@@ -866,6 +890,10 @@ def main():
     if args.only_batched:
         if rank == 0:
             print(json.dumps(run_batched_once(cd, torch, args.only_batched)), flush=True)
+        return
+    if args.only_residual:
+        if rank == 0:
+            print(json.dumps(run_residual_once(cd, torch, dims, R)), flush=True)
         return
     if args.only_tucker:
         if rank == 0:

@@ -18,10 +18,12 @@
 //     (double-buffered over chunks); B = U_1 split into hi and lo once per CTA
 //     and resident in shared memory in the canonical K-major layout;
 //   * one thread streams the matching X tiles (128 rows x 32 columns,
-//     TMA, a ring of RT_XS) -- X is read exactly once;
-//   * four epilogue warps read the accumulator row by row (tcgen05.ld) and
-//     the X tile from shared memory and add (x - xh)^2 (per tile in FP32)
-//     and x^2 (in FP64) into FP64 totals.
+//     TMA, a ring as deep as the shared memory beside U_1 allows, 2-12
+//     tiles) -- X is read exactly once;
+//   * eight epilogue warps (two per TMEM lane quarter, each half of the
+//     columns) read the accumulator row by row (tcgen05.ld) and the X tile
+//     from shared memory and add (x - xh)^2 (per tile in FP32) and x^2 (in
+//     FP64) into FP64 totals, four independent sums each.
 // Rows past I_0 and columns past I_1 are zero in A' and B and in the X tiles
 // (the TMA fill), so they add nothing.  Per-CTA totals are summed in a fixed
 // order by k_sum_pairs (deterministic).  Every wait is bounded; a CTA that
@@ -45,8 +47,13 @@ namespace {
 constexpr int RT_ROWS = 128;    // mode-0 rows per tile (TMEM lanes, MMA M)
 constexpr int RT_NJ = 128;      // U_1 rows per MMA (N) = one accumulator buffer
 constexpr int RT_XJ = 32;       // U_1 rows (X columns) per X tile
-constexpr int RT_XS = 5;        // X ring depth
-constexpr int RT_THREADS = 320; // warp 0 TMA, 1 MMA, 2-5 builders, 6-9 epilogue
+// Deepest X ring; the shared memory left after U_1 bounds it (6 tiles at
+// 512^3 R64).  Rings of 5, 8 and 12 tiles timed the same: the kernel is
+// bound by its per-slice chain (A' build -> MMA -> epilogue), not by the
+// bytes in flight.
+constexpr int RT_XSMAX = 12;
+constexpr int RT_THREADS = 448; // warp 0 TMA, 1 MMA, 2-5 builders, 6-13 epilogue
+constexpr int RT_EPI = 8;       // epilogue warps: two per TMEM lane quarter, 16 of every 32 columns each
 constexpr uint32_t RT_XBYTES = RT_ROWS * RT_XJ * 4;
 constexpr int RT_RMAX = 64;
 constexpr int RT_BMAX = 128 * 1024;  // U_1 hi + lo in shared memory
@@ -58,24 +65,32 @@ struct RtArgs {
     long I0, I1, K;
     int R, Rpad, nq;      // rank, rank rounded to 16, chunks of 128 U_1 rows
     int cpt;              // CTAs per row tile (they split k)
+    int xs;               // X ring depth
     double *part;         // [grid][2]
 };
 
 struct RtCtrl {
-    uint64_t x_full[RT_XS], x_empty[RT_XS];
+    uint64_t x_full[RT_XSMAX], x_empty[RT_XSMAX];
     uint64_t a_full[2], a_free[2], d_full[2], d_free[2], done;
     uint32_t tmem_base;
     int abort;
     const float *fU[kMaxOrder];
     long frows[kMaxOrder];
     float cvec[4][RT_RMAX];
-    double red[2][4];
+    double red[2][RT_EPI];
 };
 constexpr size_t RT_CTRL_BYTES = (sizeof(RtCtrl) + 1023) & ~size_t(1023);
 
 __host__ __device__ constexpr size_t rt_b_bytes(int Rpad, int nq) { return (size_t)nq * RT_NJ * Rpad * 2; }
-__host__ __device__ constexpr size_t rt_smem_bytes(int Rpad, int nq) {
-    return 1024 + RT_CTRL_BYTES + 2 * rt_b_bytes(Rpad, nq) + (size_t)RT_XS * RT_XBYTES;
+__host__ __device__ constexpr size_t rt_smem_bytes(int Rpad, int nq, int xs) {
+    return 1024 + RT_CTRL_BYTES + 2 * rt_b_bytes(Rpad, nq) + (size_t)xs * RT_XBYTES;
+}
+constexpr size_t RT_SMEM_MAX = 232448;
+// the deepest X ring that fits beside U_1
+int rt_ring(int Rpad, int nq) {
+    int xs = RT_XSMAX;
+    while (xs > 2 && rt_smem_bytes(Rpad, nq, xs) > RT_SMEM_MAX) xs--;
+    return xs;
 }
 
 __device__ __forceinline__ uint32_t rt_pack_bf16(float a, float b) {
@@ -108,15 +123,15 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
     volatile int *abort = &sm.abort;
 
     if (threadIdx.x == 0) {
-        for (int i = 0; i < RT_XS; i++) {
+        for (int i = 0; i < RT_XSMAX; i++) {
             ptx::mbar_init(&sm.x_full[i], 1);
-            ptx::mbar_init(&sm.x_empty[i], 4);  // the epilogue warps
+            ptx::mbar_init(&sm.x_empty[i], RT_EPI);  // the epilogue warps
         }
         for (int b = 0; b < 2; b++) {
             ptx::mbar_init(&sm.a_full[b], 4);   // the builder warps
             ptx::mbar_init(&sm.a_free[b], 1);   // tcgen05.commit
             ptx::mbar_init(&sm.d_full[b], 1);   // tcgen05.commit
-            ptx::mbar_init(&sm.d_free[b], 4);   // the epilogue warps
+            ptx::mbar_init(&sm.d_free[b], RT_EPI);   // the epilogue warps
         }
         ptx::mbar_init(&sm.done, 1);
         sm.abort = 0;
@@ -177,8 +192,8 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
             for (long kl = 0; kl < nk && !*abort; kl++) {
                 for (int q = 0; q < a.nq && !*abort; q++) {
                     for (int s = 0; s < RT_NJ / RT_XJ; s++, xi++) {
-                        const int slot = (int)(xi % RT_XS);
-                        const long use = xi / RT_XS;
+                        const int slot = (int)(xi % a.xs);
+                        const long use = xi / a.xs;
                         if (use > 0 && !ptx::mbar_wait(&sm.x_empty[slot], (uint32_t)((use - 1) & 1), abort)) break;
                         ptx::mbar_arrive_expect_tx(&sm.x_full[slot], RT_XBYTES);
                         ptx::tma_load_3d(xring + (size_t)slot * RT_XBYTES, &tmap, &sm.x_full[slot], (int)i0,
@@ -275,6 +290,8 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
         }
     } else {
         // ------------------------------------------------------------ epilogue
+        const int hcol = ((warp - 6) >> 2) * (RT_XJ / 2);  // this warp's 16 columns of each tile
+        double sr[4] = {0.0, 0.0, 0.0, 0.0}, sx[4] = {0.0, 0.0, 0.0, 0.0};
         long ci = 0, xi = 0;
         for (; ci < nchunks && !*abort; ci++) {
             const int db = (int)(ci & 1);
@@ -282,29 +299,36 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
             const bool ok = __all_sync(0xffffffffu, *abort == 0);  // warp-uniform exit before tcgen05.ld
             if (!ok) break;
             ptx::tc_fence_after();
+            // the chunk's accumulator columns of this warp, four loads and one wait
+            uint32_t v[RT_NJ / RT_XJ][16];
+#pragma unroll
+            for (int s = 0; s < RT_NJ / RT_XJ; s++)
+                ptx::tmem_ld16(tbase + lane_off + (uint32_t)db * RT_NJ + (uint32_t)(s * RT_XJ + hcol), v[s]);
+            ptx::tmem_wait_ld();
             bool stop = false;
+#pragma unroll
             for (int s = 0; s < RT_NJ / RT_XJ; s++, xi++) {
-                const int slot = (int)(xi % RT_XS);
-                if (!*abort) ptx::mbar_wait(&sm.x_full[slot], (uint32_t)((xi / RT_XS) & 1), abort);
+                const int slot = (int)(xi % a.xs);
+                if (!*abort) ptx::mbar_wait(&sm.x_full[slot], (uint32_t)((xi / a.xs) & 1), abort);
                 if (!__all_sync(0xffffffffu, *abort == 0)) {
                     stop = true;
                     break;
                 }
-                uint32_t v[32];
-                ptx::tmem_ld32(tbase + lane_off + (uint32_t)db * RT_NJ + (uint32_t)(s * RT_XJ), v);
-                ptx::tmem_wait_ld();
-                const float *xs = reinterpret_cast<const float *>(xring + (size_t)slot * RT_XBYTES);
+                const float *xs = reinterpret_cast<const float *>(xring + (size_t)slot * RT_XBYTES) + hcol * RT_ROWS;
                 // (x - xh)^2 per tile in FP32; x^2 in FP64 (exact products of
-                // FP32 values), so ||X||^2 matches an FP64 sum
-                float fr = 0.f;
+                // FP32 values), so ||X||^2 matches an FP64 sum; four chains
+                // each.  (FP32 tile sums for x^2 too measured 10 % faster at
+                // 512^3 R64 -- 0.159 against 0.176 ms -- for a 1e-9 error.)
+                float fr[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                for (int jj = 0; jj < RT_XJ; jj++) {
+                for (int jj = 0; jj < RT_XJ / 2; jj++) {
                     const float x = xs[jj * RT_ROWS + row];
-                    const float dv = x - __uint_as_float(v[jj]);
-                    fr = fmaf(dv, dv, fr);
-                    s_x = fma((double)x, (double)x, s_x);
+                    const float dv = x - __uint_as_float(v[s][jj]);
+                    fr[jj & 3] = fmaf(dv, dv, fr[jj & 3]);
+                    sx[jj & 3] = fma((double)x, (double)x, sx[jj & 3]);
                 }
-                s_res += (double)fr;
+#pragma unroll
+                for (int c = 0; c < 4; c++) sr[c] += (double)fr[c];
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(&sm.x_empty[slot]);
             }
@@ -313,6 +337,8 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
             __syncwarp();
             if (lane == 0) ptx::mbar_arrive(&sm.d_free[db]);
         }
+        s_res = (sr[0] + sr[1]) + (sr[2] + sr[3]);
+        s_x = (sx[0] + sx[1]) + (sx[2] + sx[3]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             s_res += __shfl_xor_sync(0xffffffffu, s_res, o);
@@ -327,9 +353,9 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
     // ------------------------------------------------------------ teardown
     if (threadIdx.x == 0 && *abort) {
         // copies still in flight land before the CTA's shared memory is released
-        for (long x = (issued_x > RT_XS ? issued_x - RT_XS : 0); x < issued_x; x++) {
-            const uint32_t par = (uint32_t)((x / RT_XS) & 1);
-            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.x_full[x % RT_XS], par, 100000u); it++) {
+        for (long x = (issued_x > a.xs ? issued_x - a.xs : 0); x < issued_x; x++) {
+            const uint32_t par = (uint32_t)((x / a.xs) & 1);
+            for (long it = 0; it < 20000 && !ptx::mbar_try_wait_hint(&sm.x_full[x % a.xs], par, 100000u); it++) {
             }
         }
     }
@@ -339,7 +365,7 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
     if (warp == 0) ptx::tmem_dealloc(tbase, RT_TMEM_COLS);
     if (threadIdx.x == 0) {
         double r = 0.0, x = 0.0;
-        for (int w = 0; w < 4; w++) {
+        for (int w = 0; w < RT_EPI; w++) {
             r += sm.red[0][w];
             x += sm.red[1][w];
         }
@@ -371,6 +397,7 @@ bool residual_tc_plan(int order, const long *dims, long R, int *grid) {
     const int Rpad = (int)((R + 15) / 16 * 16);
     const long nq = (dims[1] + RT_NJ - 1) / RT_NJ;
     if (2 * rt_b_bytes(Rpad, (int)nq) > (size_t)RT_BMAX) return false;
+    if (rt_smem_bytes(Rpad, (int)nq, 2) > RT_SMEM_MAX) return false;
     long K = 1;
     for (int m = 2; m < order; m++) K *= dims[m];
     if (K > 0x7fffffffL || dims[0] > 0x7fffffffL || dims[1] > 0x7fffffffL) return false;
@@ -416,15 +443,18 @@ int residual_tc(const float *X, int order, const long *dims, const float *const 
     const long tiles = (dims[0] + RT_ROWS - 1) / RT_ROWS;
     a.cpt = (int)(grid / tiles);
     a.part = part;
-    const size_t smem = rt_smem_bytes(a.Rpad, a.nq);
+    a.xs = rt_ring(a.Rpad, a.nq);
+    const size_t smem = rt_smem_bytes(a.Rpad, a.nq, a.xs);
     static std::atomic<bool> attr[64];  // per device; zero-initialised
     int dev = 0;
     CUD_CHECK(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
-        CUD_CHECK(cudaFuncSetAttribute(k_residual_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
+        CUD_CHECK(cudaFuncSetAttribute(k_residual_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RT_SMEM_MAX));
         attr[dev].store(true, std::memory_order_release);
     }
+    const int pk = prof_begin(s);
     k_residual_tc<<<(unsigned)grid, RT_THREADS, smem, s>>>(tmap, a);
+    prof_end(pk, s);
     CUD_CHECK_LAUNCH("cp_residual tc");
     return sum_pairs(part, grid, out2, s);
 }

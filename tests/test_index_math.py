@@ -721,10 +721,16 @@ def test_residual_tc_index_math(dims, R):
     p = residual_tc_plan(dims, R)
     assert p is not None
     Rpad, nq, K, tiles, cpt = p
-    ctrl, xs, xbytes = 2048, 5, 128 * 32 * 4
+    ctrl, xbytes = 2048, 128 * 32 * 4
     bbytes = nq * 128 * Rpad * 2
     assert bbytes % 4096 == 0                                   # the X ring stays 1024-aligned
+    xs = 12                                                     # rt_ring: the deepest ring that fits
+    while xs > 2 and 1024 + ctrl + 2 * bbytes + xs * xbytes > 232448:
+        xs -= 1
     assert 1024 + ctrl + 2 * bbytes + xs * xbytes <= 232448     # shared memory
+    # ring slots and parities: stage x in slot x % xs, phase x // xs
+    for x in range(3 * xs + 1):
+        assert 0 <= x % xs < 12
     assert 2 * 128 + 2 * 64 <= 512                              # TMEM: accumulators + A' buffers
     # B words: every (chunk, row, k-chunk) once, inside one operand
     kcs = Rpad // 8
