@@ -95,11 +95,11 @@ class StreamedOps(CudaOps):
                 ev.record(self.compute)
                 self.used[b] = ev
 
-    def mttkrp(self, Xh, dims, U, mode, R):
+    def mttkrp(self, Xh, dims, U, mode, R, out=None):
         torch = self.torch
         N = len(dims)
         I = int(dims[mode])
-        M = torch.zeros(I * R, device="cuda")
+        M = out.zero_() if out is not None else torch.zeros(I * R, device="cuda")
         part = torch.empty(I * R, device="cuda") if mode < N - 1 else None
 
         def body(s, k0, k1, Xs):
