@@ -43,6 +43,11 @@ struct cud_cp_plan_s {
     // Gram and fit (side stream) run beside the next sweep's first MTTKRP
     cudaGraph_t graph_multi = nullptr;
     cudaGraphExec_t exec_multi = nullptr;
+    // the Delta-fit loop on the device: a graph whose WHILE node replays one
+    // sweep and k_loop_cond until the sweep limit or the tolerance stops it
+    cudaGraph_t graph_loop = nullptr;
+    cudaGraphExec_t exec_loop = nullptr;
+    struct LoopState *loop = nullptr;  // device
     // the R x R inverse of mode n depends only on the other modes' Grams, so
     // it runs on a second stream beside the mode-n MTTKRP
     cudaStream_t side = nullptr;
@@ -52,7 +57,29 @@ struct cud_cp_plan_s {
     bool fused = false;      // sweep layout (fused_sweep_pays)
 };
 
+// State of the device-side sweep loop (plan memory, set before each launch).
+struct LoopState {
+    int done;         // sweeps run by this launch
+    int max_sweeps;
+    int check_every;  // the tolerance is judged after every check_every-th sweep
+    int pad;
+    double tol;
+};
+
 namespace {
+
+// After each sweep of the loop graph: count it and decide whether the WHILE
+// node runs another -- the host loop's rule (stop at the sweep limit, or
+// when |fit - fit_prev| < tol at a checked sweep from the second on).
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, LoopState *st, const double *fit) {
+    if (threadIdx.x != 0) return;
+    const int d = st->done + 1;
+    st->done = d;
+    bool more = d < st->max_sweeps;
+    if (more && st->tol > 0.0 && d >= 2 && d % st->check_every == 0 && fabs(fit[0] - fit[1]) < st->tol)
+        more = false;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
 
 bool valid_dims(int order, const long *dims) {
     if (order < 1 || order > kMaxOrder || !dims) return false;
@@ -350,6 +377,8 @@ extern "C" int cud_cp_plan_destroy(cud_cp_plan p) {
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->exec_multi) cudaGraphExecDestroy(p->exec_multi);
     if (p->graph_multi) cudaGraphDestroy(p->graph_multi);
+    if (p->exec_loop) cudaGraphExecDestroy(p->exec_loop);
+    if (p->graph_loop) cudaGraphDestroy(p->graph_loop);
     if (p->side) {
         cudaStreamSynchronize(p->side);
         cudaStreamDestroy(p->side);
@@ -377,6 +406,51 @@ static int plan_refresh(cud_cp_plan_s *p, cudaStream_t s) {
     for (int m = 0; m < p->order && st == CUD_OK; m++)
         st = factor_gram(p->U[m], p->dims[m], p->R, p->G + (size_t)m * p->R * p->R, s);
     return st;
+}
+
+// The device-side loop graph (optional: the host loop is kept when the
+// driver refuses any step).  Its WHILE node's body is one sweep, as
+// enqueue_sweep captures it, then k_loop_cond; the condition is 1 at each
+// launch, so the body runs at least once (the caller launches it only for a
+// sweep limit >= 1).
+void build_loop_graph(cud_cp_plan_s *p, cudaStream_t s) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h = 0;
+    cudaGraph_t body = nullptr;
+    if (ok) ok = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        ok = cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess;
+        if (ok) body = np.conditional.phGraph_out[0];
+    }
+    if (ok) ok = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                 cudaSuccess;
+    if (ok) {
+        int cst = enqueue_sweep(p, s);
+        if (cst == CUD_OK) {
+            k_loop_cond<<<1, 32, 0, s>>>(h, p->loop, p->fit);
+            if (cudaGetLastError() != cudaSuccess) cst = CUD_ERR_CUDA;
+        }
+        cudaGraph_t captured = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &captured);
+        ok = cst == CUD_OK && e == cudaSuccess;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    (void)cudaGetLastError();  // a refused step leaves the host loop in place
+    if (ok) {
+        p->graph_loop = g;
+        p->exec_loop = ex;
+    } else {
+        if (ex) cudaGraphExecDestroy(ex);
+        if (g) cudaGraphDestroy(g);
+    }
 }
 
 extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, long R,
@@ -419,7 +493,8 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     size_t off_W = off_V + up(sizeof(double) * R * R);
     size_t off_F = off_W + up(sizeof(double) * 2 * R * R);
     size_t off_C = off_F + up(sizeof(double) * 4);  // fallbacks (int) + counter
-    size_t off_P = off_C + 256;
+    size_t off_L = off_C + 256;                      // loop state
+    size_t off_P = off_L + up(sizeof(LoopState));
     size_t off_S = off_P + up(sizeof(double) * update_ws_doubles(maxd, R));
     size_t bytes = off_S + up(wsb);
     cudaError_t e = cudaMalloc((void **)&p->mem, bytes);
@@ -441,6 +516,7 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
     p->fit = (double *)(p->mem + off_F);
     p->fallbacks = (int *)(p->mem + off_C);
     p->counter = (unsigned *)(p->mem + off_C + 64);
+    p->loop = (LoopState *)(p->mem + off_L);
     p->gpart = (double *)(p->mem + off_P);
     p->ws = p->mem + off_S;
     if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
@@ -485,6 +561,7 @@ extern "C" int cud_cp_plan_create(const float *X, int order, const long *dims, l
                     st = cuda_status(e, "cp plan instantiate (multi)");
             }
         }
+        if (st == CUD_OK) build_loop_graph(p, ss.s);
     }
     if (st == CUD_OK && cudaStreamSynchronize(ss.s) != cudaSuccess) st = CUD_ERR_CUDA;
     ss.close();
@@ -621,7 +698,17 @@ extern "C" int cud_cp_als(const float *X, int order, const long *dims, long R, f
         cudaEventRecord(t0, ss.s);
         int chunk = (opt.tol > 0 || opt.target_fit > 0) ? opt.check_every : opt.max_sweeps;
         if (chunk <= 0) chunk = 1;
-        while (sweeps < opt.max_sweeps && st == CUD_OK) {
+        if (p->exec_loop && opt.tol > 0 && opt.target_fit <= 0 && opt.max_sweeps > 0) {
+            // the Delta-fit loop runs on the device: no host round trip per check
+            LoopState ls = {0, opt.max_sweeps, opt.check_every, 0, opt.tol};
+            if (cudaMemcpyAsync(p->loop, &ls, sizeof(ls), cudaMemcpyHostToDevice, ss.s) != cudaSuccess ||
+                cudaGraphLaunch(p->exec_loop, ss.s) != cudaSuccess ||
+                cudaMemcpyAsync(&ls, p->loop, sizeof(ls), cudaMemcpyDeviceToHost, ss.s) != cudaSuccess ||
+                cudaStreamSynchronize(ss.s) != cudaSuccess)
+                st = cuda_status(cudaGetLastError(), "cp loop graph");
+            sweeps = ls.done;
+        }
+        while (sweeps < opt.max_sweeps && st == CUD_OK && !(p->exec_loop && opt.tol > 0 && opt.target_fit <= 0)) {
             int n = std::min(chunk, opt.max_sweeps - sweeps);
             st = cud_cp_plan_run(p, n, ss.s);
             sweeps += n;

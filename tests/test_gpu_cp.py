@@ -69,6 +69,24 @@ def test_graph_and_eager_agree(cd, layout):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("check_every,layout", [(1, 1), (3, 1), (2, 2)])
+def test_device_loop_stops_like_host_loop(cd, check_every, layout):
+    """With a Delta-fit tolerance the sweeps run in a graph whose WHILE node
+    judges the tolerance on the device; the eager path (no graph) keeps the
+    host loop.  Same sweep count, same fit, same factors."""
+    dims, R = (40, 36, 32), 5
+    X, init = low_rank(dims, R, seed=17, noise=1e-2)
+    Ua = [dev_t(f) for f in init]
+    Ub = [dev_t(f) for f in init]
+    ra = cd.cp_als(dev_t(X), dims, R, Ua, max_sweeps=200, tol=1e-5, check_every=check_every, layout=layout)
+    rb = cd.cp_als(dev_t(X), dims, R, Ub, max_sweeps=200, tol=1e-5, check_every=check_every, layout=layout,
+                   use_graph=False)
+    assert 2 <= ra.sweeps < 200 and ra.sweeps % check_every == 0
+    assert ra.sweeps == rb.sweeps and ra.fit == rb.fit
+    for a, b in zip(Ua, Ub):
+        assert torch.equal(a, b)
+
+
 def test_four_sweep_graph_equals_single_sweeps(cd):
     """Layout 2 replays four sweeps as one graph (each sweep's last Gram and
     fit beside the next sweep's first MTTKRP); the factors and fits must be
