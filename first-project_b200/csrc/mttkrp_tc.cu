@@ -816,6 +816,32 @@ __global__ void __launch_bounds__(256) k_pack_b(KrFactors fold, long R, int Rpad
         // U0's own rows (no index arithmetic)
 #pragma unroll
         for (int j = 0; j < 8; j++) v[j] = (r < R) ? __ldg(fold.U[0] + 32 * t + 8 * kc + j + (long)r * fold.rows[0]) : 0.f;
+    } else if (fold.rows[0] % 8 == 0 && (reinterpret_cast<uintptr_t>(fold.U[0]) & 15) == 0) {
+        // the 8 rows 8 (4 t + kc) .. + 7 share every digit but the fastest
+        // (8 divides its extent): one row of each slower factor, and 8
+        // consecutive rows of the fastest as two 16-byte loads (its column r
+        // starts at r * rows_0, a multiple of 8 floats).  With three or more
+        // folded factors the product is formed in another order than below
+        // (U_0 (U_1 U_2) against (U_0 U_1) U_2): the same value to FP32
+        // rounding, ahead of the BF16 split.
+        const uint32_t d0 = (uint32_t)fold.rows[0];
+        uint32_t lin = (uint32_t)(32 * t + 8 * kc);  // < frows < 2^31 (the plan's bound)
+        uint32_t q = lin / d0;
+        const uint32_t x0 = lin - q * d0;
+        float c = 1.f;
+        for (int f = 1; f < fold.n; f++) {
+            const uint32_t d = (uint32_t)fold.rows[f], qd = q / d;
+            c *= (r < R) ? __ldg(fold.U[f] + (q - qd * d) + (long)r * d) : 0.f;
+            q = qd;
+        }
+        float4 u0 = make_float4(0.f, 0.f, 0.f, 0.f), u1 = u0;
+        if (r < R) {
+            const float4 *src = reinterpret_cast<const float4 *>(fold.U[0] + x0 + (long)r * d0);
+            u0 = __ldg(src);
+            u1 = __ldg(src + 1);
+        }
+        v[0] = u0.x * c; v[1] = u0.y * c; v[2] = u0.z * c; v[3] = u0.w * c;
+        v[4] = u1.x * c; v[5] = u1.y * c; v[6] = u1.z * c; v[7] = u1.w * c;
     } else {
 #pragma unroll
         for (int j = 0; j < 8; j++) {
