@@ -458,7 +458,7 @@ def run_residual_once(cd, torch, dims, R, reps=5):
     return {"dims": list(dims), "rank": R, "ms_per_call": round(dt * 1e3, 4),
             "kernel_ms": round(k_ms, 4) if k_ms else None,
             "kernel_gbs": round(4 * X.numel() / (k_ms * 1e-3) / 1e9, 1) if k_ms else None,
-            "fit": 1 - (r2 / x2) ** 0.5}
+            "fit": 1 - (r2 / x2) ** 0.5 if x2 > 0 else None}
 
 
 def run_tucker_once(cd, torch, dims, ranks):

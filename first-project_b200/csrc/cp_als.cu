@@ -605,10 +605,13 @@ extern "C" int cud_cp_plan_fit(cud_cp_plan p, double *fit, double *fit_prev, voi
 
 extern "C" int cud_cp_plan_true_fit(cud_cp_plan p, double *fit, void *stream) {
     if (!p) return set_status(CUD_ERR_INVALID_ARGUMENT);
-    double res2 = 0.0, x2 = 0.0;
-    int st = cud_cp_residual(p->X, p->order, p->dims, const_cast<const float *const *>(p->U), p->R, &res2, &x2,
-                             stream);
-    if (st) return st;
+    // ||X||^2 is the plan's (FP64, from its refresh): the residual pass
+    // only sums (x - xh)^2
+    double res2 = 0.0;
+    int st = cp_residual_host(p->X, p->order, p->dims, const_cast<const float *const *>(p->U), p->R, false, &res2,
+                              nullptr, as_stream(stream));
+    if (st) return set_status(st);
+    const double x2 = p->normx2;
     if (fit) *fit = 1.0 - sqrt(res2) / sqrt(x2 > 0.0 ? x2 : 1.0);
     return set_status(CUD_OK);
 }

@@ -123,8 +123,13 @@ int mttkrp_run_parts(const float *X, int order, const long *dims, const float *c
 // (order >= 3, R <= 64; the grid it launches, for sizing the partials).
 int sum_pairs(const double *part, long n, double *out, cudaStream_t s);
 bool residual_tc_plan(int order, const long *dims, long R, int *grid);
+// need_x2 = false: out2[1] (||X||^2) is left 0 -- a caller that already has
+// the norm saves the FP64 sum of squares (about a tenth of the kernel).
 int residual_tc(const float *X, int order, const long *dims, const float *const *U, long R, double *part,
-                double *out2, cudaStream_t s);
+                double *out2, cudaStream_t s, bool need_x2 = true);
+// ||X - [[U]]||^2 (and ||X||^2 when need_x2) to the host, synchronising s.
+int cp_residual_host(const float *X, int order, const long *dims, const float *const *U, long R, bool need_x2,
+                     double *res_norm2, double *x_norm2, cudaStream_t s);
 
 // Mode product Y = X x_mode W (contract.cu); W is J x dims[mode], or its
 // transpose when w_trans is set.

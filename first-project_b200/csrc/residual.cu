@@ -396,7 +396,7 @@ size_t cp_residual_ws_bytes(int order, const long *dims) {
 }
 
 int cp_residual(const float *X, int order, const long *dims, const float *const *U, long R, double *out2,
-                void *ws, cudaStream_t s) {
+                void *ws, cudaStream_t s, bool need_x2 = true) {
     if (order < 1 || order > kMaxOrder || R <= 0) return CUD_ERR_INVALID_ARGUMENT;
     ResArgs a;
     a.X = X;
@@ -413,7 +413,7 @@ int cp_residual(const float *X, int order, const long *dims, const float *const 
     }
     a.part = static_cast<double *>(ws);
     {
-        const int st = residual_tc(X, order, dims, U, R, a.part, out2, s);
+        const int st = residual_tc(X, order, dims, U, R, a.part, out2, s, need_x2);
         if (st != CUD_ERR_UNSUPPORTED) return st;
     }
     long qt, stg, ch, sp;
@@ -445,6 +445,24 @@ int cp_residual(const float *X, int order, const long *dims, const float *const 
     return CUD_OK;
 }
 
+int cp_residual_host(const float *X, int order, const long *dims, const float *const *U, long R, bool need_x2,
+                     double *res_norm2, double *x_norm2, cudaStream_t s) {
+    int st;
+    const size_t bytes = cp_residual_ws_bytes(order, dims);
+    double *ws = static_cast<double *>(scratch(kSlotReduce, bytes, &st));
+    if (!ws) return st;
+    double *out = ws + (bytes / sizeof(double) - 2);
+    st = cp_residual(X, order, dims, U, R, out, ws, s, need_x2);
+    if (st) return st;
+    double *h = pinned_scalars();
+    if (!h) return CUD_ERR_NO_MEMORY;
+    CUD_CHECK(cudaMemcpyAsync(h, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUD_CHECK(cudaStreamSynchronize(s));
+    if (res_norm2) *res_norm2 = h[0];
+    if (x_norm2) *x_norm2 = h[1];
+    return CUD_OK;
+}
+
 }  // namespace cud
 
 using namespace cud;
@@ -454,19 +472,5 @@ extern "C" int cud_cp_residual(const float *X, int order, const long *dims, cons
     if (!X || !dims || !U || order < 1 || order > kMaxOrder || R <= 0) return set_status(CUD_ERR_INVALID_ARGUMENT);
     for (int m = 0; m < order; m++)
         if (dims[m] <= 0 || !U[m]) return set_status(CUD_ERR_INVALID_ARGUMENT);
-    cudaStream_t s = as_stream(stream);
-    int st;
-    const size_t bytes = cp_residual_ws_bytes(order, dims);
-    double *ws = static_cast<double *>(scratch(kSlotReduce, bytes, &st));
-    if (!ws) return set_status(st);
-    double *out = ws + (bytes / sizeof(double) - 2);
-    st = cp_residual(X, order, dims, U, R, out, ws, s);
-    if (st) return set_status(st);
-    double *h = pinned_scalars();
-    if (!h) return set_status(CUD_ERR_NO_MEMORY);
-    CUD_CHECK(cudaMemcpyAsync(h, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CUD_CHECK(cudaStreamSynchronize(s));
-    if (res_norm2) *res_norm2 = h[0];
-    if (x_norm2) *x_norm2 = h[1];
-    return set_status(CUD_OK);
+    return set_status(cp_residual_host(X, order, dims, U, R, true, res_norm2, x_norm2, as_stream(stream)));
 }

@@ -66,6 +66,7 @@ struct RtArgs {
     int R, Rpad, nq;      // rank, rank rounded to 16, chunks of 128 U_1 rows
     int cpt;              // CTAs per row tile (they split k)
     int xs;               // X ring depth
+    int need_x2;          // also sum x^2 (the caller may know ||X||^2 already)
     double *part;         // [grid][2]
 };
 
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(RT_THREADS, 1)
                     const float x = xs[jj * RT_ROWS + row];
                     const float dv = x - __uint_as_float(v[s][jj]);
                     fr[jj & 3] = fmaf(dv, dv, fr[jj & 3]);
-                    sx[jj & 3] = fma((double)x, (double)x, sx[jj & 3]);
+                    if (a.need_x2) sx[jj & 3] = fma((double)x, (double)x, sx[jj & 3]);
                 }
 #pragma unroll
                 for (int c = 0; c < 4; c++) sr[c] += (double)fr[c];
@@ -408,7 +409,7 @@ bool residual_tc_plan(int order, const long *dims, long R, int *grid) {
 }
 
 int residual_tc(const float *X, int order, const long *dims, const float *const *U, long R, double *part,
-                double *out2, cudaStream_t s) {
+                double *out2, cudaStream_t s, bool need_x2) {
     int grid = 0;
     if (!residual_tc_plan(order, dims, R, &grid)) return CUD_ERR_UNSUPPORTED;
     if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return CUD_ERR_UNSUPPORTED;
@@ -443,6 +444,7 @@ int residual_tc(const float *X, int order, const long *dims, const float *const 
     const long tiles = (dims[0] + RT_ROWS - 1) / RT_ROWS;
     a.cpt = (int)(grid / tiles);
     a.part = part;
+    a.need_x2 = need_x2 ? 1 : 0;
     a.xs = rt_ring(a.Rpad, a.nq);
     const size_t smem = rt_smem_bytes(a.Rpad, a.nq, a.xs);
     static std::atomic<bool> attr[64];  // per device; zero-initialised
