@@ -663,33 +663,44 @@ extern "C" int cud_cp_batched_tune(int ntensors, const long *dims, const long *r
     // (threads, CTAs per SM) within the launch bounds' register budgets and
     // shared memory (~45 KB a CTA)
     const std::vector<BatchCfg> cand = {{128, 4}, {128, 5}, {192, 3}, {256, 2}, {384, 2}};
-    float best = 1e30f;
     BatchCfg bestc{192, 3};
     cudaStream_t s = as_stream(stream);
     cudaEvent_t e0, e1;
     CUD_CHECK(cudaEventCreate(&e0));
     CUD_CHECK(cudaEventCreate(&e1));
-    for (auto &c : cand) {
-        {
-            std::lock_guard<std::mutex> lk(g_tune_mu);
-            g_tune[key] = c;
+    // an untimed round (first launches load each width's kernel), then two
+    // timed rounds in turn; a candidate's time is its best of the two (one
+    // timing a candidate picked a slower shape on some runs)
+    std::vector<float> best_ms(cand.size(), 1e30f);
+    for (int round = 0; round < 3; round++) {
+        for (size_t ci = 0; ci < cand.size(); ci++) {
+            {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                g_tune[key] = cand[ci];
+            }
+            cud_cp_options opt;
+            cud_cp_default_options(&opt);
+            opt.max_sweeps = round == 0 ? 1 : 2;
+            opt.tol = 0.0;
+            opt.use_graph = 0;
+            opt.check_every = opt.max_sweeps;
+            cudaEventRecord(e0, s);
+            int st = cud_cp_als_batched(ntensors, dims, ranks, X, x_offsets, U_scratch, u_offsets, &opt,
+                                        nullptr, nullptr, nullptr, stream);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return set_status(st); }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (round > 0 && ms < best_ms[ci]) best_ms[ci] = ms;
         }
-        cud_cp_options opt;
-        cud_cp_default_options(&opt);
-        opt.max_sweeps = 2;
-        opt.tol = 0.0;
-        opt.use_graph = 0;
-        opt.check_every = 2;
-        cudaEventRecord(e0, s);
-        int st = cud_cp_als_batched(ntensors, dims, ranks, X, x_offsets, U_scratch, u_offsets, &opt,
-                                    nullptr, nullptr, nullptr, stream);
-        cudaEventRecord(e1, s);
-        cudaEventSynchronize(e1);
-        if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return set_status(st); }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) { best = ms; bestc = c; }
     }
+    float best = 1e30f;
+    for (size_t ci = 0; ci < cand.size(); ci++)
+        if (best_ms[ci] < best) {
+            best = best_ms[ci];
+            bestc = cand[ci];
+        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     {
