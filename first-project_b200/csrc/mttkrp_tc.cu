@@ -92,6 +92,8 @@ struct TcArgs {
     long blk;          // stages per constant-row block (folded rows / 32)
     int fold;          // pre-packed B path: factors folded into B, counted along gen then outer
     long frows;        // pre-packed B path: product of the folded factors' rows (= 32 * blk)
+    int pack_pdl;      // pre-packed B path: the pack was launched programmatically (may overlap
+                       // the kernel before it), so factor reads wait for the pack grid
 };
 
 struct TcCtrl {
@@ -803,8 +805,14 @@ __global__ void __launch_bounds__(256) k_pack_b(KrFactors fold, long R, int Rpad
                                                 uint8_t *__restrict__ pb, int *error) {
     const long n = blk * 4 * Rpad;
     const long id = blockIdx.x * 256L + threadIdx.x;
+    // this grid may have started early (launched programmatically after the
+    // previous kernel, e.g. the previous mode's factor update): the factors
+    // it reads and the tiles it writes wait for that kernel first
+    ptx::griddep_wait();
     // the MTTKRP kernel may start now: it waits for this grid only before it
-    // reads the packed tiles
+    // reads the packed tiles, and its other reads (X, the factors' constant
+    // rows) need nothing from this grid -- the factors are final, since this
+    // grid has passed its wait
     ptx::griddep_launch();
     if (id == 0) *error = 0;
     if (id >= n) return;
@@ -1110,6 +1118,10 @@ __global__ void __launch_bounds__(PB_THREADS, MINB)
         }
     } else {
         // ------------------------------------------------------------ constant rows
+        // after a programmatic pack launch the factors may come from a kernel
+        // that ran just before the B pack (a factor update): read them only
+        // once the pack grid, which waited for that kernel, has completed
+        if (a.pack_pdl) ptx::griddep_wait();
         SegTrack tr(st_beg, a.blk);
         bool seg_first = true;
         for (long i = 0; i < nst; i++) {
@@ -1498,8 +1510,20 @@ int mttkrp_tc(const float *X, int order, const long *dims, const float *const *U
             fold.rows[fold.n] = a.outer.rows[f];
         }
         const long items = p.blk * 4 * p.Rpad;
-        k_pack_b<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(fold, R, (int)p.Rpad, p.blk, precision,
-                                                                 const_cast<uint8_t *>(a.pb), a.error);
+        const unsigned pgrid = (unsigned)((items + 255) / 256);
+        // Below 64 MiB of X the MTTKRP is short enough that the pack's launch
+        // gap shows (128^3, R = 16: 4 % of a sweep), so the pack launches
+        // programmatically behind the kernel before it; above, the constant-row
+        // warp's early start is worth more than the hidden launch.
+        a.pack_pdl = (p.P * p.Q * p.S * 4 < (64L << 20)) ? 1 : 0;
+        if (a.pack_pdl) {
+            PdlLaunch l(pgrid, 256, 0, s);
+            CUD_CHECK(cudaLaunchKernelEx(&l.cfg, k_pack_b, fold, R, (int)p.Rpad, p.blk, precision,
+                                         const_cast<uint8_t *>(a.pb), a.error));
+        } else {
+            k_pack_b<<<pgrid, 256, 0, s>>>(fold, R, (int)p.Rpad, p.blk, precision, const_cast<uint8_t *>(a.pb),
+                                           a.error);
+        }
         CUD_CHECK_LAUNCH("mttkrp_pb pack");
         a.tmem_cols = (2 * p.Rpad + p.nb * 32 <= 256) ? 256u : 512u;
         const unsigned grid = (unsigned)(p.qtiles * p.splits);
