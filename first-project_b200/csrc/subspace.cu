@@ -15,6 +15,9 @@
 // does not converge.
 #include <cooperative_groups.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace cud {
@@ -716,6 +719,125 @@ __global__ void __launch_bounds__(256) k_si_apply_cols(const double *__restrict_
         }
 }
 
+// After each batch of steps in the loop graph: whether its WHILE node runs
+// another batch -- the host loop's rule (stop once the iteration has
+// converged or failed, or max_iters steps have run; every step of a batch
+// that has not converged runs, so st[2] counts the steps queued).
+__global__ void k_si_loop_cond(cudaGraphConditionalHandle h, const int *fail, const int *st, int max_iters) {
+    if (threadIdx.x != 0) return;
+    const bool more = *fail == 0 && st[0] == 0 && st[2] < max_iters;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+constexpr int SI_BATCH = 4;  // steps queued between two reads of the state
+
+// One batch of SI_BATCH fast-path steps from V = buffer 0 (ws), as the host
+// loop queues it; SI_BATCH is even, so the batch ends with V in buffer 0
+// again and every batch is the same launch sequence.
+struct SiSteps {
+    const double *G;
+    long n;
+    int r, nks;
+    long kchunk;
+    dim3 ga;
+    size_t smem;
+    double *ws, *part, *part2, *scal;
+    int *fail, *st;
+    void enqueue(int steps, cudaStream_t s) const {
+        const long nr = n * (long)r;
+        double *V = ws, *Y = ws + nr;
+        for (int b = 0; b < steps; b++) {
+            // two products per orthonormalisation (G^2 V): the columns' condition
+            // grows by (lambda_1 / lambda_r)^2 per step, well inside CholQR2's range
+            k_si_apply_cols<<<ga, 256, 0, s>>>(G, V, 1, n, r, kchunk, part2, st);
+            k_si_apply_cols<<<ga, 256, 0, s>>>(G, part2, nks, n, r, kchunk, part, st);
+            k_si_orth_cl<<<CL_N, CL_T, smem, s>>>(part, nks, V, n, r, Y, scal, fail, st);
+            std::swap(V, Y);
+        }
+    }
+};
+
+// Loop graphs of the fast path, one per (device, G, n, r, ws, nks,
+// max_iters): a WHILE node whose body is one batch and k_si_loop_cond, so a
+// call reads the state once instead of once per batch.  The key holds the
+// exact pointers the captured launches use.  A few entries (the Tucker
+// drivers call with one Gram and one workspace per plan); the oldest is
+// replaced.
+struct SiGraph {
+    int dev = -1;
+    const double *G = nullptr, *ws = nullptr;
+    long n = 0;
+    int r = 0, nks = 0, max_iters = 0;
+    cudaGraphExec_t ex = nullptr;
+};
+constexpr int SI_GRAPHS = 8;
+std::mutex g_si_mu;
+SiGraph g_si[SI_GRAPHS];
+int g_si_next = 0;
+
+// Capture the loop graph on a private stream (capturing records the
+// launches without running them); null when the driver refuses any step,
+// and the caller keeps the host loop.
+cudaGraphExec_t si_build_loop(const SiSteps &k, int max_iters) {
+    cudaStream_t cs = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h = 0;
+    cudaGraph_t body = nullptr;
+    if (ok) ok = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        ok = cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess;
+        if (ok) body = np.conditional.phGraph_out[0];
+    }
+    if (ok) ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                 cudaSuccess;
+    if (ok) {
+        k.enqueue(SI_BATCH, cs);
+        k_si_loop_cond<<<1, 32, 0, cs>>>(h, k.fail, k.st, max_iters);
+        const bool launched = cudaGetLastError() == cudaSuccess;
+        cudaGraph_t captured = nullptr;
+        ok = cudaStreamEndCapture(cs, &captured) == cudaSuccess && launched;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    (void)cudaGetLastError();
+    if (!ok && ex) {
+        cudaGraphExecDestroy(ex);
+        ex = nullptr;
+    }
+    if (g) cudaGraphDestroy(g);  // the executable graph keeps what it needs
+    cudaStreamDestroy(cs);
+    return ex;
+}
+
+cudaGraphExec_t si_loop_graph(int dev, const SiSteps &k, int max_iters) {
+    std::lock_guard<std::mutex> lk(g_si_mu);
+    for (const SiGraph &e : g_si)
+        if (e.ex && e.dev == dev && e.G == k.G && e.ws == k.ws && e.n == k.n && e.r == k.r && e.nks == k.nks &&
+            e.max_iters == max_iters)
+            return e.ex;
+    cudaGraphExec_t ex = si_build_loop(k, max_iters);
+    if (!ex) return nullptr;
+    SiGraph &slot = g_si[g_si_next];
+    g_si_next = (g_si_next + 1) % SI_GRAPHS;
+    // an executable graph still in flight is freed when its launch completes
+    if (slot.ex) cudaGraphExecDestroy(slot.ex);
+    slot.dev = dev; slot.G = k.G; slot.ws = k.ws; slot.n = k.n; slot.r = k.r; slot.nks = k.nks;
+    slot.max_iters = max_iters;
+    slot.ex = ex;
+    return ex;
+}
+
 }  // namespace
 
 size_t subspace_ws_doubles(long n, long r) { return 3 * (size_t)n * r + 8; }  // V, Y, W (r*r <= n*r), scalars
@@ -731,13 +853,13 @@ static int top_eigvecs_fast(const double *G, long n, long r, float *U, double *w
     const int nks = (int)std::max(0L, std::min(8L, room));
     if (nks < 1) return CUD_ERR_UNSUPPORTED;
     const size_t smem = cl_layout(n).total * sizeof(double);
+    int dev = 0;
+    CUD_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return CUD_ERR_UNSUPPORTED;
     {
         // once per device: the shared-memory opt-in, and whether a cluster
         // of this size can be resident at all
-        static int ready[64] = {0};  // 0 unknown, 1 usable, 2 not
-        int dev = 0;
-        CUD_CHECK(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= 64) return CUD_ERR_UNSUPPORTED;
+        static std::atomic<int> ready[64];  // 0 unknown, 1 usable, 2 not; zero-initialised
         if (!ready[dev]) {
             CUD_CHECK(cudaFuncSetAttribute(k_si_orth_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CL_SMEM_MAX));
             CUD_CHECK(cudaFuncSetAttribute(k_si_ritz_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CL_SMEM_MAX));
@@ -768,22 +890,23 @@ static int top_eigvecs_fast(const double *G, long n, long r, float *U, double *w
     else k_si_init<<<gi, 256, 0, s>>>(Y, n, (int)r);
     k_si_orth_cl<<<CL_N, CL_T, smem, s>>>(Y, 1, nullptr, n, (int)r, V, scal, fail, nullptr);
     CUD_CHECK_LAUNCH("subspace init");
-    // steps are queued SI_BATCH at a time; the state is read once per batch
-    // and the launches after convergence return at once.  Step j (from 1)
-    // writes buffer j % 2 (buffer 0 = the initial V).
-    constexpr int SI_BATCH = 4;
+    // Steps are queued SI_BATCH at a time and the launches after convergence
+    // return at once.  Step j (from 1) writes buffer j % 2 (buffer 0 = the
+    // initial V).  When max_iters is a whole number of batches, the batches
+    // run in the loop graph and the state is read once; otherwise the host
+    // reads it after every batch.
+    const SiSteps k{G, n, (int)r, nks, kchunk, ga, smem, ws, part, part2, scal, fail, st};
+    const cudaGraphExec_t loop = (max_iters % SI_BATCH == 0) ? si_loop_graph(dev, k, max_iters) : nullptr;
     for (int queued = 0; queued < max_iters;) {
-        const int nb = std::min(SI_BATCH, max_iters - queued);
-        for (int b = 0; b < nb; b++) {
-            // two products per orthonormalisation (G^2 V): the columns' condition
-            // grows by (lambda_1 / lambda_r)^2 per step, well inside CholQR2's range
-            k_si_apply_cols<<<ga, 256, 0, s>>>(G, V, 1, n, (int)r, kchunk, part2, st);
-            k_si_apply_cols<<<ga, 256, 0, s>>>(G, part2, nks, n, (int)r, kchunk, part, st);
-            k_si_orth_cl<<<CL_N, CL_T, smem, s>>>(part, nks, V, n, (int)r, Y, scal, fail, st);
-            std::swap(V, Y);
+        if (loop) {
+            CUD_CHECK(cudaGraphLaunch(loop, s));
+            queued = max_iters;
+        } else {
+            const int nb = std::min(SI_BATCH, max_iters - queued);
+            k.enqueue(nb, s);
+            CUD_CHECK_LAUNCH("subspace steps");
+            queued += nb;
         }
-        CUD_CHECK_LAUNCH("subspace steps");
-        queued += nb;
         CUD_CHECK(cudaMemcpyAsync(h, scal + 2, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
         CUD_CHECK(cudaStreamSynchronize(s));
         const int *hs = reinterpret_cast<const int *>(h);  // fail, pad, done, extra + 1, steps, final
