@@ -761,8 +761,9 @@ struct SiSteps {
 // max_iters): a WHILE node whose body is one batch and k_si_loop_cond, so a
 // call reads the state once instead of once per batch.  The key holds the
 // exact pointers the captured launches use.  A few entries (the Tucker
-// drivers call with one Gram and one workspace per plan); the oldest is
-// replaced.
+// drivers call with one Gram and one workspace per plan), never replaced,
+// since another thread may be launching one: once all are taken, new keys
+// keep the host loop.
 struct SiGraph {
     int dev = -1;
     const double *G = nullptr, *ws = nullptr;
@@ -773,7 +774,8 @@ struct SiGraph {
 constexpr int SI_GRAPHS = 8;
 std::mutex g_si_mu;
 SiGraph g_si[SI_GRAPHS];
-int g_si_next = 0;
+int g_si_used = 0;
+bool g_si_refused[64] = {};  // per device: the driver refused a loop graph once; keep the host loop
 
 // Capture the loop graph on a private stream (capturing records the
 // launches without running them); null when the driver refuses any step,
@@ -826,12 +828,13 @@ cudaGraphExec_t si_loop_graph(int dev, const SiSteps &k, int max_iters) {
         if (e.ex && e.dev == dev && e.G == k.G && e.ws == k.ws && e.n == k.n && e.r == k.r && e.nks == k.nks &&
             e.max_iters == max_iters)
             return e.ex;
+    if (g_si_used == SI_GRAPHS || g_si_refused[dev]) return nullptr;
     cudaGraphExec_t ex = si_build_loop(k, max_iters);
-    if (!ex) return nullptr;
-    SiGraph &slot = g_si[g_si_next];
-    g_si_next = (g_si_next + 1) % SI_GRAPHS;
-    // an executable graph still in flight is freed when its launch completes
-    if (slot.ex) cudaGraphExecDestroy(slot.ex);
+    if (!ex) {
+        g_si_refused[dev] = true;
+        return nullptr;
+    }
+    SiGraph &slot = g_si[g_si_used++];
     slot.dev = dev; slot.G = k.G; slot.ws = k.ws; slot.n = k.n; slot.r = k.r; slot.nks = k.nks;
     slot.max_iters = max_iters;
     slot.ex = ex;
