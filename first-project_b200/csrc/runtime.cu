@@ -1,4 +1,5 @@
 // Status side channel, scratch arena and pinned host scalars.
+#include <atomic>
 #include <mutex>
 #include <stdio.h>
 #include <string.h>
@@ -82,7 +83,7 @@ double *pinned_scalars() {
 // captured into a graph).  Up to kProfPairs pairs are kept until read.
 constexpr int kProfPairs = 256;
 static std::mutex g_prof_mu;
-static bool g_prof_on = false;
+static std::atomic<bool> g_prof_on{false};  // read by every MTTKRP call without the lock
 static int g_prof_n = 0;
 static cudaEvent_t g_prof_ev[2 * kProfPairs];
 static bool g_prof_made = false;
